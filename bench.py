@@ -1,0 +1,489 @@
+#!/usr/bin/env python
+"""Throughput of the fused LBM step on B200 (MLUPS and HBM-roofline fraction).
+
+Default workload: D3Q27 MRT lid-driven cavity 256^3 (Gram-Schmidt moment basis, lid 0.05 on the
+z-top face, shear rate from Re 1000, other rates 1.2), FP16-shifted storage as the headline value
+and FP32 plain storage beside it.  One bench step = one lattice time step (one kernel launch over
+all 16.8M cells); the populations (0.85 GB FP16 / 1.7 GB FP32 per buffer) are larger than L2, so
+no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Under torchrun (N > 1) every rank advances its own replica lattice (weak scaling, no data-path
+collective); the reported time is the max over ranks.  `--impl reference` times the CPU
+restatement of the reference's loop (the reference's ArrayFire CPU backend is not installed).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "lbm-arrayfire_b200"))
+
+METRIC = "MLUPS & HBM-roofline %: FP16-shifted vs FP32 plain at <=1e-3 rel L2 vs FP64"
+FALLBACK_HBM_GBS = 6650.0
+
+# ---------------------------------------------------------------------------------------------
+# workloads (the engine side); each returns (desc, mask, F0 or None = rest state)
+# ---------------------------------------------------------------------------------------------
+
+
+def wl_mrt256(lb, storage, n=256):
+    """D3Q27 MRT lid cavity n^3, Gram-Schmidt basis, lid 0.05, sv from Re 1000 at L=256."""
+    sv = 1.0 / (3.0 * (0.05 * 256 / 1000.0) + 0.5)
+    d = lb.make_desc(lb.D3Q27, lb.MRT, storage, (n, n, n), mrt_s=lb.mrt_rates(sv, 1.2),
+                     mrt_basis=lb.MRT_GRAM_SCHMIDT)
+    m = lb.setup_cavity3d(d, 0.05)
+    return d, m
+
+
+def wl_channel(lb, storage, n=None):
+    """D2Q9 channel 1024x256, circle d=40 at (200,128), inlet 0.04, zero-gradient outlet, Re 200."""
+    nu = 0.04 * 40 / 200.0
+    d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (1024, 256), omega=1.0 / (3 * nu + 0.5))
+    m = lb.setup_channel2d(d, 0.04, 200, 128, 20, True)
+    return d, m
+
+
+def wl_cavity128(lb, storage, n=None):
+    d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (128, 128), omega=lb.omega_from_re(0.1, 128, 100.0, 0))
+    m = lb.setup_cavity2d(d, 0.1)
+    return d, m
+
+
+def wl_sc1024(lb, storage, n=None):
+    d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, storage, (1024, 1024), omega=1.0, sc_G=-5.5)
+    return d, None
+
+
+def wl_bgk3d(lb, storage, n=256):
+    d = lb.make_desc(lb.D3Q27, lb.BGK, storage, (n, n, n), omega=lb.omega_from_re(0.05, n, 1000.0, 0))
+    m = lb.setup_cavity3d(d, 0.05)
+    return d, m
+
+
+def wl_cavity2d_big(lb, storage, n=8192):
+    d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (n, n), omega=lb.omega_from_re(0.1, n, 1000.0, 1))
+    m = lb.setup_cavity2d(d, 0.1)
+    return d, m
+
+
+WORKLOADS = {
+    "d3q27_mrt_gs_lid_256": (wl_mrt256, "D3Q27 MRT (Gram-Schmidt) lid cavity 256^3, lid 0.05 z-top, Re 1000"),
+    "d2q9_channel_1024x256": (wl_channel, "D2Q9 BGK channel 1024x256, cylinder d=40, inlet 0.04, Re 200"),
+    "d2q9_lid_128": (wl_cavity128, "D2Q9 BGK lid cavity 128^2, lid 0.1, Re 100"),
+    "d2q9_shanchen_1024": (wl_sc1024, "D2Q9 Shan-Chen 1024^2 periodic, G=-5.5, tau=1"),
+    "d3q27_bgk_lid_256": (wl_bgk3d, "D3Q27 BGK lid cavity 256^3"),
+    "d2q9_lid_8192": (wl_cavity2d_big, "D2Q9 BGK lid cavity 8192^2"),
+}
+
+STORAGE_NAMES = {0: "f32", 1: "f16s", 2: "bf16s", 3: "f64"}
+
+
+def storage_bytes(storage):
+    return {0: 4, 1: 2, 2: 2, 3: 8}[storage]
+
+
+def algorithmic_bytes_per_cell(d):
+    """2 Q s (read + write of every population); Shan-Chen adds the psi write and read (8 B)."""
+    b = 2 * d.q * storage_bytes(d.storage)
+    if d.collision == 2:
+        b += 8
+    return b
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            j = json.loads(p.read_text())
+            return float(j["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def dram_traffic(workload, storage):
+    """Per-launch DRAM bytes of the step kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "dram_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and not line.startswith("#") and parts[0] == workload and parts[1] == STORAGE_NAMES[storage]:
+            return float(parts[2])
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", gpu_id, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            return None
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            cols = [c.strip() for c in line.split(",")]
+            if len(cols) < 8:
+                continue
+            try:
+                sm.append(float(cols[0]))
+                smax.append(float(cols[1]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if cols[4 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gpu_id_for_smi(torch, dev):
+    try:
+        u = torch.cuda.get_device_properties(dev).uuid
+        return f"GPU-{u}"
+    except Exception:
+        return str(dev)
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU restatement (oracle) timings: the cpu_baseline object and the reference arm
+# ---------------------------------------------------------------------------------------------
+def oracle_problem_for(workload, n_side):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    sys.path.insert(0, str(ROOT / "tests"))
+    import lbm_b200 as lb
+    from helpers import oracle_problem
+
+    fn = WORKLOADS[workload][0]
+    if workload.startswith("d3q27"):
+        d, m = fn(lb, lb.F32, n_side)
+    else:
+        d, m = fn(lb, lb.F32)
+    return oracle_problem(d, m), d
+
+
+def oracle_mlups(workload, target_s, cube=None):
+    """Time the oracle (FP32, all host threads) on a sample of the workload for ~target_s seconds."""
+    import oracle as O
+
+    side = cube or 64
+    p, d = oracle_problem_for(workload, side)
+    F0 = O.init_equilibrium(p)
+    t = time.perf_counter()
+    O.run(p, F0, 1, dtype=np.float32)
+    t1 = max(time.perf_counter() - t, 1e-4)
+    steps = max(2, int(target_s / t1))
+    t = time.perf_counter()
+    O.run(p, F0, steps, dtype=np.float32)
+    dt = time.perf_counter() - t
+    cells = p.n
+    return cells * steps / dt / 1e6, cells, steps, p.shape
+
+
+def threads():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the CPU restatement of the reference loop, on rank 0 only."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    O.lib()
+    # calibrate, then pick a sample lattice so that W + K steps end within ~150 s
+    mlups0, _, _, _ = oracle_mlups(args.workload, 1.0)
+    budget_cells = mlups0 * 1e6 * 150.0 / max(1, args.steps + args.warmup)
+    if args.workload.startswith("d3q27"):
+        side = int(max(8, min(256, math.floor(budget_cells ** (1 / 3)))))
+        p, d = oracle_problem_for(args.workload, side)
+    else:
+        p, d = oracle_problem_for(args.workload, None)
+    F = O.init_equilibrium(p)
+    if args.warmup:
+        F, _, _ = O.run(p, F, args.warmup, dtype=np.float32)
+    t = time.perf_counter()
+    O.run(p, F, args.steps, dtype=np.float32)
+    dt = time.perf_counter() - t
+    value = p.n * args.steps / dt / 1e6
+    sample = f"{'x'.join(map(str, p.shape))} lattice of the same workload, {args.steps} timed steps, FP32, " \
+             f"{threads()} threads on {cpu_model()}"
+    return {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload][1], "sample_shape": list(p.shape)},
+        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": threads(), "kind": "port", "sample": sample,
+                         "note": "ArrayFire CPU backend unavailable on this box; C restatement of the reference loop"},
+        "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------------------
+def timed_steps(torch, lat, steps, dev):
+    """Device time of `steps` lattice steps on the context's stream (CUDA events)."""
+    s = torch.cuda.ExternalStream(lat.stream(), device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    lat.step(steps)
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3
+
+
+def measure(torch, lb, args, storage, dev, world, sample_clocks=False):
+    fn = WORKLOADS[args.workload][0]
+    d, m = fn(lb, storage)
+    d.device = dev
+    lat = lb.Lattice(d, m)
+    lat.step(args.warmup if args.warmup > 0 else 1)   # includes the block-width autotune
+    lat.sync()
+    torch.cuda.synchronize(dev)
+    barrier(torch, world)
+    sampler = ClockSampler(gpu_id_for_smi(torch, dev)) if sample_clocks else None
+    if sampler:
+        time.sleep(0.3)
+    elapsed = timed_steps(torch, lat, args.steps, dev)
+    clocks = sampler.stop() if sampler else None
+    torch.cuda.synchronize(dev)
+    barrier(torch, world)
+    elapsed_max = reduce_max(torch, elapsed, dev, world)
+    return d, lat, elapsed_max, clocks
+
+
+def e2e_measure(torch, lb, args, storage, dev, world):
+    """Through the public API with host buffers: pinned H2D of the start populations, K steps,
+    D2H of the macroscopic fields, all inside the timed region."""
+    fn = WORKLOADS[args.workload][0]
+    d, m = fn(lb, storage)
+    d.device = dev
+    lat = lb.Lattice(d, m)
+    N, Q = d.cells, d.q
+    _, _, _, w, _ = lb.velocities(d.lattice)
+    F_host = torch.empty(N * Q, dtype=torch.float32, pin_memory=True)
+    F_host.view(Q, N).copy_(torch.tensor(w, dtype=torch.float32)[:, None].expand(Q, N))
+    rho_host = torch.empty(N, dtype=torch.float32, pin_memory=True)
+    u_host = torch.empty(d.dim * N, dtype=torch.float32, pin_memory=True)
+    lat.step(2)  # autotune + graph build outside the timed region
+    lat.sync()
+    torch.cuda.synchronize(dev)
+    barrier(torch, world)
+    s = torch.cuda.ExternalStream(lat.stream(), device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    lat.set_populations(F_host)
+    lat.step(args.steps)
+    lat.macros_into(rho_host, u_host)
+    e1.record(s)
+    e1.synchronize()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    elapsed = reduce_max(torch, elapsed, dev, world)
+    h2d = N * Q * 4
+    d2h = N * (1 + d.dim) * 4
+    lat.close()
+    return {"value": world * N * args.steps / elapsed / 1e6, "unit": "MLUPS",
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+            "api": "lbm_set_populations (pinned host F32) + lbm_step(K) + lbm_get_macros (pinned host F32)"}
+
+
+def accuracy(lb, args):
+    """rel. L2 velocity error of FP32 and FP16-shifted storage against the FP64 run of the same
+    kernel, on a 64^3 lattice of the default workload after 1000 steps (64^3 lid with the same rates)."""
+    if not args.workload.startswith("d3q27_mrt"):
+        return None
+    res = {}
+    runs = {}
+    for st in (lb.F64, lb.F32, lb.F16S):
+        d, m = wl_mrt256(lb, st, 64)
+        with lb.Lattice(d, m) as lat:
+            lat.step(1000)
+            rho, u = lat.macros()
+        runs[st] = (rho, u, m)
+    rho64, u64, m = runs[lb.F64]
+    fluid = np.tile(m != 1, 3)
+    for st, name in ((lb.F32, "f32"), (lb.F16S, "f16s")):
+        rho, u, _ = runs[st]
+        res[f"rel_l2_u_{name}_vs_f64"] = float(np.linalg.norm(u[fluid] - u64[fluid]) / np.linalg.norm(u64[fluid]))
+        res[f"rel_l2_rho_{name}_vs_f64"] = float(np.linalg.norm(rho[m != 1] - rho64[m != 1]) /
+                                                  np.linalg.norm(rho64[m != 1]))
+    res["lattice"] = "64^3 (same rates and lid), 1000 steps"
+    return res
+
+
+def barrier(torch, world):
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def reduce_max(torch, value, dev, world):
+    if world <= 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{dev}")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import lbm_b200 as lb
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    head_storage = {"f16s": lb.F16S, "f32": lb.F32, "bf16s": lb.BF16S, "f64": lb.F64}[args.storage]
+    peak, peak_kind = peaks()
+
+    d, lat, el, clocks = measure(torch, lb, args, head_storage, dev, world, sample_clocks=(rank == 0))
+    N = d.cells
+    launches_per_step = 2 if d.collision == 2 else 1
+    bytes_cell = algorithmic_bytes_per_cell(d)
+    value = world * N * args.steps / el / 1e6
+    avg_launch_s = el / (args.steps * launches_per_step)
+    achieved = bytes_cell * N / launches_per_step / avg_launch_s / 1e9
+    traffic = dram_traffic(args.workload, head_storage)
+    lat.close()
+    del lat
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if head_storage != lb.F64 else "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload][1],
+                   "lattice": list(d.shape), "cells": N, "storage": STORAGE_NAMES[head_storage],
+                   "bytes_per_cell_update": bytes_cell,
+                   "l2": f"inputs larger than L2: {N * d.q * storage_bytes(head_storage) / 1e9:.2f} GB per population buffer"
+                   if N * d.q * storage_bytes(head_storage) > 126e6 else "lattice is L2-resident (no flush)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                     if peak_kind == "measured" else "fallback 6.65 TB/s",
+                     "kernel": {0: "k_step_bgk", 1: "k_step_mrt", 2: "k_step_sc + k_sc_psi"}[d.collision],
+                     "bytes_per_launch": bytes_cell * N / launches_per_step},
+        "gpu_launches": args.steps * launches_per_step,
+        "clocks": clocks,
+    }
+    # FP32 plain beside the 16-bit headline
+    if head_storage != lb.F32 and not args.no_compare:
+        d32, lat32, el32, _ = measure(torch, lb, args, lb.F32, dev, world)
+        lat32.close()
+        del lat32
+        v32 = world * N * args.steps / el32 / 1e6
+        b32 = algorithmic_bytes_per_cell(d32)
+        a32 = b32 * N / launches_per_step / (el32 / (args.steps * launches_per_step)) / 1e9
+        out["fp32_plain"] = {"value": v32, "unit": "MLUPS", "ms_per_step": el32 * 1e3 / args.steps,
+                             "roofline": {"achieved": a32, "peak": peak, "frac": a32 / peak,
+                                          "traffic": dram_traffic(args.workload, lb.F32)}}
+        out[f"speedup_{STORAGE_NAMES[head_storage]}_vs_f32"] = value / v32
+    if not args.no_e2e:
+        out["e2e"] = e2e_measure(torch, lb, args, head_storage, dev, world)
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        acc = accuracy(lb, args)
+        if acc:
+            out["accuracy"] = acc
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        O.lib()
+        side = 64 if args.workload.startswith("d3q27") else None
+        mlups, cells, steps, shape = oracle_mlups(args.workload, args.cpu_seconds, side)
+        out["cpu_baseline"] = {"value": mlups, "unit": "MLUPS", "cores": threads(), "kind": "port",
+                               "sample": f"{'x'.join(map(str, shape))} lattice of the same workload, {steps} steps, "
+                                         f"FP32, {threads()} threads on {cpu_model()}"}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="d3q27_mrt_gs_lid_256", choices=sorted(WORKLOADS))
+    ap.add_argument("--storage", default="f16s", choices=["f16s", "f32", "bf16s", "f64"])
+    ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.warmup < 0 or args.steps < 1:
+        raise SystemExit("steps must be >= 1 and warmup >= 0")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    import torch
+
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device(f"cuda:{local_rank}"))
+    try:
+        out = run_ours(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

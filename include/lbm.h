@@ -1,0 +1,212 @@
+/*
+ * lbm.h — C ABI of the B200-native Lattice Boltzmann engine (liblbm_b200.so).
+ *
+ * One lbm_step() call advances the populations by whole time steps with one fused
+ * sm_100a kernel per step (pull streaming + BGK/MRT/Shan-Chen collision + cell-class
+ * boundary handling).  It replaces the body of the reference's time loop: everything from
+ *   F_streamed = F(nb_index)            (cpp/d2q9_bgk_lid.cpp:124)
+ * to
+ *   F(REFLECTED) = BOUNCEDBACK           (cpp/d2q9_bgk_lid.cpp:155)
+ * and the same span in cpp/d2q9_bgk_channel_packed.cpp:54-74, cpp/d3q27_bgk_lid.cpp:160-195,
+ * rust/examples/d2q9_bgk_lid.rs:153-191 and rust/examples/d3q27_mrt_lid.rs:304-389.
+ *
+ * Conventions kept from the reference:
+ *  - population layout: column-major [nx, ny(, nz), Q], i.e. F[x + nx*(y + ny*(z + nz*i))]
+ *    (moddims(range(N*Q), nx, ny, 9) at cpp/d2q9_bgk_lid.cpp:86);
+ *  - velocity ordering and weights: D2Q9 cpp/d2q9_bgk_lid.cpp:72-79, D3Q27 cpp/d3q27_bgk_lid.cpp:98-107;
+ *  - opposite-direction map: cpp/d2q9_bgk_lid.cpp:82, cpp/d3q27_bgk_lid.cpp:111;
+ *  - periodic wrap of the pull gather (af::shift semantics, out[x] = in[x - c]);
+ *  - full-way bounce-back: a solid cell stores the reversed streamed populations after the
+ *    collision (cpp/d2q9_bgk_lid.cpp:97-98,126,155);
+ *  - boundary conditions as overwrites of rho/u before the equilibrium (cpp/d2q9_bgk_lid.cpp:141-146).
+ *
+ * Errors: every int-returning call returns LBM_OK (0) or a negative LBM_ERR_* code; no C++
+ * exception crosses this boundary (the reference's catch(af::exception) at cpp/d2q9_bgk_lid.cpp:219).
+ * lbm_last_error() gives a message for the last failing call on the calling thread.
+ * Threading: one context per host thread at a time; calls on one context are not thread-safe.
+ * Ownership: the context owns its device buffers; host pointers are borrowed for the call only.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define LBM_OK               0
+#define LBM_ERR_INVALID    (-1)  /* bad argument or descriptor field */
+#define LBM_ERR_CUDA       (-2)  /* a CUDA runtime call failed */
+#define LBM_ERR_NOMEM      (-3)  /* device or host allocation failed */
+#define LBM_ERR_DIVERGED   (-4)  /* NaN/Inf found in the populations */
+#define LBM_ERR_UNSUPPORTED (-5) /* combination not built (e.g. MRT on D2Q9) */
+#define LBM_ERR_NO_DEVICE  (-6)  /* no CUDA device / not an sm_100 device */
+#define LBM_ERR_STATE      (-7)  /* call not valid in the current state */
+
+/* ---- enumerations ---------------------------------------------------------------------- */
+enum lbm_lattice   { LBM_D2Q9 = 0, LBM_D3Q27 = 1 };
+enum lbm_collision { LBM_BGK = 0, LBM_MRT = 1, LBM_SHANCHEN = 2 };
+/* Storage of the populations in HBM.  Arithmetic is FP32 for F32/F16S/BF16S and FP64 for F64.
+ * F16S / BF16S hold the shifted population (f_i - w_i) * storage_scale in 16 bits.            */
+enum lbm_storage   { LBM_F32 = 0, LBM_F16S = 1, LBM_BF16S = 2, LBM_F64 = 3 };
+/* MRT moment basis.  REF: the raw-monomial 27x27 matrix of rust/examples/d3q27_mrt_lid.rs:167-193
+ * with its equilibrium-moment table (:357-383).  GRAM_SCHMIDT: the same rows orthogonalised in order
+ * (unweighted inner product over the 27 velocities), equilibrium moments = M * feq(rho,u).       */
+enum lbm_mrt_basis { LBM_MRT_REF = 0, LBM_MRT_GRAM_SCHMIDT = 1 };
+/* Host buffer element type for population / field transfers. */
+enum lbm_dtype     { LBM_DTYPE_F32 = 0, LBM_DTYPE_F64 = 1 };
+/* Where a transfer buffer lives. */
+enum lbm_memory    { LBM_HOST = 0, LBM_DEVICE = 1 };
+
+/* ---- cell classes ------------------------------------------------------------------------
+ * The mask holds one uint8 class id per cell (column-major like the populations).  Each class
+ * states what happens to a cell of that class in every step.  Class 0 is plain fluid unless
+ * the descriptor redefines it.  The flags reproduce the reference's boundary overwrites:
+ *   solid (ON list):   BOUNCE|SET_RHO|SET_UX|SET_UY|SET_UZ with rho=u=0  (cpp/d2q9_bgk_lid.cpp:144-146,155)
+ *   lid row:           SET_UX|SET_UY(|SET_UZ) with the lid velocity   (cpp/d2q9_bgk_lid.cpp:141-142)
+ *   channel inlet:     SET_UX|SET_RHO, rho=1                          (cpp/d2q9_bgk_channel_packed.cpp:64,68)
+ *   channel outlet:    SET_RHO, rho=1                                 (cpp/d2q9_bgk_channel_packed.cpp:69)     */
+#define LBM_MAX_CLASSES 16
+#define LBM_CELL_BOUNCE       0x01u /* store reversed streamed populations (i>=1) after collision  */
+#define LBM_CELL_SET_RHO      0x02u /* overwrite rho with class rho before the equilibrium         */
+#define LBM_CELL_SET_UX       0x04u /* overwrite u_x                                                */
+#define LBM_CELL_SET_UY       0x08u /* overwrite u_y                                                */
+#define LBM_CELL_SET_UZ       0x10u /* overwrite u_z (D3Q27)                                        */
+#define LBM_CELL_EQUILIBRIUM  0x20u /* write feq(rho,u) for every direction (Dirichlet equilibrium) */
+#define LBM_CELL_ZEROGRAD_XP  0x40u /* outlet on the x = nx-1 face: populations arriving from +x are
+                                       copied from the streamed state of cell x-1 (zero gradient)  */
+
+typedef struct lbm_cell_class {
+    uint32_t flags;
+    uint32_t reserved;      /* 0 */
+    double rho, ux, uy, uz; /* used in FP64 by F64 storage, rounded to FP32 otherwise */
+} lbm_cell_class;
+
+/* ---- lattice descriptor ------------------------------------------------------------------ */
+typedef struct lbm_desc {
+    int32_t lattice;        /* enum lbm_lattice                                               */
+    int32_t collision;      /* enum lbm_collision                                             */
+    int32_t storage;        /* enum lbm_storage                                               */
+    int32_t mrt_basis;      /* enum lbm_mrt_basis (MRT only)                                  */
+    int64_t nx, ny, nz;     /* nz = 1 for D2Q9                                                */
+    double omega;           /* BGK / Shan-Chen relaxation 1/tau                               */
+    double mrt_s[27];       /* MRT relaxation rate per moment row (rust/examples/d3q27_mrt_lid.rs:122-150) */
+    double sc_G;            /* Shan-Chen interaction strength; psi = 1 - exp(-rho)            */
+    double storage_scale;   /* F16S/BF16S: stored = (f - w) * scale; 0 selects the default    */
+    int32_t n_classes;      /* entries used in classes[] (>= 1)                               */
+    int32_t device;         /* CUDA device ordinal                                            */
+    lbm_cell_class classes[LBM_MAX_CLASSES];
+    const uint8_t* mask;    /* host, N class ids column-major; NULL = every cell class 0      */
+} lbm_desc;
+
+typedef struct lbm_ctx lbm_ctx;
+typedef struct lbm_batch lbm_batch;
+
+/* ---- library --------------------------------------------------------------------------- */
+int         lbm_abi_version(void);
+const char* lbm_strerror(int status);
+const char* lbm_last_error(void);
+/* Fill a descriptor with defaults: fluid class 0, omega 1, MRT rates 1, device 0. */
+void        lbm_desc_init(lbm_desc* d, int lattice, int collision, int storage,
+                          int64_t nx, int64_t ny, int64_t nz);
+int         lbm_q(int lattice);                          /* 9 or 27 */
+/* Velocity set and weights exactly as the reference lists them (a1 of the path). */
+int         lbm_velocities(int lattice, int32_t* cx, int32_t* cy, int32_t* cz, double* w, int32_t* opp);
+
+/* ---- single lattice ---------------------------------------------------------------------
+ * lbm_create: validates the descriptor, allocates two population buffers (ping-pong) plus the mask
+ * on the device, and sets every population to feq(rho=1, u=0) of each cell's class values.       */
+int  lbm_create(const lbm_desc* d, lbm_ctx** out);
+void lbm_destroy(lbm_ctx* c);
+/* Populations in the reference layout [nx,ny(,nz),Q].  src/dst: host or device pointer. */
+int  lbm_set_populations(lbm_ctx* c, const void* src, int dtype, int memory);
+int  lbm_get_populations(lbm_ctx* c, void* dst, int dtype, int memory);
+/* F = feq(rho, u) per cell, the reference's start state (cpp/d2q9_bgk_lid.cpp:100-107).
+ * rho: N doubles or NULL (=1); u: dim*N doubles [ux | uy (| uz)] or NULL (=0).  Host pointers. */
+int  lbm_init_equilibrium(lbm_ctx* c, const double* rho, const double* u);
+/* Advance nsteps time steps, asynchronously on the context stream. */
+int  lbm_step(lbm_ctx* c, int64_t nsteps);
+int  lbm_sync(lbm_ctx* c);
+/* Macroscopic fields the last step's collision used, after the class overwrites (the reference's
+ * DENSITY / UX / UY / UZ after an iteration).  Before any step: moments of the current populations.
+ * rho: N values; u: dim*N values [ux | uy (| uz)]. Either may be NULL.                            */
+int  lbm_get_macros(lbm_ctx* c, void* rho, void* u, int dtype, int memory);
+/* FP64 sums over all cells of the current populations: out[0] = mass, out[1..3] = momentum.
+ * Returns LBM_ERR_DIVERGED when a population is NaN or Inf.                                       */
+int  lbm_sums_fp64(lbm_ctx* c, double out[4]);
+/* Steady-state residual in FP64: sqrt(sum |u_t - u_{t-1}|^2 / sum |u_t|^2) over class-0 cells. */
+int  lbm_residual_fp64(lbm_ctx* c, double* out);
+/* Device time of the most recent lbm_step call in milliseconds (CUDA events on the context stream). */
+int  lbm_last_step_ms(lbm_ctx* c, float* ms);
+int64_t lbm_steps_done(const lbm_ctx* c);
+/* The context's CUDA stream (cudaStream_t) and device buffers, for callers that interoperate. */
+void* lbm_stream(lbm_ctx* c);
+int   lbm_set_stream(lbm_ctx* c, void* stream);          /* NULL restores the context's own */
+/* Current population buffer on the device (storage type of the descriptor) and its byte size. */
+void* lbm_device_populations(lbm_ctx* c, size_t* bytes);
+int   lbm_get_desc(const lbm_ctx* c, lbm_desc* out);
+/* Block width (threads along x) used by the step kernel; 0 = autotune on first step. */
+int   lbm_set_block(lbm_ctx* c, int threads_x);
+int   lbm_get_block(const lbm_ctx* c);
+
+/* ---- batched ensemble -------------------------------------------------------------------
+ * Many independent lattices (any mix of D2Q9/D3Q27 BGK, sizes and rates, one storage type)
+ * advanced by one kernel launch per step over a tile table; nsteps of those are captured in a
+ * CUDA graph and replayed.                                                                      */
+int  lbm_batch_create(const lbm_desc* descs, int n, lbm_batch** out);
+void lbm_batch_destroy(lbm_batch* b);
+int  lbm_batch_size(const lbm_batch* b);
+int  lbm_batch_step(lbm_batch* b, int64_t nsteps);
+int  lbm_batch_sync(lbm_batch* b);
+int  lbm_batch_get_populations(lbm_batch* b, int k, void* dst, int dtype, int memory);
+int  lbm_batch_set_populations(lbm_batch* b, int k, const void* src, int dtype, int memory);
+int  lbm_batch_get_macros(lbm_batch* b, int k, void* rho, void* u, int dtype, int memory);
+int  lbm_batch_sums_fp64(lbm_batch* b, int k, double out[4]);
+int64_t lbm_batch_cells(const lbm_batch* b);
+void* lbm_batch_stream(lbm_batch* b);
+/* Tile shape chosen by the autotuner (cells per tile along x, tiles launched per step). */
+int  lbm_batch_tile_info(const lbm_batch* b, int* tile_x, int64_t* n_tiles);
+
+/* ---- problem set-up helpers (the reference's loop-invariant state, layer L3) --------------
+ * Each fills mask[N] (column-major) and the descriptor's class table so that the per-cell
+ * behaviour equals the reference driver's sequence of overwrites.                              */
+/* D2Q9 lid-driven cavity: solid x=0, x=nx-1, y=0; lid row y=ny-1, x=1..nx-2 (cpp/d2q9_bgk_lid.cpp:64,90-91,141-146). */
+int lbm_setup_cavity2d(lbm_desc* d, uint8_t* mask, double u_lid);
+/* D3Q27 lid-driven cavity: fluid x=1..nx-2, y=1..ny-2, z=1..nz-1; lid plane z=nz-1 (cpp/d3q27_bgk_lid.cpp:119-120,179-186). */
+int lbm_setup_cavity3d(lbm_desc* d, uint8_t* mask, double u_lid);
+/* D2Q9 channel: solid circle (x-ox)^2+(y-oy)^2 <= r^2 and rows y=0, y=ny-1.  config_mode = 0 gives the
+ * reference's equilibrium forcing (inlet u_x + rho=1 at x=0, rho=1 at x=nx-1, periodic in x;
+ * cpp/d2q9_bgk_channel_packed.cpp:37-39,64-69).  config_mode = 1 gives an equilibrium inlet
+ * (rho=1, u=(u_in,0)) and a zero-gradient outlet.                                               */
+int lbm_setup_channel2d(lbm_desc* d, uint8_t* mask, double u_in, double ox, double oy, double r,
+                        int config_mode);
+/* D3Q27 duct: walls y=0, y=ny-1, z=0, z=nz-1, solid sphere centre (ox,oy,oz) radius r,
+ * equilibrium inlet at x=0, zero-gradient outlet at x=nx-1.                                      */
+int lbm_setup_duct3d(lbm_desc* d, uint8_t* mask, double u_in, double ox, double oy, double oz,
+                     double r);
+/* Index-list shim: accept the reference's solid-node list ON = where(BOUND) (linear column-major
+ * indices, cpp/d2q9_bgk_lid.cpp:94) and mark those cells with class `cls`.                      */
+int lbm_mask_from_index_list(uint8_t* mask, int64_t n_cells, const int64_t* on, int64_t n_on,
+                             uint8_t cls);
+/* Reference-driver relaxation rules: tau = 3 nu + 1/2, omega = 1/tau with
+ *   rule 0: nu = u * L / Re        (C++ drivers, cpp/d2q9_bgk_lid.cpp:45)
+ *   rule 1: nu = u * 2 * L / Re    (Rust drivers, rust/examples/d2q9_bgk_lid.rs:52)            */
+double lbm_omega_from_re(double u, double L, double re, int rule);
+/* MRT rate vector of the reference (s0=s1=1.3, sv=1.1, sb=0.9, ...; rust/examples/d3q27_mrt_lid.rs:111-150). */
+void lbm_mrt_reference_rates(double s[27]);
+/* MRT rates with shear rate sv for rows 4-6,8,9 and `other` for every other row. */
+void lbm_mrt_rates(double s[27], double sv, double other);
+/* One host-side MRT collision of a single cell (FP64): f_out = M^-1 (m - S (m - meq(rho,u))), m = M f_in.
+ * Used for the reference's MRT start state (rust/examples/d3q27_mrt_lid.rs:228-287).             */
+int lbm_mrt_collide_host(const lbm_desc* d, const double f_in[27], double rho, const double u[3],
+                         double f_out[27]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM_B200_H */

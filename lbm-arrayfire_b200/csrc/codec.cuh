@@ -1,0 +1,61 @@
+// codec.cuh — how one population is held in HBM.
+//
+//   F32   : the population itself (the reference's f32 arrays)
+//   F64   : the population itself in double; the FP64 run of the same kernel
+//   F16S  : half((f_i - w_i) * scale)            "shifted" storage, FP32 arithmetic
+//   BF16S : bfloat16((f_i - w_i) * scale)
+// Shifting by the rest weight keeps only the deviation from rest in the 16-bit word; `scale`
+// (a power of two) lifts the small deviations out of the FP16 subnormal range.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cstdint>
+
+namespace lbm {
+
+template <class S>
+struct Codec;
+
+template <>
+struct Codec<float> {
+    using Real = float;
+    static constexpr int kBytes = 4;
+    __device__ __forceinline__ static float load(const float* p, float, float) { return __ldg(p); }
+    __device__ __forceinline__ static void store(float* p, float v, float, float) { *p = v; }
+};
+
+template <>
+struct Codec<double> {
+    using Real = double;
+    static constexpr int kBytes = 8;
+    __device__ __forceinline__ static double load(const double* p, double, double) { return __ldg(p); }
+    __device__ __forceinline__ static void store(double* p, double v, double, double) { *p = v; }
+};
+
+template <>
+struct Codec<__half> {
+    using Real = float;
+    static constexpr int kBytes = 2;
+    __device__ __forceinline__ static float load(const __half* p, float w, float inv_scale) {
+        return fmaf(__half2float(__ldg(p)), inv_scale, w);
+    }
+    __device__ __forceinline__ static void store(__half* p, float v, float w, float scale) {
+        *p = __float2half_rn((v - w) * scale);
+    }
+};
+
+template <>
+struct Codec<__nv_bfloat16> {
+    using Real = float;
+    static constexpr int kBytes = 2;
+    __device__ __forceinline__ static float load(const __nv_bfloat16* p, float w, float inv_scale) {
+        return fmaf(__bfloat162float(__ldg(p)), inv_scale, w);
+    }
+    __device__ __forceinline__ static void store(__nv_bfloat16* p, float v, float w, float scale) {
+        *p = __float2bfloat16_rn((v - w) * scale);
+    }
+};
+
+}  // namespace lbm

@@ -1,0 +1,514 @@
+// kernels.cuh — the fused per-time-step kernels.
+//
+// One thread owns one cell.  Per step it
+//   1. pulls Q populations from the previous buffer (periodic wrap: af::shift semantics,
+//      cpp/d2q9_bgk_lid.cpp:18-28,124) — Q coalesced loads along x, one HBM read each;
+//   2. forms rho and u (cpp/d2q9_bgk_lid.cpp:131-138), applies its cell class (the reference's
+//      boundary overwrites, :141-146) and collides (BGK :149-153 / MRT / Shan-Chen);
+//   3. applies full-way bounce-back for solid classes (:126,155) and writes Q populations.
+// HBM traffic per cell and step: Q loads + Q stores of the storage type (+1 mask byte).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "codec.cuh"
+#include "lattice.cuh"
+#include "mrt.cuh"
+
+namespace lbm {
+
+constexpr uint32_t kBounce = 0x01u, kSetRho = 0x02u, kSetUx = 0x04u, kSetUy = 0x08u, kSetUz = 0x10u,
+                   kEquilibrium = 0x20u, kZeroGradXp = 0x40u;
+constexpr int kMaxClasses = 16;
+
+template <class R>
+struct ClassTable {
+    uint32_t flags[kMaxClasses];
+    R rho[kMaxClasses], ux[kMaxClasses], uy[kMaxClasses], uz[kMaxClasses];
+};
+
+template <class R>
+struct StepParams {
+    const void* fin;
+    void* fout;
+    const uint8_t* mask;  // nullptr: every cell is class 0
+    int nx, ny, nz;
+    long long N;          // cells
+    R omega, one_m_omega;
+    R scale, inv_scale;   // 16-bit storage codec
+    R G;                  // Shan-Chen strength
+    R* psi;               // Shan-Chen psi field (N)
+    R* rho_out;           // macro kernel outputs
+    R* u_out;
+    ClassTable<R> cls;
+    MrtCoef<R> mrt;
+};
+
+// Row base offsets of the 3 (D2Q9) or 9 (D3Q27) neighbour rows of (y, z), wrap included.
+template <class L>
+struct Rows {
+    long long base[3][3];  // [dy+1][dz+1]
+    __device__ __forceinline__ Rows(int y, int z, int nx, int ny, int nz) {
+        const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
+        const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+                base[a][b] = ((long long)zs[b] * ny + ys[a]) * (long long)nx;
+    }
+    // source row of direction (cy, cz): pull from y - cy, z - cz
+    __device__ __forceinline__ long long src(int cy, int cz) const { return base[1 - cy][1 - cz]; }
+};
+
+// Pull gather of one cell.  x-wrap per thread; xs for c_x = +1 is x-1, for c_x = -1 it is x+1.
+template <class L, class S, class P, class R>
+__device__ __forceinline__ void pull(const S* __restrict__ fin, const P& p, const Rows<L>& rows, int x,
+                                     R (&fs)[L::Q]) {
+    const int xm = x == 0 ? p.nx - 1 : x - 1;
+    const int xp = x == p.nx - 1 ? 0 : x + 1;
+    static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
+        const int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
+        const long long idx = (long long)i * p.N + rows.src(cy, cz) + xs;
+        fs[i] = Codec<S>::load(fin + idx, R(L::w(i)), p.inv_scale);
+    });
+}
+
+// Zero-gradient outlet: populations arriving from +x are taken from cell x-1's streamed state,
+// i.e. F_i(x - 1 - c_i) = F_i(x, y - cy, z - cz) for c_x = -1.
+template <class L, class S, class P, class R>
+__device__ __forceinline__ void pull_zerograd(const S* __restrict__ fin, const P& p, const Rows<L>& rows, int x,
+                                              R (&fs)[L::Q]) {
+    static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        if constexpr (L::cx(i) == -1) {
+            const long long idx = (long long)i * p.N + rows.src(L::cy(i), L::cz(i)) + x;
+            fs[i] = Codec<S>::load(fin + idx, R(L::w(i)), p.inv_scale);
+        }
+    });
+}
+
+template <class L, class R>
+__device__ __forceinline__ void moments(const R (&fs)[L::Q], R& rho, R& ux, R& uy, R& uz) {
+    R r = R(0), jx = R(0), jy = R(0), jz = R(0);
+    static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        r += fs[i];
+        if constexpr (L::cx(i) == 1) jx += fs[i];
+        if constexpr (L::cx(i) == -1) jx -= fs[i];
+        if constexpr (L::cy(i) == 1) jy += fs[i];
+        if constexpr (L::cy(i) == -1) jy -= fs[i];
+        if constexpr (L::cz(i) == 1) jz += fs[i];
+        if constexpr (L::cz(i) == -1) jz -= fs[i];
+    });
+    rho = r;
+    ux = jx / r;
+    uy = jy / r;
+    uz = L::DIM == 3 ? jz / r : R(0);
+}
+
+template <class T, class R>
+__device__ __forceinline__ void apply_class(const ClassTable<T>& ct, int cls, uint32_t fl, R& rho, R& ux,
+                                            R& uy, R& uz, int dim) {
+    if (fl & kSetRho) rho = R(ct.rho[cls]);
+    if (fl & kSetUx) ux = R(ct.ux[cls]);
+    if (fl & kSetUy) uy = R(ct.uy[cls]);
+    if ((fl & kSetUz) && dim == 3) uz = R(ct.uz[cls]);
+}
+
+// feq_i = w_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2)   (cpp/d2q9_bgk_lid.cpp:151)
+template <class L, int I, class R>
+__device__ __forceinline__ R feq_i(R wrho, R base, R ux, R uy, R uz) {
+    constexpr int cx = L::cx(I), cy = L::cy(I), cz = L::cz(I);
+    R eu = R(0);
+    if constexpr (cx == 1) eu = eu + ux;
+    if constexpr (cx == -1) eu = eu - ux;
+    if constexpr (cy == 1) eu = eu + uy;
+    if constexpr (cy == -1) eu = eu - uy;
+    if constexpr (cz == 1) eu = eu + uz;
+    if constexpr (cz == -1) eu = eu - uz;
+    return wrho * (base + eu * (R(3) + R(4.5) * eu));
+}
+
+template <class L, class R>
+__device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R (&feq)[L::Q]) {
+    const R base = R(1) - R(1.5) * (ux * ux + uy * uy + uz * uz);
+    static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        feq[i] = feq_i<L, i>(R(L::w(i)) * rho, base, ux, uy, uz);
+    });
+}
+
+template <class L, class S, class P, class R>
+__device__ __forceinline__ void store_cell(S* __restrict__ fout, const P& p, long long c, const R (&out)[L::Q]) {
+    static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        Codec<S>::store(fout + (long long)i * p.N + c, out[i], R(L::w(i)), p.scale);
+    });
+}
+
+template <class T>
+__device__ __forceinline__ void cell_class(const uint8_t* __restrict__ mask, const ClassTable<T>& ct,
+                                           long long c, int& cls, uint32_t& fl) {
+    cls = mask ? (int)__ldg(mask + c) : 0;
+    fl = ct.flags[cls];
+}
+
+// ---- BGK ---------------------------------------------------------------------------------
+// One cell of a BGK step.  P supplies mask, cls, nx, ny, nz, N, omega, one_m_omega, scale and
+// inv_scale (StepParams for one lattice, BatchLattice for one member of an ensemble).
+template <class L, class S, class P>
+__device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, S* __restrict__ fout, int x, int y,
+                                         int z) {
+    using R = typename Codec<S>::Real;
+    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
+    const long long c = rows.base[1][1] + x;
+    R fs[L::Q];
+    pull<L, S>(fin, p, rows, x, fs);
+    int cls;
+    uint32_t fl;
+    cell_class(p.mask, p.cls, c, cls, fl);
+    if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
+    R rho, ux, uy, uz;
+    moments<L, R>(fs, rho, ux, uy, uz);
+    if (fl) apply_class(p.cls, cls, fl, rho, ux, uy, uz, L::DIM);
+    R out[L::Q];
+    const R base = R(1) - R(1.5) * (ux * ux + uy * uy + uz * uz);
+    const R omega = R(p.omega), one_m = R(p.one_m_omega);
+    static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        const R fe = feq_i<L, i>(R(L::w(i)) * rho, base, ux, uy, uz);
+        out[i] = (fl & kEquilibrium) ? fe : omega * fe + one_m * fs[i];
+    });
+    if (fl & kBounce) {
+        static_for<L::Q - 1>([&](auto I) {
+            constexpr int i = I + 1;
+            out[L::opp(i)] = fs[i];
+        });
+    }
+    store_cell<L, S>(fout, p, c, out);
+}
+
+template <class L, class S>
+__global__ void __launch_bounds__(512) k_step_bgk(StepParams<typename Codec<S>::Real> p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= p.nx) return;
+    bgk_cell<L, S>(p, static_cast<const S*>(p.fin), static_cast<S*>(p.fout), x, blockIdx.y, blockIdx.z);
+}
+
+// ---- MRT (D3Q27) -------------------------------------------------------------------------
+template <int BASIS, class S>
+__global__ void __launch_bounds__(256) k_step_mrt(StepParams<typename Codec<S>::Real> p) {
+    using L = D3Q27;
+    using R = typename Codec<S>::Real;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= p.nx) return;
+    const int y = blockIdx.y, z = blockIdx.z;
+    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
+    const long long c = rows.base[1][1] + x;
+    const S* __restrict__ fin = static_cast<const S*>(p.fin);
+    R fs[27];
+    pull<L, S>(fin, p, rows, x, fs);
+    int cls;
+    uint32_t fl;
+    cell_class(p.mask, p.cls, c, cls, fl);
+    if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
+    // populations -> tensor slots (a register renaming)
+    R T[27];
+    static_for<27>([&](auto I) {
+        constexpr int i = I;
+        T[L::slot(i)] = fs[i];
+    });
+    mrt_forward<BASIS>(T);
+    R rho = T[0];
+    const R inv = R(1) / rho;
+    R ux = T[1] * inv, uy = T[3] * inv, uz = T[9] * inv;
+    if (fl) apply_class(p.cls, cls, fl, rho, ux, uy, uz, 3);
+    R q[11];
+    q[0] = rho;
+    q[1] = rho * ux;
+    q[2] = rho * uy;
+    q[3] = rho * uz;
+    q[4] = q[1] * ux;
+    q[5] = q[2] * uy;
+    q[6] = q[3] * uz;
+    q[7] = q[1] * uy;
+    q[8] = q[1] * uz;
+    q[9] = q[2] * uz;
+    q[10] = ux * ux + uy * uy + uz * uz;
+    mrt_relax<BASIS>(T, q, p.mrt);
+    mrt_inverse<BASIS>(T);
+    R out[27];
+    static_for<27>([&](auto I) {
+        constexpr int i = I;
+        out[i] = T[L::slot(i)];
+    });
+    if (fl & (kEquilibrium | kBounce)) {
+        if (fl & kEquilibrium) equilibrium<L, R>(rho, ux, uy, uz, out);
+        if (fl & kBounce) {
+            // reload the streamed populations (the transform overwrote them in place)
+            pull<L, S>(fin, p, rows, x, fs);
+            if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
+            static_for<26>([&](auto I) {
+                constexpr int i = I + 1;
+                out[L::opp(i)] = fs[i];
+            });
+        }
+    }
+    store_cell<L, S>(static_cast<S*>(p.fout), p, c, out);
+}
+
+// ---- Shan-Chen (D2Q9) --------------------------------------------------------------------
+// Pass 1: psi = 1 - exp(-rho) of the streamed density of every cell.
+template <class S>
+__global__ void __launch_bounds__(512) k_sc_psi(StepParams<typename Codec<S>::Real> p) {
+    using L = D2Q9;
+    using R = typename Codec<S>::Real;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= p.nx) return;
+    const int y = blockIdx.y, z = blockIdx.z;
+    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
+    const long long c = rows.base[1][1] + x;
+    const S* __restrict__ fin = static_cast<const S*>(p.fin);
+    R fs[9];
+    pull<L, S>(fin, p, rows, x, fs);
+    int cls;
+    uint32_t fl;
+    cell_class(p.mask, p.cls, c, cls, fl);
+    if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
+    R rho = R(0);
+    static_for<9>([&](auto I) { rho += fs[I]; });
+    if (fl & kSetRho) rho = R(p.cls.rho[cls]);
+    p.psi[c] = R(1) - exp(-rho);
+}
+
+// Shan-Chen force F = -G psi(x) sum_i w_i psi(x + c_i) c_i at cell (x, y) (periodic).
+template <class R>
+__device__ __forceinline__ void sc_force(const StepParams<R>& p, const Rows<D2Q9>& rows, int x,
+                                         long long c, R& Fx, R& Fy) {
+    using L = D2Q9;
+    const int xm = x == 0 ? p.nx - 1 : x - 1;
+    const int xp = x == p.nx - 1 ? 0 : x + 1;
+    R sx = R(0), sy = R(0);
+    static_for<8>([&](auto I) {
+        constexpr int i = I + 1;
+        constexpr int cx = L::cx(i), cy = L::cy(i);
+        // neighbour x + c_i: the source row of the opposite direction
+        const int xn = cx == 1 ? xp : (cx == -1 ? xm : x);
+        const R v = R(L::w(i)) * __ldg(p.psi + rows.src(-cy, 0) + xn);
+        if constexpr (cx == 1) sx += v;
+        if constexpr (cx == -1) sx -= v;
+        if constexpr (cy == 1) sy += v;
+        if constexpr (cy == -1) sy -= v;
+    });
+    const R g = -p.G * __ldg(p.psi + c);
+    Fx = g * sx;
+    Fy = g * sy;
+}
+
+template <class S>
+__global__ void __launch_bounds__(512) k_step_sc(StepParams<typename Codec<S>::Real> p) {
+    using L = D2Q9;
+    using R = typename Codec<S>::Real;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= p.nx) return;
+    const int y = blockIdx.y, z = blockIdx.z;
+    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
+    const long long c = rows.base[1][1] + x;
+    const S* __restrict__ fin = static_cast<const S*>(p.fin);
+    R fs[9];
+    pull<L, S>(fin, p, rows, x, fs);
+    int cls;
+    uint32_t fl;
+    cell_class(p.mask, p.cls, c, cls, fl);
+    if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
+    R rho, ux, uy, uz;
+    moments<L, R>(fs, rho, ux, uy, uz);
+    if (fl) apply_class(p.cls, cls, fl, rho, ux, uy, uz, 2);
+    R Fx, Fy;
+    sc_force(p, rows, x, c, Fx, Fy);
+    R vx = ux, vy = uy;
+    if (rho > R(0)) {
+        const R k = R(1) / (p.omega * rho);
+        vx = ux + Fx * k;
+        vy = uy + Fy * k;
+    }
+    R out[9];
+    const R base = R(1) - R(1.5) * (vx * vx + vy * vy);
+    static_for<9>([&](auto I) {
+        constexpr int i = I;
+        const R fe = feq_i<L, i>(R(L::w(i)) * rho, base, vx, vy, R(0));
+        out[i] = (fl & kEquilibrium) ? fe : p.omega * fe + p.one_m_omega * fs[i];
+    });
+    if (fl & kBounce) {
+        static_for<8>([&](auto I) {
+            constexpr int i = I + 1;
+            out[L::opp(i)] = fs[i];
+        });
+    }
+    store_cell<L, S>(static_cast<S*>(p.fout), p, c, out);
+}
+
+// ---- macroscopic fields ------------------------------------------------------------------
+// pulled = 1: the fields the last step's collision used (pull from the previous buffer, class
+// overwrites, Shan-Chen velocity u + F/(2 rho)).  pulled = 0: local moments of p.fin.
+template <class L, class S, class O>
+__global__ void k_macros(StepParams<typename Codec<S>::Real> p, int pulled, int collision, O* rho_out,
+                         O* u_out) {
+    using R = typename Codec<S>::Real;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= p.nx) return;
+    const int y = blockIdx.y, z = blockIdx.z;
+    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
+    const long long c = rows.base[1][1] + x;
+    const S* __restrict__ fin = static_cast<const S*>(p.fin);
+    R fs[L::Q];
+    int cls;
+    uint32_t fl;
+    cell_class(p.mask, p.cls, c, cls, fl);
+    if (pulled) {
+        pull<L, S>(fin, p, rows, x, fs);
+        if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
+    } else {
+        static_for<L::Q>([&](auto I) {
+            constexpr int i = I;
+            fs[i] = Codec<S>::load(fin + (long long)i * p.N + c, R(L::w(i)), p.inv_scale);
+        });
+    }
+    R rho, ux, uy, uz;
+    moments<L, R>(fs, rho, ux, uy, uz);
+    if (pulled && fl) apply_class(p.cls, cls, fl, rho, ux, uy, uz, L::DIM);
+    if constexpr (L::DIM == 2) {
+        if (pulled && collision == 2) {
+            R Fx, Fy;
+            sc_force(p, rows, x, c, Fx, Fy);
+            if (rho > R(0)) {
+                ux = ux + Fx / (R(2) * rho);
+                uy = uy + Fy / (R(2) * rho);
+            }
+        }
+    }
+    if (rho_out) rho_out[c] = O(rho);
+    if (u_out) {
+        u_out[c] = O(ux);
+        u_out[p.N + c] = O(uy);
+        if (L::DIM == 3) u_out[2 * p.N + c] = O(uz);
+    }
+}
+
+// ---- FP64 conservation sums and steady-state residual ------------------------------------
+struct Sums {
+    double m, jx, jy, jz;
+    unsigned long long bad;  // non-finite populations seen
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Stage 1: one partial per block over a grid-stride range of cells (fixed grid -> deterministic).
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_sums_partial(const S* __restrict__ f, long long N, float inv_scale,
+                                                       Sums* __restrict__ partial) {
+    using R = typename Codec<S>::Real;
+    double m = 0, jx = 0, jy = 0, jz = 0;
+    unsigned long long bad = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N;
+         c += (long long)gridDim.x * blockDim.x) {
+        static_for<L::Q>([&](auto I) {
+            constexpr int i = I;
+            const double v = (double)Codec<S>::load(f + (long long)i * N + c, R(L::w(i)), R(inv_scale));
+            if (!isfinite(v)) ++bad;
+            m += v;
+            if constexpr (L::cx(i) != 0) jx += L::cx(i) * v;
+            if constexpr (L::cy(i) != 0) jy += L::cy(i) * v;
+            if constexpr (L::cz(i) != 0) jz += L::cz(i) * v;
+        });
+    }
+    __shared__ double sh[4][8];
+    __shared__ unsigned long long shb[8];
+    m = warp_sum(m);
+    jx = warp_sum(jx);
+    jy = warp_sum(jy);
+    jz = warp_sum(jz);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        sh[0][wid] = m;
+        sh[1][wid] = jx;
+        sh[2][wid] = jy;
+        sh[3][wid] = jz;
+        shb[wid] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Sums s{0, 0, 0, 0, 0};
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            s.m += sh[0][w];
+            s.jx += sh[1][w];
+            s.jy += sh[2][w];
+            s.jz += sh[3][w];
+            s.bad += shb[w];
+        }
+        partial[blockIdx.x] = s;
+    }
+}
+
+// Stage 2: one thread folds the partials in index order.
+__global__ void k_sums_final(const Sums* __restrict__ partial, int n, Sums* __restrict__ out);
+
+// Residual partials: sum |u_a - u_b|^2 and |u_a|^2 over class-0 cells (local moments).
+template <class L, class S>
+__global__ void __launch_bounds__(256) k_residual_partial(const S* __restrict__ fa, const S* __restrict__ fb,
+                                                           const uint8_t* __restrict__ mask, long long N,
+                                                           float inv_scale, Sums* __restrict__ partial) {
+    using R = typename Codec<S>::Real;
+    double num = 0, den = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N;
+         c += (long long)gridDim.x * blockDim.x) {
+        if (mask && __ldg(mask + c) != 0) continue;
+        double ra = 0, xa = 0, ya = 0, za = 0, rb = 0, xb = 0, yb = 0, zb = 0;
+        static_for<L::Q>([&](auto I) {
+            constexpr int i = I;
+            const double a = (double)Codec<S>::load(fa + (long long)i * N + c, R(L::w(i)), R(inv_scale));
+            const double b = (double)Codec<S>::load(fb + (long long)i * N + c, R(L::w(i)), R(inv_scale));
+            ra += a;
+            rb += b;
+            xa += L::cx(i) * a;
+            xb += L::cx(i) * b;
+            ya += L::cy(i) * a;
+            yb += L::cy(i) * b;
+            za += L::cz(i) * a;
+            zb += L::cz(i) * b;
+        });
+        const double dx = xa / ra - xb / rb, dy = ya / ra - yb / rb, dz = za / ra - zb / rb;
+        num += dx * dx + dy * dy + dz * dz;
+        den += (xa * xa + ya * ya + za * za) / (ra * ra);
+    }
+    __shared__ double sh[2][8];
+    num = warp_sum(num);
+    den = warp_sum(den);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        sh[0][wid] = num;
+        sh[1][wid] = den;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Sums s{0, 0, 0, 0, 0};
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            s.m += sh[0][w];
+            s.jx += sh[1][w];
+        }
+        partial[blockIdx.x] = s;
+    }
+}
+
+}  // namespace lbm

@@ -1,0 +1,704 @@
+// runtime.cu — the single-lattice context behind the C ABI: device buffers (ping-pong
+// populations, mask, Shan-Chen psi, reduction partials), kernel dispatch, CUDA-graph capture of
+// step chunks, the block-width autotuner, population/field transfers and FP64 reductions.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "kernels.cuh"
+
+namespace lbm {
+
+__global__ void k_sums_final(const Sums* __restrict__ partial, int n, Sums* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Sums s{0, 0, 0, 0, 0};
+    for (int i = 0; i < n; ++i) {
+        s.m += partial[i].m;
+        s.jx += partial[i].jx;
+        s.jy += partial[i].jy;
+        s.jz += partial[i].jz;
+        s.bad += partial[i].bad;
+    }
+    *out = s;
+}
+
+// One plane of populations (direction i) from plain values to the storage codec and back.
+template <class S, class In>
+__global__ void k_encode_plane(const In* __restrict__ src, S* __restrict__ dst, long long n, double w, double scale) {
+    using R = typename Codec<S>::Real;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        Codec<S>::store(dst + k, R(src[k]), R(w), R(scale));
+}
+template <class S, class Out>
+__global__ void k_decode_plane(const S* __restrict__ src, Out* __restrict__ dst, long long n, double w,
+                               double inv_scale) {
+    using R = typename Codec<S>::Real;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        dst[k] = Out(Codec<S>::load(src + k, R(w), R(inv_scale)));
+}
+
+// F = feq(rho, u) for every cell; rho/u may be null (1 and 0).
+template <class L, class S>
+__global__ void k_init_eq(S* __restrict__ f, long long N, const double* __restrict__ rho,
+                          const double* __restrict__ u, double scale) {
+    using R = typename Codec<S>::Real;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+        const R r = rho ? R(rho[c]) : R(1);
+        const R ux = u ? R(u[c]) : R(0), uy = u ? R(u[N + c]) : R(0);
+        const R uz = (u && L::DIM == 3) ? R(u[2 * N + c]) : R(0);
+        R feq[L::Q];
+        equilibrium<L, R>(r, ux, uy, uz, feq);
+        static_for<L::Q>([&](auto I) {
+            constexpr int i = I;
+            Codec<S>::store(f + (long long)i * N + c, feq[i], R(L::w(i)), R(scale));
+        });
+    }
+}
+
+template <class T>
+struct Tag {
+    using type = T;
+};
+
+template <class F>
+static void dispatch_storage(int storage, F&& f) {
+    switch (storage) {
+        case LBM_F32: f(Tag<float>{}); break;
+        case LBM_F16S: f(Tag<__half>{}); break;
+        case LBM_BF16S: f(Tag<__nv_bfloat16>{}); break;
+        default: f(Tag<double>{}); break;
+    }
+}
+
+template <class F>
+static void dispatch_lattice(int lattice, F&& f) {
+    if (lattice == LBM_D2Q9)
+        f(Tag<D2Q9>{});
+    else
+        f(Tag<D3Q27>{});
+}
+
+static int grid_blocks(long long n, int threads) {
+    long long b = (n + threads - 1) / threads;
+    return (int)std::max(1LL, std::min(b, 148LL * 16));
+}
+
+}  // namespace lbm
+
+using namespace lbm;
+
+struct lbm_ctx {
+    lbm_desc d{};
+    int q = 0, dim = 0, sbytes = 0;
+    long long N = 0;
+    void* f[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint8_t* mask = nullptr;
+    void* psi = nullptr;
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+    Sums* partial = nullptr;
+    Sums* sums_out = nullptr;
+    int reduce_blocks = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bool timed = false;
+    int block = 0;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int gsteps = 0;
+    bool has_prev = false;
+    long long steps = 0;
+    double scale = 1.0;
+    StepParams<float> pf{};
+    StepParams<double> pd{};
+};
+
+namespace lbm {
+
+template <class R>
+static StepParams<R> make_params(const lbm_ctx* c) {
+    StepParams<R> p{};
+    const lbm_desc& d = c->d;
+    p.mask = c->mask;
+    p.nx = (int)d.nx;
+    p.ny = (int)d.ny;
+    p.nz = (int)d.nz;
+    p.N = c->N;
+    p.omega = R(d.omega);
+    p.one_m_omega = R(1) - R(d.omega);
+    p.scale = R(c->scale);
+    p.inv_scale = R(1.0 / c->scale);
+    p.G = R(d.sc_G);
+    p.psi = static_cast<R*>(c->psi);
+    for (int k = 0; k < kMaxClasses; ++k) {
+        const bool used = k < d.n_classes;
+        p.cls.flags[k] = used ? d.classes[k].flags : 0u;
+        p.cls.rho[k] = R(used ? d.classes[k].rho : 1.0);
+        p.cls.ux[k] = R(used ? d.classes[k].ux : 0.0);
+        p.cls.uy[k] = R(used ? d.classes[k].uy : 0.0);
+        p.cls.uz[k] = R(used ? d.classes[k].uz : 0.0);
+    }
+    if (d.collision == LBM_MRT) {
+        MrtCoef<double> k;
+        mrt_coefficients(d.mrt_basis, d.mrt_s, k);
+        for (int t = 0; t < 27; ++t) {
+            p.mrt.alpha[t] = R(k.alpha[t]);
+            p.mrt.beta[t] = R(k.beta[t]);
+        }
+        for (int t = 0; t < 9; ++t) {
+            p.mrt.A[t] = R(k.A[t]);
+            p.mrt.B[t] = R(k.B[t]);
+        }
+    }
+    return p;
+}
+
+template <class R>
+static StepParams<R>& params_of(lbm_ctx* c);
+template <>
+StepParams<float>& params_of<float>(lbm_ctx* c) {
+    return c->pf;
+}
+template <>
+StepParams<double>& params_of<double>(lbm_ctx* c) {
+    return c->pd;
+}
+
+// Launch one time step reading buffer `from` and writing the other one.
+static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
+    const dim3 blk(block), grid((unsigned)((c->d.nx + block - 1) / block), (unsigned)c->d.ny, (unsigned)c->d.nz);
+    dispatch_storage(c->d.storage, [&](auto tag) {
+        using S = typename decltype(tag)::type;
+        using R = typename Codec<S>::Real;
+        StepParams<R> p = params_of<R>(c);
+        p.fin = c->f[from];
+        p.fout = c->f[from ^ 1];
+        switch (c->d.collision) {
+            case LBM_BGK:
+                if (c->d.lattice == LBM_D2Q9)
+                    k_step_bgk<D2Q9, S><<<grid, blk, 0, s>>>(p);
+                else
+                    k_step_bgk<D3Q27, S><<<grid, blk, 0, s>>>(p);
+                break;
+            case LBM_MRT:
+                if (c->d.mrt_basis == LBM_MRT_REF)
+                    k_step_mrt<kMrtRef, S><<<grid, blk, 0, s>>>(p);
+                else
+                    k_step_mrt<kMrtGramSchmidt, S><<<grid, blk, 0, s>>>(p);
+                break;
+            default:
+                k_sc_psi<S><<<grid, blk, 0, s>>>(p);
+                k_step_sc<S><<<grid, blk, 0, s>>>(p);
+                break;
+        }
+    });
+}
+
+static int max_block(const lbm_ctx* c) { return c->d.collision == LBM_MRT ? 256 : 512; }
+
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tune_cache;
+
+static std::string tune_key(const lbm_ctx* c) {
+    const lbm_desc& d = c->d;
+    char buf[160];
+    snprintf(buf, sizeof(buf), "%d/%d/%d/%d/%lld/%lld/%lld", d.lattice, d.collision, d.storage, d.mrt_basis,
+             (long long)d.nx, (long long)d.ny, (long long)d.nz);
+    return buf;
+}
+
+// Pick the block width by timing candidates on the real buffers: each trial reads the current
+// buffer and writes the other one, which the next step overwrites anyway.
+static int autotune(lbm_ctx* c) {
+    const std::string key = tune_key(c);
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            c->block = it->second;
+            return LBM_OK;
+        }
+    }
+    const int maxb = max_block(c);
+    const long long nxr = ((c->d.nx + 31) / 32) * 32;
+    std::vector<int> cands;
+    for (int b : {32, 64, 128, 256, 512})
+        if (b <= maxb && (b <= nxr || b == 32)) cands.push_back(b);
+    if (cands.size() == 1) {
+        c->block = cands[0];
+    } else {
+        cudaEvent_t a, b;
+        LBM_CK(cudaEventCreate(&a));
+        LBM_CK(cudaEventCreate(&b));
+        float best = 1e30f;
+        int best_b = cands[0];
+        const long long bytes = c->N * c->q * (long long)c->sbytes * 2;
+        const int reps = bytes > (256LL << 20) ? 2 : 6;
+        for (int blk : cands) {
+            launch_step(c, c->cur, c->stream, blk);
+            LBM_CK(cudaEventRecord(a, c->stream));
+            for (int r = 0; r < reps; ++r) launch_step(c, c->cur, c->stream, blk);
+            LBM_CK(cudaEventRecord(b, c->stream));
+            LBM_CK(cudaEventSynchronize(b));
+            float ms = 0;
+            LBM_CK(cudaEventElapsedTime(&ms, a, b));
+            if (ms < best) {
+                best = ms;
+                best_b = blk;
+            }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        LBM_CK(cudaGetLastError());
+        c->block = best_b;
+    }
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune_cache[key] = c->block;
+    return LBM_OK;
+}
+
+static void drop_graphs(lbm_ctx* c) {
+    for (auto& g : c->gexec)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    c->gsteps = 0;
+}
+
+// Capture `gsteps` (even) consecutive steps starting from each buffer parity.
+static int build_graphs(lbm_ctx* c) {
+    drop_graphs(c);
+    const double bytes = (double)c->N * c->q * c->sbytes * 2.0;
+    const double est_us = bytes / 5.0e6 + 2.0;  // ~5 TB/s plus launch latency
+    int g = (int)std::ceil(400.0 / est_us);
+    g = std::max(2, std::min(256, g + (g & 1)));
+    for (int start = 0; start < 2; ++start) {
+        cudaGraph_t graph;
+        LBM_CK(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
+        for (int s = 0; s < g; ++s) launch_step(c, (start + s) & 1, c->own, c->block);
+        LBM_CK(cudaStreamEndCapture(c->own, &graph));
+        cudaError_t e = cudaGraphInstantiate(&c->gexec[start], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
+    }
+    c->gsteps = g;
+    return LBM_OK;
+}
+
+static int ensure_staging(lbm_ctx* c, size_t bytes) {
+    if (c->staging_bytes >= bytes) return LBM_OK;
+    if (c->staging) cudaFree(c->staging);
+    c->staging = nullptr;
+    c->staging_bytes = 0;
+    if (cudaMalloc(&c->staging, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(LBM_ERR_NOMEM, "staging allocation failed");
+    }
+    c->staging_bytes = bytes;
+    return LBM_OK;
+}
+
+static void destroy_ctx(lbm_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->d.device);
+    if (c->own) cudaStreamSynchronize(c->own);
+    if (c->stream && c->stream != c->own) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    cudaFree(c->f[0]);
+    cudaFree(c->f[1]);
+    cudaFree(c->mask);
+    cudaFree(c->psi);
+    cudaFree(c->staging);
+    cudaFree(c->partial);
+    cudaFree(c->sums_out);
+    if (c->e0) cudaEventDestroy(c->e0);
+    if (c->e1) cudaEventDestroy(c->e1);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+}
+
+int ctx_buffers(lbm_ctx* c, void** f0, void** f1, const uint8_t** mask) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    *f0 = c->f[0];
+    *f1 = c->f[1];
+    *mask = c->mask;
+    return LBM_OK;
+}
+
+void ctx_set_current(lbm_ctx* c, int cur, bool has_prev, long long steps_added) {
+    c->cur = cur;
+    c->has_prev = has_prev;
+    c->steps += steps_added;
+}
+
+static int check_device(int dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return set_error(LBM_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (dev < 0 || dev >= n) return set_error(LBM_ERR_INVALID, "device ordinal out of range");
+    cudaDeviceProp prop;
+    LBM_CK(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10 || prop.minor != 0)
+        return set_error(LBM_ERR_NO_DEVICE, std::string("liblbm_b200 is built for sm_100a (B200); device is ") +
+                                                prop.name);
+    return LBM_OK;
+}
+
+}  // namespace lbm
+
+extern "C" {
+
+int lbm_create(const lbm_desc* d, lbm_ctx** out) {
+    if (!out) return set_error(LBM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int rc = validate_desc(d);
+    if (rc) return rc;
+    if ((rc = check_device(d->device))) return rc;
+    LBM_CK(cudaSetDevice(d->device));
+    lbm_ctx* c = new lbm_ctx();
+    c->d = *d;
+    c->d.mask = nullptr;
+    c->q = desc_q(d);
+    c->dim = d->lattice == LBM_D2Q9 ? 2 : 3;
+    c->N = desc_cells(d);
+    c->sbytes = storage_bytes(d->storage);
+    c->scale = d->storage_scale > 0 ? d->storage_scale : default_scale(d->storage);
+    const size_t fbytes = (size_t)c->N * c->q * c->sbytes;
+    c->reduce_blocks = grid_blocks(c->N, 256);
+    bool ok = cudaMalloc(&c->f[0], fbytes) == cudaSuccess && cudaMalloc(&c->f[1], fbytes) == cudaSuccess &&
+              cudaMalloc(&c->partial, sizeof(Sums) * c->reduce_blocks) == cudaSuccess &&
+              cudaMalloc(&c->sums_out, sizeof(Sums)) == cudaSuccess;
+    if (ok && d->mask) ok = cudaMalloc(&c->mask, (size_t)c->N) == cudaSuccess;
+    if (ok && d->collision == LBM_SHANCHEN)
+        ok = cudaMalloc(&c->psi, (size_t)c->N * (d->storage == LBM_F64 ? 8 : 4)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        destroy_ctx(c);
+        return set_error(LBM_ERR_NOMEM, "device allocation failed");
+    }
+    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->e0) != cudaSuccess || cudaEventCreate(&c->e1) != cudaSuccess) {
+        destroy_ctx(c);
+        return set_error(LBM_ERR_CUDA, "stream/event creation failed");
+    }
+    c->stream = c->own;
+    if (d->mask) {
+        for (long long k = 0; k < c->N; ++k)
+            if (d->mask[k] >= d->n_classes) {
+                destroy_ctx(c);
+                return set_error(LBM_ERR_INVALID, "mask holds a class id >= n_classes");
+            }
+        if (cudaMemcpy(c->mask, d->mask, (size_t)c->N, cudaMemcpyHostToDevice) != cudaSuccess) {
+            destroy_ctx(c);
+            return set_error(LBM_ERR_CUDA, "mask upload failed");
+        }
+    }
+    c->pf = make_params<float>(c);
+    c->pd = make_params<double>(c);
+    rc = lbm_init_equilibrium(c, nullptr, nullptr);
+    if (rc) {
+        destroy_ctx(c);
+        return rc;
+    }
+    *out = c;
+    return LBM_OK;
+}
+
+void lbm_destroy(lbm_ctx* c) { destroy_ctx(c); }
+
+int lbm_init_equilibrium(lbm_ctx* c, const double* rho, const double* u) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    LBM_CK(cudaSetDevice(c->d.device));
+    double* drho = nullptr;
+    double* du = nullptr;
+    if (rho || u) {
+        int rc = ensure_staging(c, sizeof(double) * (size_t)c->N * (1 + c->dim));
+        if (rc) return rc;
+        drho = static_cast<double*>(c->staging);
+        du = drho + c->N;
+        if (rho) LBM_CK(cudaMemcpyAsync(drho, rho, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+        if (u) LBM_CK(cudaMemcpyAsync(du, u, sizeof(double) * c->N * c->dim, cudaMemcpyHostToDevice, c->stream));
+    }
+    const int blocks = grid_blocks(c->N, 256);
+    dispatch_storage(c->d.storage, [&](auto tag) {
+        using S = typename decltype(tag)::type;
+        dispatch_lattice(c->d.lattice, [&](auto lt) {
+            using L = typename decltype(lt)::type;
+            k_init_eq<L, S><<<blocks, 256, 0, c->stream>>>(static_cast<S*>(c->f[c->cur]), c->N,
+                                                            rho ? drho : nullptr, u ? du : nullptr, c->scale);
+        });
+    });
+    LBM_CK(cudaGetLastError());
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    c->has_prev = false;
+    return LBM_OK;
+}
+
+int lbm_set_populations(lbm_ctx* c, const void* src, int dtype, int memory) {
+    if (!c || !src) return set_error(LBM_ERR_INVALID, "NULL argument");
+    if (dtype != LBM_DTYPE_F32 && dtype != LBM_DTYPE_F64) return set_error(LBM_ERR_INVALID, "dtype must be F32 or F64");
+    if (memory != LBM_HOST && memory != LBM_DEVICE) return set_error(LBM_ERR_INVALID, "memory must be HOST or DEVICE");
+    LBM_CK(cudaSetDevice(c->d.device));
+    const size_t elt = dtype == LBM_DTYPE_F32 ? 4 : 8;
+    const cudaMemcpyKind kind = memory == LBM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const bool same = (dtype == LBM_DTYPE_F32 && c->d.storage == LBM_F32) ||
+                      (dtype == LBM_DTYPE_F64 && c->d.storage == LBM_F64);
+    if (same) {
+        LBM_CK(cudaMemcpyAsync(c->f[c->cur], src, elt * c->N * c->q, kind, c->stream));
+    } else {
+        if (memory == LBM_HOST) {
+            int rc = ensure_staging(c, elt * c->N);
+            if (rc) return rc;
+        }
+        const int blocks = grid_blocks(c->N, 256);
+        for (int i = 0; i < c->q; ++i) {
+            const char* plane = static_cast<const char*>(src) + elt * c->N * i;
+            const void* in = plane;
+            if (memory == LBM_HOST) {
+                LBM_CK(cudaMemcpyAsync(c->staging, plane, elt * c->N, kind, c->stream));
+                in = c->staging;
+            }
+            const double w = c->d.lattice == LBM_D2Q9 ? D2Q9::w(i) : D3Q27::w(i);
+            dispatch_storage(c->d.storage, [&](auto tag) {
+                using S = typename decltype(tag)::type;
+                S* dst = static_cast<S*>(c->f[c->cur]) + (long long)i * c->N;
+                if (dtype == LBM_DTYPE_F32)
+                    k_encode_plane<S, float><<<blocks, 256, 0, c->stream>>>(static_cast<const float*>(in), dst, c->N, w,
+                                                                           c->scale);
+                else
+                    k_encode_plane<S, double><<<blocks, 256, 0, c->stream>>>(static_cast<const double*>(in), dst, c->N,
+                                                                            w, c->scale);
+            });
+            LBM_CK(cudaGetLastError());
+        }
+    }
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    c->has_prev = false;
+    return LBM_OK;
+}
+
+int lbm_get_populations(lbm_ctx* c, void* dst, int dtype, int memory) {
+    if (!c || !dst) return set_error(LBM_ERR_INVALID, "NULL argument");
+    if (dtype != LBM_DTYPE_F32 && dtype != LBM_DTYPE_F64) return set_error(LBM_ERR_INVALID, "dtype must be F32 or F64");
+    if (memory != LBM_HOST && memory != LBM_DEVICE) return set_error(LBM_ERR_INVALID, "memory must be HOST or DEVICE");
+    LBM_CK(cudaSetDevice(c->d.device));
+    const size_t elt = dtype == LBM_DTYPE_F32 ? 4 : 8;
+    const cudaMemcpyKind kind = memory == LBM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    const bool same = (dtype == LBM_DTYPE_F32 && c->d.storage == LBM_F32) ||
+                      (dtype == LBM_DTYPE_F64 && c->d.storage == LBM_F64);
+    if (same) {
+        LBM_CK(cudaMemcpyAsync(dst, c->f[c->cur], elt * c->N * c->q, kind, c->stream));
+    } else {
+        if (memory == LBM_HOST) {
+            int rc = ensure_staging(c, elt * c->N);
+            if (rc) return rc;
+        }
+        const int blocks = grid_blocks(c->N, 256);
+        for (int i = 0; i < c->q; ++i) {
+            char* plane = static_cast<char*>(dst) + elt * c->N * i;
+            void* out = memory == LBM_HOST ? c->staging : plane;
+            const double w = c->d.lattice == LBM_D2Q9 ? D2Q9::w(i) : D3Q27::w(i);
+            dispatch_storage(c->d.storage, [&](auto tag) {
+                using S = typename decltype(tag)::type;
+                const S* srcp = static_cast<const S*>(c->f[c->cur]) + (long long)i * c->N;
+                if (dtype == LBM_DTYPE_F32)
+                    k_decode_plane<S, float><<<blocks, 256, 0, c->stream>>>(srcp, static_cast<float*>(out), c->N, w,
+                                                                           1.0 / c->scale);
+                else
+                    k_decode_plane<S, double><<<blocks, 256, 0, c->stream>>>(srcp, static_cast<double*>(out), c->N, w,
+                                                                            1.0 / c->scale);
+            });
+            LBM_CK(cudaGetLastError());
+            if (memory == LBM_HOST) LBM_CK(cudaMemcpyAsync(plane, c->staging, elt * c->N, kind, c->stream));
+        }
+    }
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    return LBM_OK;
+}
+
+int lbm_step(lbm_ctx* c, int64_t nsteps) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    if (nsteps < 0) return set_error(LBM_ERR_INVALID, "nsteps must be >= 0");
+    if (nsteps == 0) return LBM_OK;
+    LBM_CK(cudaSetDevice(c->d.device));
+    if (c->block == 0) {
+        int rc = autotune(c);
+        if (rc) return rc;
+    }
+    LBM_CK(cudaEventRecord(c->e0, c->stream));
+    long long n = nsteps;
+    if (n >= 2) {
+        if (!c->gsteps) {
+            int rc = build_graphs(c);
+            if (rc) return rc;
+        }
+        while (n >= c->gsteps) {
+            LBM_CK(cudaGraphLaunch(c->gexec[c->cur], c->stream));
+            n -= c->gsteps;
+        }
+    }
+    while (n > 0) {
+        launch_step(c, c->cur, c->stream, c->block);
+        c->cur ^= 1;
+        --n;
+    }
+    LBM_CK(cudaGetLastError());
+    LBM_CK(cudaEventRecord(c->e1, c->stream));
+    c->timed = true;
+    c->has_prev = true;
+    c->steps += nsteps;
+    return LBM_OK;
+}
+
+int lbm_sync(lbm_ctx* c) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    LBM_CK(cudaSetDevice(c->d.device));
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    return LBM_OK;
+}
+
+int lbm_last_step_ms(lbm_ctx* c, float* ms) {
+    if (!c || !ms) return set_error(LBM_ERR_INVALID, "NULL argument");
+    if (!c->timed) return set_error(LBM_ERR_STATE, "no step has been issued");
+    LBM_CK(cudaSetDevice(c->d.device));
+    LBM_CK(cudaEventSynchronize(c->e1));
+    LBM_CK(cudaEventElapsedTime(ms, c->e0, c->e1));
+    return LBM_OK;
+}
+
+int64_t lbm_steps_done(const lbm_ctx* c) { return c ? c->steps : -1; }
+
+int lbm_get_macros(lbm_ctx* c, void* rho, void* u, int dtype, int memory) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    if (dtype != LBM_DTYPE_F32 && dtype != LBM_DTYPE_F64) return set_error(LBM_ERR_INVALID, "dtype must be F32 or F64");
+    if (memory != LBM_HOST && memory != LBM_DEVICE) return set_error(LBM_ERR_INVALID, "memory must be HOST or DEVICE");
+    if (!rho && !u) return LBM_OK;
+    LBM_CK(cudaSetDevice(c->d.device));
+    const size_t elt = dtype == LBM_DTYPE_F32 ? 4 : 8;
+    void* drho = rho;
+    void* du = u;
+    if (memory == LBM_HOST) {
+        int rc = ensure_staging(c, elt * c->N * (1 + c->dim));
+        if (rc) return rc;
+        drho = rho ? c->staging : nullptr;
+        du = u ? static_cast<char*>(c->staging) + elt * c->N : nullptr;
+    }
+    const int pulled = c->has_prev ? 1 : 0;
+    const int src = c->has_prev ? (c->cur ^ 1) : c->cur;
+    const int block = 128;
+    const dim3 grid((unsigned)((c->d.nx + block - 1) / block), (unsigned)c->d.ny, (unsigned)c->d.nz);
+    dispatch_storage(c->d.storage, [&](auto tag) {
+        using S = typename decltype(tag)::type;
+        using R = typename Codec<S>::Real;
+        StepParams<R> p = params_of<R>(c);
+        p.fin = c->f[src];
+        dispatch_lattice(c->d.lattice, [&](auto lt) {
+            using L = typename decltype(lt)::type;
+            if (dtype == LBM_DTYPE_F32)
+                k_macros<L, S, float><<<grid, block, 0, c->stream>>>(p, pulled, c->d.collision, static_cast<float*>(drho),
+                                                                     static_cast<float*>(du));
+            else
+                k_macros<L, S, double><<<grid, block, 0, c->stream>>>(p, pulled, c->d.collision,
+                                                                      static_cast<double*>(drho), static_cast<double*>(du));
+        });
+    });
+    LBM_CK(cudaGetLastError());
+    if (memory == LBM_HOST) {
+        if (rho) LBM_CK(cudaMemcpyAsync(rho, drho, elt * c->N, cudaMemcpyDeviceToHost, c->stream));
+        if (u) LBM_CK(cudaMemcpyAsync(u, du, elt * c->N * c->dim, cudaMemcpyDeviceToHost, c->stream));
+    }
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    return LBM_OK;
+}
+
+int lbm_sums_fp64(lbm_ctx* c, double out[4]) {
+    if (!c || !out) return set_error(LBM_ERR_INVALID, "NULL argument");
+    LBM_CK(cudaSetDevice(c->d.device));
+    dispatch_storage(c->d.storage, [&](auto tag) {
+        using S = typename decltype(tag)::type;
+        dispatch_lattice(c->d.lattice, [&](auto lt) {
+            using L = typename decltype(lt)::type;
+            k_sums_partial<L, S><<<c->reduce_blocks, 256, 0, c->stream>>>(static_cast<const S*>(c->f[c->cur]), c->N,
+                                                                          (float)(1.0 / c->scale), c->partial);
+        });
+    });
+    k_sums_final<<<1, 32, 0, c->stream>>>(c->partial, c->reduce_blocks, c->sums_out);
+    LBM_CK(cudaGetLastError());
+    Sums s;
+    LBM_CK(cudaMemcpyAsync(&s, c->sums_out, sizeof(Sums), cudaMemcpyDeviceToHost, c->stream));
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    out[0] = s.m;
+    out[1] = s.jx;
+    out[2] = s.jy;
+    out[3] = s.jz;
+    if (s.bad) return set_error(LBM_ERR_DIVERGED, std::to_string(s.bad) + " non-finite populations");
+    return LBM_OK;
+}
+
+int lbm_residual_fp64(lbm_ctx* c, double* out) {
+    if (!c || !out) return set_error(LBM_ERR_INVALID, "NULL argument");
+    if (!c->has_prev) return set_error(LBM_ERR_STATE, "residual needs at least one step since the last set/init");
+    LBM_CK(cudaSetDevice(c->d.device));
+    dispatch_storage(c->d.storage, [&](auto tag) {
+        using S = typename decltype(tag)::type;
+        dispatch_lattice(c->d.lattice, [&](auto lt) {
+            using L = typename decltype(lt)::type;
+            k_residual_partial<L, S><<<c->reduce_blocks, 256, 0, c->stream>>>(
+                static_cast<const S*>(c->f[c->cur]), static_cast<const S*>(c->f[c->cur ^ 1]), c->mask, c->N,
+                (float)(1.0 / c->scale), c->partial);
+        });
+    });
+    k_sums_final<<<1, 32, 0, c->stream>>>(c->partial, c->reduce_blocks, c->sums_out);
+    LBM_CK(cudaGetLastError());
+    Sums s;
+    LBM_CK(cudaMemcpyAsync(&s, c->sums_out, sizeof(Sums), cudaMemcpyDeviceToHost, c->stream));
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    *out = s.jx > 0 ? std::sqrt(s.m / s.jx) : 0.0;
+    if (!std::isfinite(*out)) return set_error(LBM_ERR_DIVERGED, "residual is not finite");
+    return LBM_OK;
+}
+
+void* lbm_stream(lbm_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int lbm_set_stream(lbm_ctx* c, void* stream) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    LBM_CK(cudaSetDevice(c->d.device));
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own;
+    return LBM_OK;
+}
+
+void* lbm_device_populations(lbm_ctx* c, size_t* bytes) {
+    if (!c) return nullptr;
+    if (bytes) *bytes = (size_t)c->N * c->q * c->sbytes;
+    return c->f[c->cur];
+}
+
+int lbm_get_desc(const lbm_ctx* c, lbm_desc* out) {
+    if (!c || !out) return set_error(LBM_ERR_INVALID, "NULL argument");
+    *out = c->d;
+    return LBM_OK;
+}
+
+int lbm_set_block(lbm_ctx* c, int threads_x) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    if (threads_x != 0 && (threads_x < 32 || threads_x > max_block(c) || (threads_x & 31)))
+        return set_error(LBM_ERR_INVALID, "block width must be 0 or a multiple of 32 within the kernel's launch bound");
+    LBM_CK(cudaSetDevice(c->d.device));
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->block = threads_x;
+    return LBM_OK;
+}
+
+int lbm_get_block(const lbm_ctx* c) { return c ? c->block : 0; }
+
+}  // extern "C"

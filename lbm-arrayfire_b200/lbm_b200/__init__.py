@@ -1,0 +1,469 @@
+"""Python binding of liblbm_b200.so (the B200 Lattice Boltzmann engine) over its C ABI.
+
+The binding is a thin ctypes layer: every call goes through the ``extern "C"`` entry points declared
+in ``include/lbm.h``; there is no Python or CPU fallback.  If the shared library is missing the
+import fails with a message saying how to build it.
+
+The objects mirror the reference drivers' state (michaltakac/lbm-arrayfire ``cpp/*.cpp``,
+``rust/examples/*.rs``): a population array ``F`` in column-major ``[nx, ny(, nz), Q]`` layout,
+a solid/lid/inlet mask and the scalar relaxation parameters; ``Lattice.step(n)`` replaces ``n``
+iterations of the reference's ``while`` loop body (e.g. cpp/d2q9_bgk_lid.cpp:123-155).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = [
+    "LIB_PATH", "lib", "LbmError", "Desc", "CellClass", "Lattice", "Batch",
+    "D2Q9", "D3Q27", "BGK", "MRT", "SHANCHEN", "F32", "F16S", "BF16S", "F64",
+    "MRT_REF", "MRT_GRAM_SCHMIDT", "BOUNCE", "SET_RHO", "SET_UX", "SET_UY", "SET_UZ",
+    "EQUILIBRIUM", "ZEROGRAD_XP", "velocities", "omega_from_re", "mrt_reference_rates", "mrt_rates",
+    "mrt_collide_host", "setup_cavity2d", "setup_cavity3d", "setup_channel2d", "setup_duct3d",
+    "mask_from_index_list", "EXPORTED_SYMBOLS",
+]
+
+LIB_PATH = Path(os.environ.get("LBM_B200_LIB", Path(__file__).resolve().parent / "liblbm_b200.so"))
+
+D2Q9, D3Q27 = 0, 1
+BGK, MRT, SHANCHEN = 0, 1, 2
+F32, F16S, BF16S, F64 = 0, 1, 2, 3
+MRT_REF, MRT_GRAM_SCHMIDT = 0, 1
+DTYPE_F32, DTYPE_F64 = 0, 1
+HOST, DEVICE = 0, 1
+BOUNCE, SET_RHO, SET_UX, SET_UY, SET_UZ, EQUILIBRIUM, ZEROGRAD_XP = 1, 2, 4, 8, 16, 32, 64
+MAX_CLASSES = 16
+
+ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "diverged",
+          -5: "unsupported", -6: "no device", -7: "invalid state"}
+
+
+class LbmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)} ({code}): {msg}")
+        self.code = code
+
+
+class CellClass(C.Structure):
+    _fields_ = [("flags", C.c_uint32), ("reserved", C.c_uint32), ("rho", C.c_double), ("ux", C.c_double),
+                ("uy", C.c_double), ("uz", C.c_double)]
+
+
+class Desc(C.Structure):
+    _fields_ = [
+        ("lattice", C.c_int32), ("collision", C.c_int32), ("storage", C.c_int32), ("mrt_basis", C.c_int32),
+        ("nx", C.c_int64), ("ny", C.c_int64), ("nz", C.c_int64),
+        ("omega", C.c_double), ("mrt_s", C.c_double * 27), ("sc_G", C.c_double),
+        ("storage_scale", C.c_double), ("n_classes", C.c_int32), ("device", C.c_int32),
+        ("classes", CellClass * MAX_CLASSES), ("mask", C.POINTER(C.c_uint8)),
+    ]
+
+    @property
+    def q(self) -> int:
+        return 9 if self.lattice == D2Q9 else 27
+
+    @property
+    def dim(self) -> int:
+        return 2 if self.lattice == D2Q9 else 3
+
+    @property
+    def cells(self) -> int:
+        return int(self.nx * self.ny * self.nz)
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny) if self.lattice == D2Q9 else (self.nx, self.ny, self.nz)
+
+
+# name -> (restype, argtypes); the complete ABI of include/lbm.h
+_P = C.c_void_p
+_DP = C.POINTER(Desc)
+_SIGS = {
+    "lbm_abi_version": (C.c_int, []),
+    "lbm_strerror": (C.c_char_p, [C.c_int]),
+    "lbm_last_error": (C.c_char_p, []),
+    "lbm_desc_init": (None, [_DP, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64]),
+    "lbm_q": (C.c_int, [C.c_int]),
+    "lbm_velocities": (C.c_int, [C.c_int, _P, _P, _P, _P, _P]),
+    "lbm_create": (C.c_int, [_DP, C.POINTER(_P)]),
+    "lbm_destroy": (None, [_P]),
+    "lbm_set_populations": (C.c_int, [_P, _P, C.c_int, C.c_int]),
+    "lbm_get_populations": (C.c_int, [_P, _P, C.c_int, C.c_int]),
+    "lbm_init_equilibrium": (C.c_int, [_P, _P, _P]),
+    "lbm_step": (C.c_int, [_P, C.c_int64]),
+    "lbm_sync": (C.c_int, [_P]),
+    "lbm_get_macros": (C.c_int, [_P, _P, _P, C.c_int, C.c_int]),
+    "lbm_sums_fp64": (C.c_int, [_P, _P]),
+    "lbm_residual_fp64": (C.c_int, [_P, _P]),
+    "lbm_last_step_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "lbm_steps_done": (C.c_int64, [_P]),
+    "lbm_stream": (_P, [_P]),
+    "lbm_set_stream": (C.c_int, [_P, _P]),
+    "lbm_device_populations": (_P, [_P, C.POINTER(C.c_size_t)]),
+    "lbm_get_desc": (C.c_int, [_P, _DP]),
+    "lbm_set_block": (C.c_int, [_P, C.c_int]),
+    "lbm_get_block": (C.c_int, [_P]),
+    "lbm_batch_create": (C.c_int, [_DP, C.c_int, C.POINTER(_P)]),
+    "lbm_batch_destroy": (None, [_P]),
+    "lbm_batch_size": (C.c_int, [_P]),
+    "lbm_batch_step": (C.c_int, [_P, C.c_int64]),
+    "lbm_batch_sync": (C.c_int, [_P]),
+    "lbm_batch_get_populations": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int]),
+    "lbm_batch_set_populations": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int]),
+    "lbm_batch_get_macros": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, C.c_int]),
+    "lbm_batch_sums_fp64": (C.c_int, [_P, C.c_int, _P]),
+    "lbm_batch_cells": (C.c_int64, [_P]),
+    "lbm_batch_stream": (_P, [_P]),
+    "lbm_batch_tile_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
+    "lbm_setup_cavity2d": (C.c_int, [_DP, _P, C.c_double]),
+    "lbm_setup_cavity3d": (C.c_int, [_DP, _P, C.c_double]),
+    "lbm_setup_channel2d": (C.c_int, [_DP, _P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]),
+    "lbm_setup_duct3d": (C.c_int, [_DP, _P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]),
+    "lbm_mask_from_index_list": (C.c_int, [_P, C.c_int64, _P, C.c_int64, C.c_uint8]),
+    "lbm_omega_from_re": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_int]),
+    "lbm_mrt_reference_rates": (None, [_P]),
+    "lbm_mrt_rates": (None, [_P, C.c_double, C.c_double]),
+    "lbm_mrt_collide_host": (C.c_int, [_DP, _P, C.c_double, _P, _P]),
+}
+EXPORTED_SYMBOLS = tuple(_SIGS)
+
+_lib = None
+
+
+def lib():
+    """Load liblbm_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C lbm-arrayfire_b200` "
+                              "(or __graft_entry__.build())")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise LbmError(rc, lib().lbm_last_error().decode())
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _torch_ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def velocities(lattice: int):
+    q = 9 if lattice == D2Q9 else 27
+    cx, cy, cz, opp = (np.zeros(q, np.int32) for _ in range(4))
+    w = np.zeros(q)
+    _check(lib().lbm_velocities(lattice, _ptr(cx), _ptr(cy), _ptr(cz), _ptr(w), _ptr(opp)))
+    return cx, cy, cz, w, opp
+
+
+def omega_from_re(u: float, L: float, re: float, rule: int = 0) -> float:
+    return lib().lbm_omega_from_re(u, L, re, rule)
+
+
+def mrt_reference_rates() -> np.ndarray:
+    s = np.zeros(27)
+    lib().lbm_mrt_reference_rates(_ptr(s))
+    return s
+
+
+def mrt_rates(sv: float, other: float) -> np.ndarray:
+    s = np.zeros(27)
+    lib().lbm_mrt_rates(_ptr(s), sv, other)
+    return s
+
+
+def make_desc(lattice: int, collision: int, storage: int, shape, *, omega: float = 1.0, mrt_s=None,
+              mrt_basis: int = MRT_REF, sc_G: float = 0.0, storage_scale: float = 0.0, device: int = 0) -> Desc:
+    d = Desc()
+    nx, ny = int(shape[0]), int(shape[1])
+    nz = int(shape[2]) if len(shape) > 2 else 1
+    lib().lbm_desc_init(C.byref(d), lattice, collision, storage, nx, ny, nz)
+    d.omega = omega
+    if mrt_s is not None:
+        for i, v in enumerate(mrt_s):
+            d.mrt_s[i] = float(v)
+    d.mrt_basis = mrt_basis
+    d.sc_G = sc_G
+    d.storage_scale = storage_scale
+    d.device = device
+    return d
+
+
+def set_classes(d: Desc, classes):
+    """classes: list of (flags, rho, ux, uy, uz)."""
+    d.n_classes = len(classes)
+    for k, (fl, r, ux, uy, uz) in enumerate(classes):
+        d.classes[k].flags, d.classes[k].rho = fl, r
+        d.classes[k].ux, d.classes[k].uy, d.classes[k].uz = ux, uy, uz
+
+
+def classes_of(d: Desc):
+    return [(d.classes[k].flags, d.classes[k].rho, d.classes[k].ux, d.classes[k].uy, d.classes[k].uz)
+            for k in range(d.n_classes)]
+
+
+def _mask_buf(d: Desc) -> np.ndarray:
+    return np.zeros(d.cells, dtype=np.uint8)
+
+
+def setup_cavity2d(d: Desc, u_lid: float) -> np.ndarray:
+    m = _mask_buf(d)
+    _check(lib().lbm_setup_cavity2d(C.byref(d), _ptr(m), u_lid))
+    return m
+
+
+def setup_cavity3d(d: Desc, u_lid: float) -> np.ndarray:
+    m = _mask_buf(d)
+    _check(lib().lbm_setup_cavity3d(C.byref(d), _ptr(m), u_lid))
+    return m
+
+
+def setup_channel2d(d: Desc, u_in: float, ox: float, oy: float, r: float, config_mode: bool) -> np.ndarray:
+    m = _mask_buf(d)
+    _check(lib().lbm_setup_channel2d(C.byref(d), _ptr(m), u_in, ox, oy, r, int(config_mode)))
+    return m
+
+
+def setup_duct3d(d: Desc, u_in: float, ox: float, oy: float, oz: float, r: float) -> np.ndarray:
+    m = _mask_buf(d)
+    _check(lib().lbm_setup_duct3d(C.byref(d), _ptr(m), u_in, ox, oy, oz, r))
+    return m
+
+
+def mask_from_index_list(n_cells: int, on, cls: int, mask=None) -> np.ndarray:
+    m = np.zeros(n_cells, np.uint8) if mask is None else mask
+    on = np.ascontiguousarray(on, dtype=np.int64)
+    _check(lib().lbm_mask_from_index_list(_ptr(m), n_cells, _ptr(on), on.size, cls))
+    return m
+
+
+def mrt_collide_host(d: Desc, f_in, rho: float, u) -> np.ndarray:
+    f_in = np.ascontiguousarray(f_in, dtype=np.float64)
+    uu = np.ascontiguousarray(u, dtype=np.float64)
+    out = np.zeros(27)
+    _check(lib().lbm_mrt_collide_host(C.byref(d), _ptr(f_in), rho, _ptr(uu), _ptr(out)))
+    return out
+
+
+class Lattice:
+    """One lattice on one GPU (an ``lbm_ctx``)."""
+
+    def __init__(self, desc: Desc, mask: np.ndarray | None = None):
+        self._mask = None
+        if mask is not None:
+            self._mask = np.ascontiguousarray(mask, dtype=np.uint8).ravel(order="F") \
+                if mask.ndim > 1 else np.ascontiguousarray(mask, dtype=np.uint8)
+            desc.mask = self._mask.ctypes.data_as(C.POINTER(C.c_uint8))
+        self.desc = desc
+        h = C.c_void_p()
+        _check(lib().lbm_create(C.byref(desc), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lbm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def q(self):
+        return self.desc.q
+
+    @property
+    def n(self):
+        return self.desc.cells
+
+    @property
+    def dim(self):
+        return self.desc.dim
+
+    def step(self, n: int = 1):
+        _check(lib().lbm_step(self._h, n))
+
+    def sync(self):
+        _check(lib().lbm_sync(self._h))
+
+    def last_step_ms(self) -> float:
+        ms = C.c_float()
+        _check(lib().lbm_last_step_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    @property
+    def steps_done(self) -> int:
+        return lib().lbm_steps_done(self._h)
+
+    def stream(self) -> int:
+        return lib().lbm_stream(self._h) or 0
+
+    def set_stream(self, stream: int | None):
+        _check(lib().lbm_set_stream(self._h, C.c_void_p(stream or 0)))
+
+    def set_block(self, threads_x: int):
+        _check(lib().lbm_set_block(self._h, threads_x))
+
+    def block(self) -> int:
+        return lib().lbm_get_block(self._h)
+
+    def device_populations(self):
+        nbytes = C.c_size_t()
+        p = lib().lbm_device_populations(self._h, C.byref(nbytes))
+        return p, nbytes.value
+
+    def init_equilibrium(self, rho=None, u=None):
+        r = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64).ravel(order="F")
+        uu = None if u is None else np.ascontiguousarray(u, dtype=np.float64).ravel()
+        _check(lib().lbm_init_equilibrium(self._h, None if r is None else _ptr(r), None if uu is None else _ptr(uu)))
+
+    def set_populations(self, F):
+        """F: host numpy (float32/float64, flat column-major N*Q) or a CUDA torch tensor."""
+        if hasattr(F, "data_ptr"):
+            dt = DTYPE_F32 if str(F.dtype) == "torch.float32" else DTYPE_F64
+            _check(lib().lbm_set_populations(self._h, _torch_ptr(F), dt, DEVICE if F.is_cuda else HOST))
+            return
+        F = np.ascontiguousarray(F)
+        if F.dtype not in (np.float32, np.float64):
+            F = F.astype(np.float64)
+        assert F.size == self.n * self.q
+        _check(lib().lbm_set_populations(self._h, _ptr(F), DTYPE_F32 if F.dtype == np.float32 else DTYPE_F64, HOST))
+
+    def get_populations(self, dtype=np.float64, out=None):
+        if out is not None and hasattr(out, "data_ptr"):
+            dt = DTYPE_F32 if str(out.dtype) == "torch.float32" else DTYPE_F64
+            _check(lib().lbm_get_populations(self._h, _torch_ptr(out), dt, DEVICE if out.is_cuda else HOST))
+            return out
+        F = np.empty(self.n * self.q, dtype=dtype) if out is None else out
+        _check(lib().lbm_get_populations(self._h, _ptr(F), DTYPE_F32 if F.dtype == np.float32 else DTYPE_F64, HOST))
+        return F
+
+    def macros(self, dtype=np.float64):
+        """(rho[N], u[dim*N]) — the fields the last step's collision used."""
+        rho = np.empty(self.n, dtype=dtype)
+        u = np.empty(self.dim * self.n, dtype=dtype)
+        _check(lib().lbm_get_macros(self._h, _ptr(rho), _ptr(u), DTYPE_F32 if dtype == np.float32 else DTYPE_F64,
+                                    HOST))
+        return rho, u
+
+    def macros_into(self, rho, u):
+        """Write the macros into host or device buffers (numpy arrays or torch tensors)."""
+        def p(a):
+            if a is None:
+                return None, HOST, DTYPE_F64
+            if hasattr(a, "data_ptr"):
+                return _torch_ptr(a), DEVICE if a.is_cuda else HOST, \
+                    DTYPE_F32 if str(a.dtype) == "torch.float32" else DTYPE_F64
+            return _ptr(a), HOST, DTYPE_F32 if a.dtype == np.float32 else DTYPE_F64
+        pr, mr, dr = p(rho)
+        pu, mu, du = p(u)
+        _check(lib().lbm_get_macros(self._h, pr, pu, dr if rho is not None else du, mr if rho is not None else mu))
+
+    def sums(self) -> np.ndarray:
+        out = np.zeros(4)
+        _check(lib().lbm_sums_fp64(self._h, _ptr(out)))
+        return out
+
+    def residual(self) -> float:
+        out = C.c_double()
+        _check(lib().lbm_residual_fp64(self._h, C.byref(out)))
+        return out.value
+
+
+class Batch:
+    """Many independent lattices advanced by one launch per step (an ``lbm_batch``)."""
+
+    def __init__(self, descs, masks):
+        self._masks = []
+        arr = (Desc * len(descs))()
+        for k, (d, m) in enumerate(zip(descs, masks)):
+            if m is not None:
+                mm = np.ascontiguousarray(m, dtype=np.uint8).ravel(order="F") if m.ndim > 1 else \
+                    np.ascontiguousarray(m, dtype=np.uint8)
+                self._masks.append(mm)
+                d.mask = mm.ctypes.data_as(C.POINTER(C.c_uint8))
+            arr[k] = d
+        self.descs = list(descs)
+        h = C.c_void_p()
+        _check(lib().lbm_batch_create(arr, len(descs), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lbm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return lib().lbm_batch_size(self._h)
+
+    @property
+    def cells(self) -> int:
+        return lib().lbm_batch_cells(self._h)
+
+    def step(self, n: int = 1):
+        _check(lib().lbm_batch_step(self._h, n))
+
+    def sync(self):
+        _check(lib().lbm_batch_sync(self._h))
+
+    def stream(self) -> int:
+        return lib().lbm_batch_stream(self._h) or 0
+
+    def tile_info(self):
+        tx = C.c_int()
+        nt = C.c_int64()
+        _check(lib().lbm_batch_tile_info(self._h, C.byref(tx), C.byref(nt)))
+        return tx.value, nt.value
+
+    def get_populations(self, k: int, dtype=np.float64):
+        d = self.descs[k]
+        F = np.empty(d.cells * d.q, dtype=dtype)
+        _check(lib().lbm_batch_get_populations(self._h, k, _ptr(F), DTYPE_F32 if dtype == np.float32 else DTYPE_F64,
+                                               HOST))
+        return F
+
+    def set_populations(self, k: int, F):
+        F = np.ascontiguousarray(F)
+        _check(lib().lbm_batch_set_populations(self._h, k, _ptr(F),
+                                               DTYPE_F32 if F.dtype == np.float32 else DTYPE_F64, HOST))
+
+    def macros(self, k: int, dtype=np.float64):
+        d = self.descs[k]
+        rho = np.empty(d.cells, dtype=dtype)
+        u = np.empty(d.dim * d.cells, dtype=dtype)
+        _check(lib().lbm_batch_get_macros(self._h, k, _ptr(rho), _ptr(u),
+                                          DTYPE_F32 if dtype == np.float32 else DTYPE_F64, HOST))
+        return rho, u
+
+    def sums(self, k: int) -> np.ndarray:
+        out = np.zeros(4)
+        _check(lib().lbm_batch_sums_fp64(self._h, k, _ptr(out)))
+        return out

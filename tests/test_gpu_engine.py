@@ -1,0 +1,207 @@
+"""Engine behaviour on the GPU beyond parity: transfers, graph vs single-step stepping, split vs
+continuous runs (checkpoint/resume), block widths, reductions, divergence detection, batched
+ensembles — all through the C ABI."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from helpers import O, cavity2d, cavity3d, channel2d, lb, mrt_cavity, oracle_problem, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def test_population_round_trip_exact():
+    d, m, F0 = cavity2d(n=64, storage=lb.F32)
+    rng = np.random.default_rng(0)
+    F = (F0 * (1 + 0.01 * rng.standard_normal(F0.size))).astype(np.float32)
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(F)
+        assert np.array_equal(lat.get_populations(np.float32), F)
+        lat.set_populations(F.astype(np.float64))
+        assert np.array_equal(lat.get_populations(np.float64), F.astype(np.float64))
+    d.storage = lb.F64
+    with lb.Lattice(d, m) as lat:
+        F64 = F0 * (1 + 0.01 * rng.standard_normal(F0.size))
+        lat.set_populations(F64)
+        assert np.array_equal(lat.get_populations(np.float64), F64)
+
+
+@pytest.mark.parametrize("storage,bound", [(lb.F16S, 2.0 ** -11 / 16384 * 4), (lb.BF16S, 2.0 ** -8 * 0.3)])
+def test_shifted_round_trip_error_is_bounded(storage, bound):
+    d, m, F0 = cavity2d(n=32, storage=storage)
+    rng = np.random.default_rng(1)
+    F = F0 * (1 + 0.05 * rng.standard_normal(F0.size))
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(F)
+        G = lat.get_populations(np.float64)
+    # error relative to the stored deviation from the rest weight
+    assert np.max(np.abs(G - F)) <= bound * 1.01
+
+
+def test_macros_before_any_step_are_local_moments():
+    d, m, F0 = cavity2d(n=32)
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(F0)
+        rho, u = lat.macros()
+    assert np.allclose(rho, 1.0, atol=1e-6)
+    assert np.allclose(u, 0.0, atol=1e-6)
+
+
+def test_graph_chunks_equal_single_steps():
+    d, m, F0 = cavity2d(n=128)
+    with lb.Lattice(d, m) as a, lb.Lattice(d, m) as b:
+        a.set_populations(F0)
+        b.set_populations(F0)
+        a.step(777)
+        for _ in range(777):
+            b.step(1)
+        assert np.array_equal(a.get_populations(np.float32), b.get_populations(np.float32))
+        assert a.steps_done == b.steps_done == 777
+
+
+def test_split_run_equals_continuous_run():
+    d, m, F0 = mrt_cavity(n=16, u_lid=0.1)
+    with lb.Lattice(d, m) as a:
+        a.set_populations(F0)
+        a.step(120)
+        ref = a.get_populations(np.float32)
+    with lb.Lattice(d, m) as b:
+        b.set_populations(F0)
+        b.step(50)
+        ckpt = b.get_populations(np.float32)
+    with lb.Lattice(d, m) as c:
+        c.set_populations(ckpt)
+        c.step(70)
+        assert np.array_equal(c.get_populations(np.float32), ref)
+
+
+def test_block_width_does_not_change_results():
+    d, m, F0 = cavity3d(n=(70, 12, 9), u_lid=0.1, omega=1.4)
+    out = []
+    for bx in (32, 64, 128, 256):
+        with lb.Lattice(d, m) as lat:
+            lat.set_block(bx)
+            lat.set_populations(F0)
+            lat.step(21)
+            assert lat.block() == bx
+            out.append(lat.get_populations(np.float32))
+    for o in out[1:]:
+        assert np.array_equal(o, out[0])
+
+
+def test_autotune_picks_a_legal_block():
+    d, m, F0 = cavity2d(n=256)
+    with lb.Lattice(d, m) as lat:
+        lat.step(4)
+        assert lat.block() in (32, 64, 128, 256, 512)
+        assert lat.last_step_ms() > 0
+
+
+def test_sums_match_oracle_and_detect_nan():
+    d, m, F0 = cavity2d(n=64)
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(F0)
+        lat.step(100)
+        F = lat.get_populations(np.float64)
+        s = lat.sums()
+        assert np.allclose(s, O.sums(oracle_problem(d, m), F), rtol=1e-12, atol=1e-12)
+        F[123] = np.nan
+        lat.set_populations(F)
+        with pytest.raises(lb.LbmError) as e:
+            lat.sums()
+        assert e.value.code == -4
+
+
+def test_residual_decreases_towards_steady_state():
+    d, m, F0 = cavity2d(n=64, u_lid=0.05, re=50)
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(F0)
+        with pytest.raises(lb.LbmError):
+            lat.residual()
+        lat.step(200)
+        r1 = lat.residual()
+        lat.step(5000)
+        r2 = lat.residual()
+    assert r2 < r1 and r2 < 1e-4
+
+
+def test_device_pointer_transfers_with_torch():
+    torch = pytest.importorskip("torch")
+    d, m, F0 = cavity2d(n=64)
+    with lb.Lattice(d, m) as lat:
+        t = torch.tensor(F0, dtype=torch.float32, device="cuda")
+        lat.set_populations(t)
+        lat.step(10)
+        out = torch.empty_like(t)
+        lat.get_populations(out=out)
+        torch.cuda.synchronize()
+        ref = lat.get_populations(np.float32)
+        assert np.array_equal(out.cpu().numpy(), ref)
+        rho = torch.empty(d.cells, dtype=torch.float64, device="cuda")
+        u = torch.empty(2 * d.cells, dtype=torch.float64, device="cuda")
+        lat.macros_into(rho, u)
+        r2, u2 = lat.macros()
+        assert np.array_equal(rho.cpu().numpy(), r2)
+
+
+def test_external_stream():
+    torch = pytest.importorskip("torch")
+    d, m, F0 = cavity2d(n=64)
+    s = torch.cuda.Stream()
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(F0)
+        lat.set_stream(s.cuda_stream)
+        lat.step(10)
+        lat.sync()
+        a = lat.get_populations(np.float32)
+        lat.set_stream(None)
+    with lb.Lattice(d, m) as lat2:
+        lat2.set_populations(F0)
+        lat2.step(10)
+        assert np.array_equal(lat2.get_populations(np.float32), a)
+
+
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S])
+def test_batch_equals_individual_lattices(storage):
+    members = []
+    for n in (48, 80):
+        d, m, F0 = cavity2d(n=n, u_lid=0.1, re=300, storage=storage)
+        members.append((d, m, F0))
+    d, m, F0 = cavity3d(n=(20, 14, 12), u_lid=0.05, omega=1.2, storage=storage)
+    members.append((d, m, F0))
+    dd = lb.make_desc(lb.D3Q27, lb.BGK, storage, (40, 16, 16), omega=1.6)
+    mm = lb.setup_duct3d(dd, 0.04, 11, 8, 8, 4)
+    solid = mm == 1
+    F0 = O.init_equilibrium(oracle_problem(dd, mm), rho=np.where(solid, 0.0, 1.0),
+                            u=np.concatenate([np.where(solid, 0.0, 0.04), np.zeros(2 * mm.size)]))
+    members.append((dd, mm, F0))
+    b = lb.Batch([x[0] for x in members], [x[1] for x in members])
+    for k, (_, _, F0) in enumerate(members):
+        b.set_populations(k, np.asarray(F0, dtype=np.float64))
+    b.step(37)
+    tx, nt = b.tile_info()
+    assert tx in (64, 128, 256) and nt > 0
+    for k, (d, m, F0) in enumerate(members):
+        with lb.Lattice(d, m) as lat:
+            lat.set_populations(np.asarray(F0, dtype=np.float64))
+            lat.step(37)
+            assert np.array_equal(b.get_populations(k, np.float32), lat.get_populations(np.float32)), k
+            r1, u1 = b.macros(k)
+            r2, u2 = lat.macros()
+            assert np.array_equal(u1, u2)
+    b.close()
+
+
+def test_duct3d_config_mode_parity():
+    dd = lb.make_desc(lb.D3Q27, lb.BGK, lb.F32, (48, 16, 16), omega=1.7)
+    mm = lb.setup_duct3d(dd, 0.04, 13, 8, 8, 4)
+    solid = mm == 1
+    F0 = O.init_equilibrium(oracle_problem(dd, mm), rho=np.where(solid, 0.0, 1.0),
+                            u=np.concatenate([np.where(solid, 0.0, 0.04), np.zeros(2 * mm.size)]))
+    with lb.Lattice(dd, mm) as lat:
+        lat.set_populations(F0)
+        lat.step(200)
+        F = lat.get_populations(np.float64)
+    Fo, _, _ = O.run(oracle_problem(dd, mm), F0, 200, dtype=np.float32)
+    assert rel_l2(F, Fo) < 1e-5
