@@ -280,11 +280,19 @@ def timed_steps(torch, lat, steps, dev):
     return e0.elapsed_time(e1) / 1e3
 
 
-def measure(torch, lb, args, storage, dev, world, sample_clocks=False):
+def build_workload(lb, args, storage):
     fn = WORKLOADS[args.workload][0]
-    d, m = fn(lb, storage)
+    if args.size and args.workload.startswith("d3q27"):
+        return fn(lb, storage, args.size)
+    return fn(lb, storage)
+
+
+def measure(torch, lb, args, storage, dev, world, sample_clocks=False):
+    d, m = build_workload(lb, args, storage)
     d.device = dev
     lat = lb.Lattice(d, m)
+    if args.block:
+        lat.set_block(args.block)
     lat.step(args.warmup if args.warmup > 0 else 1)   # includes the block-width autotune
     lat.sync()
     torch.cuda.synchronize(dev)
@@ -303,10 +311,11 @@ def measure(torch, lb, args, storage, dev, world, sample_clocks=False):
 def e2e_measure(torch, lb, args, storage, dev, world):
     """Through the public API with host buffers: pinned H2D of the start populations, K steps,
     D2H of the macroscopic fields, all inside the timed region."""
-    fn = WORKLOADS[args.workload][0]
-    d, m = fn(lb, storage)
+    d, m = build_workload(lb, args, storage)
     d.device = dev
     lat = lb.Lattice(d, m)
+    if args.block:
+        lat.set_block(args.block)
     N, Q = d.cells, d.q
     _, _, _, w, _ = lb.velocities(d.lattice)
     F_host = torch.empty(N * Q, dtype=torch.float32, pin_memory=True)
@@ -456,6 +465,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--size", type=int, default=0, help="cube side for D3Q27 workloads (default: the config's)")
+    ap.add_argument("--block", type=int, default=0, help="fixed block width (default: autotune)")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:
         raise SystemExit("steps must be >= 1 and warmup >= 0")

@@ -58,6 +58,16 @@ enum lbm_storage   { LBM_F32 = 0, LBM_F16S = 1, LBM_BF16S = 2, LBM_F64 = 3 };
  * with its equilibrium-moment table (:357-383).  GRAM_SCHMIDT: the same rows orthogonalised in order
  * (unweighted inner product over the 27 velocities), equilibrium moments = M * feq(rho,u).       */
 enum lbm_mrt_basis { LBM_MRT_REF = 0, LBM_MRT_GRAM_SCHMIDT = 1 };
+/* How the step arithmetic treats the populations.
+ * DEVIATION (default): every kernel computes on d_i = f_i - w_i (moments, equilibrium, MRT
+ *   transform); rho = 1 + sum d.  More accurate in FP32 than the reference: no cancellation of the
+ *   O(w) parts and no systematic density drift.  Required for F16S/BF16S storage.
+ * ABSOLUTE: the reference's arithmetic on the populations themselves (rho = sum f,
+ *   F = omega FEQ + (1 - omega) F_streamed, cpp/d2q9_bgk_lid.cpp:131-153), so FP32 results carry the
+ *   same rounding behaviour as the reference's FP32 runs.  BGK and Shan-Chen, F32 or F64 storage,
+ *   single lattices (MRT always uses DEVIATION: its factorised transform cannot reproduce the
+ *   rounding of the reference's dense FP32 GEMMs anyway).                                        */
+enum lbm_arithmetic { LBM_ARITH_DEVIATION = 0, LBM_ARITH_ABSOLUTE = 1 };
 /* Host buffer element type for population / field transfers. */
 enum lbm_dtype     { LBM_DTYPE_F32 = 0, LBM_DTYPE_F64 = 1 };
 /* Where a transfer buffer lives. */
@@ -93,6 +103,8 @@ typedef struct lbm_desc {
     int32_t collision;      /* enum lbm_collision                                             */
     int32_t storage;        /* enum lbm_storage                                               */
     int32_t mrt_basis;      /* enum lbm_mrt_basis (MRT only)                                  */
+    int32_t arithmetic;     /* enum lbm_arithmetic                                            */
+    int32_t reserved0;      /* 0                                                              */
     int64_t nx, ny, nz;     /* nz = 1 for D2Q9                                                */
     double omega;           /* BGK / Shan-Chen relaxation 1/tau                               */
     double mrt_s[27];       /* MRT relaxation rate per moment row (rust/examples/d3q27_mrt_lid.rs:122-150) */

@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(256) k_batch_bgk(const BatchLattice<typename C
     const BatchLattice<R>& p = lats[t.lat];
     const int x = t.x0 + threadIdx.x;
     if (x >= p.nx) return;
-    bgk_cell<L, S>(p, static_cast<const S*>(p.f[parity]), static_cast<S*>(p.f[parity ^ 1]), x, t.y, t.z);
+    bgk_cell<L, S, false>(p, static_cast<const S*>(p.f[parity]), static_cast<S*>(p.f[parity ^ 1]), x, t.y, t.z);
 }
 
 template <class T>
@@ -193,6 +193,8 @@ int lbm_batch_create(const lbm_desc* descs, int n, lbm_batch** out) {
         int rc = validate_desc(&descs[k]);
         if (rc) return rc;
         if (descs[k].collision != LBM_BGK) return set_error(LBM_ERR_UNSUPPORTED, "batched ensembles are BGK only");
+        if (descs[k].arithmetic != LBM_ARITH_DEVIATION)
+            return set_error(LBM_ERR_UNSUPPORTED, "batched ensembles use deviation arithmetic");
         if (descs[k].storage != descs[0].storage) return set_error(LBM_ERR_INVALID, "one storage type per batch");
         if (descs[k].device != descs[0].device) return set_error(LBM_ERR_INVALID, "one device per batch");
     }

@@ -6,6 +6,11 @@
 //   BF16S : bfloat16((f_i - w_i) * scale)
 // Shifting by the rest weight keeps only the deviation from rest in the 16-bit word; `scale`
 // (a power of two) lifts the small deviations out of the FP16 subnormal range.
+//
+// The step kernels compute on deviations d = f - w as well (load_dev / store_dev): for F32/F64 the
+// subtraction is exact for populations within a factor of two of their weight (Sterbenz), and
+// working on the small deviations avoids the cancellation of the O(w) parts in the moment sums and
+// transforms; for the 16-bit codecs the stored word already is the deviation.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -24,6 +29,8 @@ struct Codec<float> {
     static constexpr int kBytes = 4;
     __device__ __forceinline__ static float load(const float* p, float, float) { return __ldg(p); }
     __device__ __forceinline__ static void store(float* p, float v, float, float) { *p = v; }
+    __device__ __forceinline__ static float load_dev(const float* p, float w, float) { return __ldg(p) - w; }
+    __device__ __forceinline__ static void store_dev(float* p, float d, float w, float) { *p = w + d; }
 };
 
 template <>
@@ -32,6 +39,8 @@ struct Codec<double> {
     static constexpr int kBytes = 8;
     __device__ __forceinline__ static double load(const double* p, double, double) { return __ldg(p); }
     __device__ __forceinline__ static void store(double* p, double v, double, double) { *p = v; }
+    __device__ __forceinline__ static double load_dev(const double* p, double w, double) { return __ldg(p) - w; }
+    __device__ __forceinline__ static void store_dev(double* p, double d, double w, double) { *p = w + d; }
 };
 
 template <>
@@ -44,6 +53,12 @@ struct Codec<__half> {
     __device__ __forceinline__ static void store(__half* p, float v, float w, float scale) {
         *p = __float2half_rn((v - w) * scale);
     }
+    __device__ __forceinline__ static float load_dev(const __half* p, float, float inv_scale) {
+        return __half2float(__ldg(p)) * inv_scale;
+    }
+    __device__ __forceinline__ static void store_dev(__half* p, float d, float, float scale) {
+        *p = __float2half_rn(d * scale);
+    }
 };
 
 template <>
@@ -55,6 +70,12 @@ struct Codec<__nv_bfloat16> {
     }
     __device__ __forceinline__ static void store(__nv_bfloat16* p, float v, float w, float scale) {
         *p = __float2bfloat16_rn((v - w) * scale);
+    }
+    __device__ __forceinline__ static float load_dev(const __nv_bfloat16* p, float, float inv_scale) {
+        return __bfloat162float(__ldg(p)) * inv_scale;
+    }
+    __device__ __forceinline__ static void store_dev(__nv_bfloat16* p, float d, float, float scale) {
+        *p = __float2bfloat16_rn(d * scale);
     }
 };
 

@@ -63,10 +63,12 @@ struct Rows {
     __device__ __forceinline__ long long src(int cy, int cz) const { return base[1 - cy][1 - cz]; }
 };
 
-// Pull gather of one cell.  x-wrap per thread; xs for c_x = +1 is x-1, for c_x = -1 it is x+1.
-template <class L, class S, class P, class R>
+// Pull gather of one cell.  ABS = false: deviations d_i = f_i - w_i; ABS = true: the populations
+// themselves.  x-wrap per thread; the source x of c_x = +1 is x-1 and of c_x = -1 is x+1
+// (af::shift: out[x] = in[x - c]).
+template <class L, class S, bool ABS, class P, class R>
 __device__ __forceinline__ void pull(const S* __restrict__ fin, const P& p, const Rows<L>& rows, int x,
-                                     R (&fs)[L::Q]) {
+                                     R (&d)[L::Q]) {
     const int xm = x == 0 ? p.nx - 1 : x - 1;
     const int xp = x == p.nx - 1 ? 0 : x + 1;
     static_for<L::Q>([&](auto I) {
@@ -74,55 +76,76 @@ __device__ __forceinline__ void pull(const S* __restrict__ fin, const P& p, cons
         constexpr int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
         const int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
         const long long idx = (long long)i * p.N + rows.src(cy, cz) + xs;
-        fs[i] = Codec<S>::load(fin + idx, R(L::w(i)), p.inv_scale);
+        if constexpr (ABS)
+            d[i] = Codec<S>::load(fin + idx, R(L::w(i)), R(p.inv_scale));
+        else
+            d[i] = Codec<S>::load_dev(fin + idx, R(L::w(i)), R(p.inv_scale));
     });
 }
 
 // Zero-gradient outlet: populations arriving from +x are taken from cell x-1's streamed state,
 // i.e. F_i(x - 1 - c_i) = F_i(x, y - cy, z - cz) for c_x = -1.
-template <class L, class S, class P, class R>
+template <class L, class S, bool ABS, class P, class R>
 __device__ __forceinline__ void pull_zerograd(const S* __restrict__ fin, const P& p, const Rows<L>& rows, int x,
-                                              R (&fs)[L::Q]) {
+                                              R (&d)[L::Q]) {
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
         if constexpr (L::cx(i) == -1) {
             const long long idx = (long long)i * p.N + rows.src(L::cy(i), L::cz(i)) + x;
-            fs[i] = Codec<S>::load(fin + idx, R(L::w(i)), p.inv_scale);
+            if constexpr (ABS)
+                d[i] = Codec<S>::load(fin + idx, R(L::w(i)), R(p.inv_scale));
+            else
+                d[i] = Codec<S>::load_dev(fin + idx, R(L::w(i)), R(p.inv_scale));
         }
     });
 }
 
-template <class L, class R>
-__device__ __forceinline__ void moments(const R (&fs)[L::Q], R& rho, R& ux, R& uy, R& uz) {
+// Moments (cpp/d2q9_bgk_lid.cpp:131-138): rho = sum f, j = sum c f, u = j / rho.  On deviations
+// sum d = rho - 1 and sum c d = j (sum c w = 0).  Both rho and drho = rho - 1 are returned.
+template <class L, bool ABS, class R>
+__device__ __forceinline__ void moments(const R (&v)[L::Q], R& rho, R& drho, R& ux, R& uy, R& uz) {
     R r = R(0), jx = R(0), jy = R(0), jz = R(0);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
-        r += fs[i];
-        if constexpr (L::cx(i) == 1) jx += fs[i];
-        if constexpr (L::cx(i) == -1) jx -= fs[i];
-        if constexpr (L::cy(i) == 1) jy += fs[i];
-        if constexpr (L::cy(i) == -1) jy -= fs[i];
-        if constexpr (L::cz(i) == 1) jz += fs[i];
-        if constexpr (L::cz(i) == -1) jz -= fs[i];
+        r += v[i];
+        if constexpr (L::cx(i) == 1) jx += v[i];
+        if constexpr (L::cx(i) == -1) jx -= v[i];
+        if constexpr (L::cy(i) == 1) jy += v[i];
+        if constexpr (L::cy(i) == -1) jy -= v[i];
+        if constexpr (L::cz(i) == 1) jz += v[i];
+        if constexpr (L::cz(i) == -1) jz -= v[i];
     });
-    rho = r;
-    ux = jx / r;
-    uy = jy / r;
-    uz = L::DIM == 3 ? jz / r : R(0);
+    if constexpr (ABS) {
+        rho = r;
+        drho = r - R(1);
+    } else {
+        drho = r;
+        rho = R(1) + r;
+    }
+    ux = jx / rho;
+    uy = jy / rho;
+    uz = L::DIM == 3 ? jz / rho : R(0);
 }
 
+// The reference's boundary overwrites of DENSITY/UX/UY/UZ (cpp/d2q9_bgk_lid.cpp:141-146).
 template <class T, class R>
-__device__ __forceinline__ void apply_class(const ClassTable<T>& ct, int cls, uint32_t fl, R& rho, R& ux,
-                                            R& uy, R& uz, int dim) {
-    if (fl & kSetRho) rho = R(ct.rho[cls]);
+__device__ __forceinline__ void apply_class(const ClassTable<T>& ct, int cls, uint32_t fl, R& rho, R& drho,
+                                            R& ux, R& uy, R& uz, int dim) {
+    if (fl & kSetRho) {
+        rho = R(ct.rho[cls]);
+        drho = rho - R(1);
+    }
     if (fl & kSetUx) ux = R(ct.ux[cls]);
     if (fl & kSetUy) uy = R(ct.uy[cls]);
     if ((fl & kSetUz) && dim == 3) uz = R(ct.uz[cls]);
 }
 
-// feq_i = w_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2)   (cpp/d2q9_bgk_lid.cpp:151)
-template <class L, int I, class R>
-__device__ __forceinline__ R feq_i(R wrho, R base, R ux, R uy, R uz) {
+// Equilibrium of direction I (cpp/d2q9_bgk_lid.cpp:151):
+//   ABS:  feq_i       = w_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2)
+//   else: feq_i - w_i = w_i ((rho - 1) + rho (3 eu + 4.5 eu^2 - 1.5 u^2))
+// usq15 = 1.5 |u|^2.
+template <class L, int I, bool ABS, class R>
+__device__ __forceinline__ R feq_i(R rho, R drho, R usq15, R ux, R uy, R uz) {
     constexpr int cx = L::cx(I), cy = L::cy(I), cz = L::cz(I);
     R eu = R(0);
     if constexpr (cx == 1) eu = eu + ux;
@@ -131,23 +154,40 @@ __device__ __forceinline__ R feq_i(R wrho, R base, R ux, R uy, R uz) {
     if constexpr (cy == -1) eu = eu - uy;
     if constexpr (cz == 1) eu = eu + uz;
     if constexpr (cz == -1) eu = eu - uz;
-    return wrho * (base + eu * (R(3) + R(4.5) * eu));
+    if constexpr (ABS)
+        return (R(L::w(I)) * rho) * ((R(1) - usq15) + eu * (R(3) + R(4.5) * eu));
+    else
+        return R(L::w(I)) * (drho + rho * (eu * (R(3) + R(4.5) * eu) - usq15));
 }
 
-template <class L, class R>
-__device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R (&feq)[L::Q]) {
-    const R base = R(1) - R(1.5) * (ux * ux + uy * uy + uz * uz);
+template <class L, bool ABS, class R>
+__device__ __forceinline__ void equilibrium_v(R rho, R drho, R ux, R uy, R uz, R (&feq)[L::Q]) {
+    const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
-        feq[i] = feq_i<L, i>(R(L::w(i)) * rho, base, ux, uy, uz);
+        feq[i] = feq_i<L, i, ABS>(rho, drho, usq15, ux, uy, uz);
     });
 }
 
-template <class L, class S, class P, class R>
+// feq_i = w_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2) (absolute values, used to initialise)
+template <class L, class R>
+__device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R (&feq)[L::Q]) {
+    R dev[L::Q];
+    equilibrium_v<L, false>(rho, rho - R(1), ux, uy, uz, dev);
+    static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        feq[i] = R(L::w(i)) + dev[i];
+    });
+}
+
+template <class L, class S, bool ABS, class P, class R>
 __device__ __forceinline__ void store_cell(S* __restrict__ fout, const P& p, long long c, const R (&out)[L::Q]) {
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
-        Codec<S>::store(fout + (long long)i * p.N + c, out[i], R(L::w(i)), p.scale);
+        if constexpr (ABS)
+            Codec<S>::store(fout + (long long)i * p.N + c, out[i], R(L::w(i)), R(p.scale));
+        else
+            Codec<S>::store_dev(fout + (long long)i * p.N + c, out[i], R(L::w(i)), R(p.scale));
     });
 }
 
@@ -159,49 +199,55 @@ __device__ __forceinline__ void cell_class(const uint8_t* __restrict__ mask, con
 }
 
 // ---- BGK ---------------------------------------------------------------------------------
-// One cell of a BGK step.  P supplies mask, cls, nx, ny, nz, N, omega, one_m_omega, scale and
-// inv_scale (StepParams for one lattice, BatchLattice for one member of an ensemble).
-template <class L, class S, class P>
+// One cell of a BGK step: F = omega FEQ + (1 - omega) F_streamed (cpp/d2q9_bgk_lid.cpp:153), on
+// the populations (ABS) or with w_i subtracted on both sides (deviation arithmetic).
+// P supplies mask, cls, nx, ny, nz, N, omega, one_m_omega, scale and inv_scale (StepParams for one
+// lattice, BatchLattice for one member of an ensemble).
+template <class L, class S, bool ABS, class P>
 __device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, S* __restrict__ fout, int x, int y,
                                          int z) {
     using R = typename Codec<S>::Real;
     const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
     const long long c = rows.base[1][1] + x;
-    R fs[L::Q];
-    pull<L, S>(fin, p, rows, x, fs);
+    R v[L::Q];
+    pull<L, S, ABS>(fin, p, rows, x, v);
     int cls;
     uint32_t fl;
     cell_class(p.mask, p.cls, c, cls, fl);
-    if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
-    R rho, ux, uy, uz;
-    moments<L, R>(fs, rho, ux, uy, uz);
-    if (fl) apply_class(p.cls, cls, fl, rho, ux, uy, uz, L::DIM);
+    if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+    R rho, drho, ux, uy, uz;
+    moments<L, ABS>(v, rho, drho, ux, uy, uz);
+    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
     R out[L::Q];
-    const R base = R(1) - R(1.5) * (ux * ux + uy * uy + uz * uz);
+    const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
     const R omega = R(p.omega), one_m = R(p.one_m_omega);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
-        const R fe = feq_i<L, i>(R(L::w(i)) * rho, base, ux, uy, uz);
-        out[i] = (fl & kEquilibrium) ? fe : omega * fe + one_m * fs[i];
+        const R fe = feq_i<L, i, ABS>(rho, drho, usq15, ux, uy, uz);
+        out[i] = (fl & kEquilibrium) ? fe : omega * fe + one_m * v[i];
     });
     if (fl & kBounce) {
+        // F(REFLECTED) = BOUNCEDBACK (cpp/d2q9_bgk_lid.cpp:155); w_opp(i) = w_i
         static_for<L::Q - 1>([&](auto I) {
             constexpr int i = I + 1;
-            out[L::opp(i)] = fs[i];
+            out[L::opp(i)] = v[i];
         });
     }
-    store_cell<L, S>(fout, p, c, out);
+    store_cell<L, S, ABS>(fout, p, c, out);
 }
 
-template <class L, class S>
+template <class L, class S, bool ABS>
 __global__ void __launch_bounds__(512) k_step_bgk(StepParams<typename Codec<S>::Real> p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
-    bgk_cell<L, S>(p, static_cast<const S*>(p.fin), static_cast<S*>(p.fout), x, blockIdx.y, blockIdx.z);
+    bgk_cell<L, S, ABS>(p, static_cast<const S*>(p.fin), static_cast<S*>(p.fout), x, blockIdx.y, blockIdx.z);
 }
 
 // ---- MRT (D3Q27) -------------------------------------------------------------------------
-template <int BASIS, class S>
+// With deviation arithmetic the transform acts on d = f - w: M d = M f - M w, and M w = meq(rho = 1,
+// u = 0) for both bases, so the relaxation m* = m - S (m - meq) carries over with every equilibrium
+// moment replaced by its deviation from rest, i.e. the cell quantity rho replaced by rho - 1.
+template <int BASIS, class S, bool ABS>
 __global__ void __launch_bounds__(256) k_step_mrt(StepParams<typename Codec<S>::Real> p) {
     using L = D3Q27;
     using R = typename Codec<S>::Real;
@@ -211,25 +257,28 @@ __global__ void __launch_bounds__(256) k_step_mrt(StepParams<typename Codec<S>::
     const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
     const long long c = rows.base[1][1] + x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
-    R fs[27];
-    pull<L, S>(fin, p, rows, x, fs);
+    R T[27];
     int cls;
     uint32_t fl;
-    cell_class(p.mask, p.cls, c, cls, fl);
-    if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
-    // populations -> tensor slots (a register renaming)
-    R T[27];
-    static_for<27>([&](auto I) {
-        constexpr int i = I;
-        T[L::slot(i)] = fs[i];
-    });
+    {
+        R v[27];
+        pull<L, S, ABS>(fin, p, rows, x, v);
+        cell_class(p.mask, p.cls, c, cls, fl);
+        if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+        // populations -> tensor slots (a register renaming)
+        static_for<27>([&](auto I) {
+            constexpr int i = I;
+            T[L::slot(i)] = v[i];
+        });
+    }
     mrt_forward<BASIS>(T);
-    R rho = T[0];
+    R rho = ABS ? T[0] : R(1) + T[0];
+    R drho = ABS ? T[0] - R(1) : T[0];
     const R inv = R(1) / rho;
     R ux = T[1] * inv, uy = T[3] * inv, uz = T[9] * inv;
-    if (fl) apply_class(p.cls, cls, fl, rho, ux, uy, uz, 3);
+    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 3);
     R q[11];
-    q[0] = rho;
+    q[0] = ABS ? rho : drho;
     q[1] = rho * ux;
     q[2] = rho * uy;
     q[3] = rho * uz;
@@ -248,23 +297,24 @@ __global__ void __launch_bounds__(256) k_step_mrt(StepParams<typename Codec<S>::
         out[i] = T[L::slot(i)];
     });
     if (fl & (kEquilibrium | kBounce)) {
-        if (fl & kEquilibrium) equilibrium<L, R>(rho, ux, uy, uz, out);
+        if (fl & kEquilibrium) equilibrium_v<L, ABS>(rho, drho, ux, uy, uz, out);
         if (fl & kBounce) {
             // reload the streamed populations (the transform overwrote them in place)
-            pull<L, S>(fin, p, rows, x, fs);
-            if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
+            R v[27];
+            pull<L, S, ABS>(fin, p, rows, x, v);
+            if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
             static_for<26>([&](auto I) {
                 constexpr int i = I + 1;
-                out[L::opp(i)] = fs[i];
+                out[L::opp(i)] = v[i];
             });
         }
     }
-    store_cell<L, S>(static_cast<S*>(p.fout), p, c, out);
+    store_cell<L, S, ABS>(static_cast<S*>(p.fout), p, c, out);
 }
 
 // ---- Shan-Chen (D2Q9) --------------------------------------------------------------------
 // Pass 1: psi = 1 - exp(-rho) of the streamed density of every cell.
-template <class S>
+template <class S, bool ABS>
 __global__ void __launch_bounds__(512) k_sc_psi(StepParams<typename Codec<S>::Real> p) {
     using L = D2Q9;
     using R = typename Codec<S>::Real;
@@ -274,14 +324,15 @@ __global__ void __launch_bounds__(512) k_sc_psi(StepParams<typename Codec<S>::Re
     const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
     const long long c = rows.base[1][1] + x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
-    R fs[9];
-    pull<L, S>(fin, p, rows, x, fs);
+    R v[9];
+    pull<L, S, ABS>(fin, p, rows, x, v);
     int cls;
     uint32_t fl;
     cell_class(p.mask, p.cls, c, cls, fl);
-    if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
-    R rho = R(0);
-    static_for<9>([&](auto I) { rho += fs[I]; });
+    if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+    R sum = R(0);
+    static_for<9>([&](auto I) { sum += v[I]; });
+    R rho = ABS ? sum : R(1) + sum;
     if (fl & kSetRho) rho = R(p.cls.rho[cls]);
     p.psi[c] = R(1) - exp(-rho);
 }
@@ -310,7 +361,7 @@ __device__ __forceinline__ void sc_force(const StepParams<R>& p, const Rows<D2Q9
     Fy = g * sy;
 }
 
-template <class S>
+template <class S, bool ABS>
 __global__ void __launch_bounds__(512) k_step_sc(StepParams<typename Codec<S>::Real> p) {
     using L = D2Q9;
     using R = typename Codec<S>::Real;
@@ -320,17 +371,18 @@ __global__ void __launch_bounds__(512) k_step_sc(StepParams<typename Codec<S>::R
     const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
     const long long c = rows.base[1][1] + x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
-    R fs[9];
-    pull<L, S>(fin, p, rows, x, fs);
+    R v[9];
+    pull<L, S, ABS>(fin, p, rows, x, v);
     int cls;
     uint32_t fl;
     cell_class(p.mask, p.cls, c, cls, fl);
-    if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
-    R rho, ux, uy, uz;
-    moments<L, R>(fs, rho, ux, uy, uz);
-    if (fl) apply_class(p.cls, cls, fl, rho, ux, uy, uz, 2);
+    if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+    R rho, drho, ux, uy, uz;
+    moments<L, ABS>(v, rho, drho, ux, uy, uz);
+    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 2);
     R Fx, Fy;
     sc_force(p, rows, x, c, Fx, Fy);
+    // velocity shift u_eq = u + tau F / rho (Shan & Chen 1993)
     R vx = ux, vy = uy;
     if (rho > R(0)) {
         const R k = R(1) / (p.omega * rho);
@@ -338,19 +390,19 @@ __global__ void __launch_bounds__(512) k_step_sc(StepParams<typename Codec<S>::R
         vy = uy + Fy * k;
     }
     R out[9];
-    const R base = R(1) - R(1.5) * (vx * vx + vy * vy);
+    const R usq15 = R(1.5) * (vx * vx + vy * vy);
     static_for<9>([&](auto I) {
         constexpr int i = I;
-        const R fe = feq_i<L, i>(R(L::w(i)) * rho, base, vx, vy, R(0));
-        out[i] = (fl & kEquilibrium) ? fe : p.omega * fe + p.one_m_omega * fs[i];
+        const R fe = feq_i<L, i, ABS>(rho, drho, usq15, vx, vy, R(0));
+        out[i] = (fl & kEquilibrium) ? fe : p.omega * fe + p.one_m_omega * v[i];
     });
     if (fl & kBounce) {
         static_for<8>([&](auto I) {
             constexpr int i = I + 1;
-            out[L::opp(i)] = fs[i];
+            out[L::opp(i)] = v[i];
         });
     }
-    store_cell<L, S>(static_cast<S*>(p.fout), p, c, out);
+    store_cell<L, S, ABS>(static_cast<S*>(p.fout), p, c, out);
 }
 
 // ---- macroscopic fields ------------------------------------------------------------------
@@ -366,22 +418,22 @@ __global__ void k_macros(StepParams<typename Codec<S>::Real> p, int pulled, int 
     const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
     const long long c = rows.base[1][1] + x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
-    R fs[L::Q];
+    R d[L::Q];
     int cls;
     uint32_t fl;
     cell_class(p.mask, p.cls, c, cls, fl);
     if (pulled) {
-        pull<L, S>(fin, p, rows, x, fs);
-        if (fl & kZeroGradXp) pull_zerograd<L, S>(fin, p, rows, x, fs);
+        pull<L, S, false>(fin, p, rows, x, d);
+        if (fl & kZeroGradXp) pull_zerograd<L, S, false>(fin, p, rows, x, d);
     } else {
         static_for<L::Q>([&](auto I) {
             constexpr int i = I;
-            fs[i] = Codec<S>::load(fin + (long long)i * p.N + c, R(L::w(i)), p.inv_scale);
+            d[i] = Codec<S>::load_dev(fin + (long long)i * p.N + c, R(L::w(i)), p.inv_scale);
         });
     }
-    R rho, ux, uy, uz;
-    moments<L, R>(fs, rho, ux, uy, uz);
-    if (pulled && fl) apply_class(p.cls, cls, fl, rho, ux, uy, uz, L::DIM);
+    R rho, drho, ux, uy, uz;
+    moments<L, false>(d, rho, drho, ux, uy, uz);
+    if (pulled && fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
     if constexpr (L::DIM == 2) {
         if (pulled && collision == 2) {
             R Fx, Fy;

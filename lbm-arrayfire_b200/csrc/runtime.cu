@@ -28,18 +28,29 @@ __global__ void k_sums_final(const Sums* __restrict__ partial, int n, Sums* __re
 }
 
 // One plane of populations (direction i) from plain values to the storage codec and back.
+// The 16-bit codecs take the deviation in the caller's precision, so an FP64 source is rounded once.
 template <class S, class In>
 __global__ void k_encode_plane(const In* __restrict__ src, S* __restrict__ dst, long long n, double w, double scale) {
     using R = typename Codec<S>::Real;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-        Codec<S>::store(dst + k, R(src[k]), R(w), R(scale));
+    constexpr bool kShifted = Codec<S>::kBytes == 2;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        if constexpr (kShifted)
+            Codec<S>::store_dev(dst + k, R(src[k] - In(w)), R(w), R(scale));
+        else
+            Codec<S>::store(dst + k, R(src[k]), R(w), R(scale));
+    }
 }
 template <class S, class Out>
 __global__ void k_decode_plane(const S* __restrict__ src, Out* __restrict__ dst, long long n, double w,
                                double inv_scale) {
     using R = typename Codec<S>::Real;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-        dst[k] = Out(Codec<S>::load(src + k, R(w), R(inv_scale)));
+    constexpr bool kShifted = Codec<S>::kBytes == 2;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        if constexpr (kShifted)
+            dst[k] = Out(w) + Out(Codec<S>::load_dev(src + k, R(w), R(inv_scale)));
+        else
+            dst[k] = Out(Codec<S>::load(src + k, R(w), R(inv_scale)));
+    }
 }
 
 // F = feq(rho, u) for every cell; rho/u may be null (1 and 0).
@@ -178,22 +189,35 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
         StepParams<R> p = params_of<R>(c);
         p.fin = c->f[from];
         p.fout = c->f[from ^ 1];
+        const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
         switch (c->d.collision) {
             case LBM_BGK:
-                if (c->d.lattice == LBM_D2Q9)
-                    k_step_bgk<D2Q9, S><<<grid, blk, 0, s>>>(p);
-                else
-                    k_step_bgk<D3Q27, S><<<grid, blk, 0, s>>>(p);
+                if (c->d.lattice == LBM_D2Q9) {
+                    if (abs_arith)
+                        k_step_bgk<D2Q9, S, true><<<grid, blk, 0, s>>>(p);
+                    else
+                        k_step_bgk<D2Q9, S, false><<<grid, blk, 0, s>>>(p);
+                } else {
+                    if (abs_arith)
+                        k_step_bgk<D3Q27, S, true><<<grid, blk, 0, s>>>(p);
+                    else
+                        k_step_bgk<D3Q27, S, false><<<grid, blk, 0, s>>>(p);
+                }
                 break;
-            case LBM_MRT:
+            case LBM_MRT:  // deviation arithmetic only (validate_desc)
                 if (c->d.mrt_basis == LBM_MRT_REF)
-                    k_step_mrt<kMrtRef, S><<<grid, blk, 0, s>>>(p);
+                    k_step_mrt<kMrtRef, S, false><<<grid, blk, 0, s>>>(p);
                 else
-                    k_step_mrt<kMrtGramSchmidt, S><<<grid, blk, 0, s>>>(p);
+                    k_step_mrt<kMrtGramSchmidt, S, false><<<grid, blk, 0, s>>>(p);
                 break;
             default:
-                k_sc_psi<S><<<grid, blk, 0, s>>>(p);
-                k_step_sc<S><<<grid, blk, 0, s>>>(p);
+                if (abs_arith) {
+                    k_sc_psi<S, true><<<grid, blk, 0, s>>>(p);
+                    k_step_sc<S, true><<<grid, blk, 0, s>>>(p);
+                } else {
+                    k_sc_psi<S, false><<<grid, blk, 0, s>>>(p);
+                    k_step_sc<S, false><<<grid, blk, 0, s>>>(p);
+                }
                 break;
         }
     });

@@ -47,6 +47,12 @@ int validate_desc(const lbm_desc* d) {
         return set_error(LBM_ERR_UNSUPPORTED, "Shan-Chen is built for D2Q9 only");
     if (d->collision == LBM_MRT && d->mrt_basis != LBM_MRT_REF && d->mrt_basis != LBM_MRT_GRAM_SCHMIDT)
         return set_error(LBM_ERR_INVALID, "unknown MRT basis");
+    if (d->arithmetic != LBM_ARITH_DEVIATION && d->arithmetic != LBM_ARITH_ABSOLUTE)
+        return set_error(LBM_ERR_INVALID, "unknown arithmetic mode");
+    if (d->arithmetic == LBM_ARITH_ABSOLUTE && d->storage != LBM_F32 && d->storage != LBM_F64)
+        return set_error(LBM_ERR_UNSUPPORTED, "absolute arithmetic needs F32 or F64 storage");
+    if (d->arithmetic == LBM_ARITH_ABSOLUTE && d->collision == LBM_MRT)
+        return set_error(LBM_ERR_UNSUPPORTED, "MRT runs in deviation arithmetic only");
     if (d->nx < 1 || d->ny < 1 || d->nz < 1) return set_error(LBM_ERR_INVALID, "lattice extents must be >= 1");
     if (d->lattice == LBM_D2Q9 && d->nz != 1) return set_error(LBM_ERR_INVALID, "D2Q9 needs nz == 1");
     if (d->nx > 0x7fffffffLL || d->ny > 65535 || d->nz > 65535)

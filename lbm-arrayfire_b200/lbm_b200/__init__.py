@@ -32,6 +32,7 @@ D2Q9, D3Q27 = 0, 1
 BGK, MRT, SHANCHEN = 0, 1, 2
 F32, F16S, BF16S, F64 = 0, 1, 2, 3
 MRT_REF, MRT_GRAM_SCHMIDT = 0, 1
+ARITH_DEVIATION, ARITH_ABSOLUTE = 0, 1
 DTYPE_F32, DTYPE_F64 = 0, 1
 HOST, DEVICE = 0, 1
 BOUNCE, SET_RHO, SET_UX, SET_UY, SET_UZ, EQUILIBRIUM, ZEROGRAD_XP = 1, 2, 4, 8, 16, 32, 64
@@ -55,6 +56,7 @@ class CellClass(C.Structure):
 class Desc(C.Structure):
     _fields_ = [
         ("lattice", C.c_int32), ("collision", C.c_int32), ("storage", C.c_int32), ("mrt_basis", C.c_int32),
+        ("arithmetic", C.c_int32), ("reserved0", C.c_int32),
         ("nx", C.c_int64), ("ny", C.c_int64), ("nz", C.c_int64),
         ("omega", C.c_double), ("mrt_s", C.c_double * 27), ("sc_G", C.c_double),
         ("storage_scale", C.c_double), ("n_classes", C.c_int32), ("device", C.c_int32),
@@ -187,11 +189,13 @@ def mrt_rates(sv: float, other: float) -> np.ndarray:
 
 
 def make_desc(lattice: int, collision: int, storage: int, shape, *, omega: float = 1.0, mrt_s=None,
-              mrt_basis: int = MRT_REF, sc_G: float = 0.0, storage_scale: float = 0.0, device: int = 0) -> Desc:
+              mrt_basis: int = MRT_REF, sc_G: float = 0.0, storage_scale: float = 0.0, device: int = 0,
+              arithmetic: int = ARITH_DEVIATION) -> Desc:
     d = Desc()
     nx, ny = int(shape[0]), int(shape[1])
     nz = int(shape[2]) if len(shape) > 2 else 1
     lib().lbm_desc_init(C.byref(d), lattice, collision, storage, nx, ny, nz)
+    d.arithmetic = arithmetic
     d.omega = omega
     if mrt_s is not None:
         for i, v in enumerate(mrt_s):

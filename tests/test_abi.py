@@ -154,6 +154,12 @@ def test_descriptor_validation_precedes_device():
     d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (8, 8))
     d.classes[0].flags = 0x100
     bad.append((d, -1))
+    d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (8, 8), arithmetic=7)
+    bad.append((d, -1))
+    d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F16S, (8, 8), arithmetic=lb.ARITH_ABSOLUTE)
+    bad.append((d, -5))
+    d = lb.make_desc(lb.D3Q27, lb.MRT, lb.F32, (8, 8, 8), arithmetic=lb.ARITH_ABSOLUTE)
+    bad.append((d, -5))
     for desc, code in bad:
         h = C.c_void_p()
         assert lb.lib().lbm_create(C.byref(desc), C.byref(h)) == code
