@@ -166,6 +166,25 @@ int   lbm_get_desc(const lbm_ctx* c, lbm_desc* out);
 int   lbm_set_block(lbm_ctx* c, int threads_x);
 int   lbm_get_block(const lbm_ctx* c);
 
+/* ---- conservation sums without allocation -----------------------------------------------
+ * No counterpart in the reference.  For callers that cannot let a library call cudaMalloc or
+ * cudaFree — applications whose device memory belongs to another allocator (a framework's caching
+ * allocator, a pool reserved up front), where an extra cudaMalloc can fail or fragment the pool and a
+ * cudaFree synchronises the whole device.  Computes the same FP64 mass/momentum sums as
+ * lbm_sums_fp64, over a caller-owned population buffer on the current device (the engine's storage
+ * format and layout, e.g. from lbm_device_populations), with no allocation of any kind: the scratch
+ * (one partial per block + the result) is a fixed array in the library's device image, held by every
+ * GPU that loads the library until the process exits (640 KB).
+ *  - At most LBM_NOALLOC_MAX_CELLS cells; larger lattices are rejected with LBM_ERR_INVALID.
+ *  - The first call on each device looks up the array's device address (cudaGetSymbolAddress); make
+ *    that first call before any stream capture.
+ *  - Every call shares the one array, so calls that overlap on the GPU (other host threads, other
+ *    streams) race; serialise them.  The call synchronises `stream` (a cudaStream_t, NULL = default).
+ *  - Returns LBM_ERR_DIVERGED when a population is NaN or Inf (out is still filled).              */
+#define LBM_NOALLOC_MAX_CELLS 67108864LL
+int  lbm_sums_fp64_noalloc(const void* populations, int lattice, int storage, int64_t nx, int64_t ny,
+                           int64_t nz, double storage_scale, void* stream, double out[4]);
+
 /* ---- batched ensemble -------------------------------------------------------------------
  * Many independent lattices (any mix of D2Q9/D3Q27 BGK, sizes and rates, one storage type)
  * advanced by one kernel launch per step over a tile table; nsteps of those are captured in a

@@ -108,6 +108,7 @@ _SIGS = {
     "lbm_get_desc": (C.c_int, [_P, _DP]),
     "lbm_set_block": (C.c_int, [_P, C.c_int]),
     "lbm_get_block": (C.c_int, [_P]),
+    "lbm_sums_fp64_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_double, _P, _P]),
     "lbm_batch_create": (C.c_int, [_DP, C.c_int, C.POINTER(_P)]),
     "lbm_batch_destroy": (None, [_P]),
     "lbm_batch_size": (C.c_int, [_P]),
