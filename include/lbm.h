@@ -47,6 +47,7 @@ extern "C" {
 #define LBM_ERR_UNSUPPORTED (-5) /* combination not built (e.g. MRT on D2Q9) */
 #define LBM_ERR_NO_DEVICE  (-6)  /* no CUDA device / not an sm_100 device */
 #define LBM_ERR_STATE      (-7)  /* call not valid in the current state */
+#define LBM_ERR_TIMEOUT    (-8)  /* a bounded device-side wait gave up (the step kernel returned early) */
 
 /* ---- enumerations ---------------------------------------------------------------------- */
 enum lbm_lattice   { LBM_D2Q9 = 0, LBM_D3Q27 = 1 };
@@ -143,6 +144,7 @@ int  lbm_get_populations(lbm_ctx* c, void* dst, int dtype, int memory);
 int  lbm_init_equilibrium(lbm_ctx* c, const double* rho, const double* u);
 /* Advance nsteps time steps, asynchronously on the context stream. */
 int  lbm_step(lbm_ctx* c, int64_t nsteps);
+/* Wait for the context's stream; returns LBM_ERR_TIMEOUT if a step kernel gave up a bounded wait. */
 int  lbm_sync(lbm_ctx* c);
 /* Macroscopic fields the last step's collision used, after the class overwrites (the reference's
  * DENSITY / UX / UY / UZ after an iteration).  Before any step: moments of the current populations.
@@ -165,6 +167,13 @@ int   lbm_get_desc(const lbm_ctx* c, lbm_desc* out);
 /* Block width (threads along x) used by the step kernel; 0 = autotune on first step. */
 int   lbm_set_block(lbm_ctx* c, int threads_x);
 int   lbm_get_block(const lbm_ctx* c);
+/* Step-kernel family.  PLAIN: one thread per cell, populations read straight from HBM.  ROWS
+ * (D3Q27 BGK/MRT, deviation arithmetic, F32/F16S/BF16S, nx in {128, 256, 512}): whole rows staged in
+ * shared memory by bulk copies (TMA) through an mbarrier ring.  AUTO (default): the autotuner times
+ * the eligible ones.  Both give bit-identical results.                                             */
+enum lbm_kernel { LBM_KERNEL_AUTO = 0, LBM_KERNEL_PLAIN = 1, LBM_KERNEL_ROWS = 2 };
+int   lbm_set_kernel(lbm_ctx* c, int kind);
+int   lbm_get_kernel(const lbm_ctx* c);              /* the family in use (PLAIN or ROWS), or AUTO before the first step */
 
 /* ---- conservation sums without allocation -----------------------------------------------
  * No counterpart in the reference.  For callers that cannot let a library call cudaMalloc or

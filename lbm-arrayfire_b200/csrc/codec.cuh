@@ -11,6 +11,8 @@
 // subtraction is exact for populations within a factor of two of their weight (Sterbenz), and
 // working on the small deviations avoids the cancellation of the O(w) parts in the moment sums and
 // transforms; for the 16-bit codecs the stored word already is the deviation.
+// load/load_dev read global memory through the read-only path (__ldg); dev() decodes a value that
+// was read by other means (e.g. from shared memory, which __ldg must not be given).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -29,6 +31,7 @@ struct Codec<float> {
     static constexpr int kBytes = 4;
     __device__ __forceinline__ static float load(const float* p, float, float) { return __ldg(p); }
     __device__ __forceinline__ static void store(float* p, float v, float, float) { *p = v; }
+    __device__ __forceinline__ static float dev(float raw, float w, float) { return raw - w; }
     __device__ __forceinline__ static float load_dev(const float* p, float w, float) { return __ldg(p) - w; }
     __device__ __forceinline__ static void store_dev(float* p, float d, float w, float) { *p = w + d; }
 };
@@ -39,6 +42,7 @@ struct Codec<double> {
     static constexpr int kBytes = 8;
     __device__ __forceinline__ static double load(const double* p, double, double) { return __ldg(p); }
     __device__ __forceinline__ static void store(double* p, double v, double, double) { *p = v; }
+    __device__ __forceinline__ static double dev(double raw, double w, double) { return raw - w; }
     __device__ __forceinline__ static double load_dev(const double* p, double w, double) { return __ldg(p) - w; }
     __device__ __forceinline__ static void store_dev(double* p, double d, double w, double) { *p = w + d; }
 };
@@ -52,6 +56,9 @@ struct Codec<__half> {
     }
     __device__ __forceinline__ static void store(__half* p, float v, float w, float scale) {
         *p = __float2half_rn((v - w) * scale);
+    }
+    __device__ __forceinline__ static float dev(__half raw, float, float inv_scale) {
+        return __half2float(raw) * inv_scale;
     }
     __device__ __forceinline__ static float load_dev(const __half* p, float, float inv_scale) {
         return __half2float(__ldg(p)) * inv_scale;
@@ -70,6 +77,9 @@ struct Codec<__nv_bfloat16> {
     }
     __device__ __forceinline__ static void store(__nv_bfloat16* p, float v, float w, float scale) {
         *p = __float2bfloat16_rn((v - w) * scale);
+    }
+    __device__ __forceinline__ static float dev(__nv_bfloat16 raw, float, float inv_scale) {
+        return __bfloat162float(raw) * inv_scale;
     }
     __device__ __forceinline__ static float load_dev(const __nv_bfloat16* p, float, float inv_scale) {
         return __bfloat162float(__ldg(p)) * inv_scale;

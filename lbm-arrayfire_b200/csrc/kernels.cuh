@@ -140,12 +140,10 @@ __device__ __forceinline__ void apply_class(const ClassTable<T>& ct, int cls, ui
     if ((fl & kSetUz) && dim == 3) uz = R(ct.uz[cls]);
 }
 
-// Equilibrium of direction I (cpp/d2q9_bgk_lid.cpp:151):
-//   ABS:  feq_i       = w_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2)
-//   else: feq_i - w_i = w_i ((rho - 1) + rho (3 eu + 4.5 eu^2 - 1.5 u^2))
-// usq15 = 1.5 |u|^2.
-template <class L, int I, bool ABS, class R>
-__device__ __forceinline__ R feq_i(R rho, R drho, R usq15, R ux, R uy, R uz) {
+// Equilibrium of direction I in the reference's form (cpp/d2q9_bgk_lid.cpp:151), absolute values:
+//   feq_i = w_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2),   usq15 = 1.5 |u|^2
+template <class L, int I, class R>
+__device__ __forceinline__ R feq_abs_i(R rho, R usq15, R ux, R uy, R uz) {
     constexpr int cx = L::cx(I), cy = L::cy(I), cz = L::cz(I);
     R eu = R(0);
     if constexpr (cx == 1) eu = eu + ux;
@@ -154,26 +152,59 @@ __device__ __forceinline__ R feq_i(R rho, R drho, R usq15, R ux, R uy, R uz) {
     if constexpr (cy == -1) eu = eu - uy;
     if constexpr (cz == 1) eu = eu + uz;
     if constexpr (cz == -1) eu = eu - uz;
-    if constexpr (ABS)
-        return (R(L::w(I)) * rho) * ((R(1) - usq15) + eu * (R(3) + R(4.5) * eu));
-    else
-        return R(L::w(I)) * (drho + rho * (eu * (R(3) + R(4.5) * eu) - usq15));
+    return (R(L::w(I)) * rho) * ((R(1) - usq15) + eu * (R(3) + R(4.5) * eu));
+}
+
+// Deviation equilibrium feq_i - w_i = w_i ((rho - 1) + rho (4.5 eu^2 - 1.5 u^2)) +- w_i rho 3 eu,
+// evaluated once per pair of opposite directions: the symmetric part is shared and the
+// momentum-carrying part is exactly antisymmetric.
+template <class L, class R>
+__device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz, R (&fe)[L::Q]) {
+    const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
+    const R rho3 = R(3) * rho;
+    const R rho45 = R(4.5) * rho;
+    const R base = drho - rho * usq15;
+    static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int o = L::opp(i);
+        if constexpr (i == 0) {
+            fe[0] = R(L::w(0)) * base;
+        } else if constexpr (i < o) {
+            constexpr int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
+            R eu = R(0);
+            if constexpr (cx == 1) eu = eu + ux;
+            if constexpr (cx == -1) eu = eu - ux;
+            if constexpr (cy == 1) eu = eu + uy;
+            if constexpr (cy == -1) eu = eu - uy;
+            if constexpr (cz == 1) eu = eu + uz;
+            if constexpr (cz == -1) eu = eu - uz;
+            const R w = R(L::w(i));
+            const R sym = w * (base + rho45 * (eu * eu));
+            const R anti = w * (rho3 * eu);
+            fe[i] = sym + anti;
+            fe[o] = sym - anti;
+        }
+    });
 }
 
 template <class L, bool ABS, class R>
 __device__ __forceinline__ void equilibrium_v(R rho, R drho, R ux, R uy, R uz, R (&feq)[L::Q]) {
-    const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
-    static_for<L::Q>([&](auto I) {
-        constexpr int i = I;
-        feq[i] = feq_i<L, i, ABS>(rho, drho, usq15, ux, uy, uz);
-    });
+    if constexpr (ABS) {
+        const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
+        static_for<L::Q>([&](auto I) {
+            constexpr int i = I;
+            feq[i] = feq_abs_i<L, i>(rho, usq15, ux, uy, uz);
+        });
+    } else {
+        equilibrium_dev<L, R>(rho, drho, ux, uy, uz, feq);
+    }
 }
 
 // feq_i = w_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2) (absolute values, used to initialise)
 template <class L, class R>
 __device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R (&feq)[L::Q]) {
     R dev[L::Q];
-    equilibrium_v<L, false>(rho, rho - R(1), ux, uy, uz, dev);
+    equilibrium_dev<L, R>(rho, rho - R(1), ux, uy, uz, dev);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
         feq[i] = R(L::w(i)) + dev[i];
@@ -199,10 +230,33 @@ __device__ __forceinline__ void cell_class(const uint8_t* __restrict__ mask, con
 }
 
 // ---- BGK ---------------------------------------------------------------------------------
-// One cell of a BGK step: F = omega FEQ + (1 - omega) F_streamed (cpp/d2q9_bgk_lid.cpp:153), on
-// the populations (ABS) or with w_i subtracted on both sides (deviation arithmetic).
-// P supplies mask, cls, nx, ny, nz, N, omega, one_m_omega, scale and inv_scale (StepParams for one
-// lattice, BatchLattice for one member of an ensemble).
+// Collision of one cell from its streamed populations v (ABS) or deviations v = f - w:
+// F = omega FEQ + (1 - omega) F_streamed (cpp/d2q9_bgk_lid.cpp:153), the class overwrites before it
+// and the full-way bounce-back after it (:155).  P supplies cls, omega, one_m_omega.
+template <class L, bool ABS, class P, class R>
+__device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, const R (&v)[L::Q], R (&out)[L::Q]) {
+    R rho, drho, ux, uy, uz;
+    moments<L, ABS>(v, rho, drho, ux, uy, uz);
+    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
+    R fe[L::Q];
+    equilibrium_v<L, ABS>(rho, drho, ux, uy, uz, fe);
+    const R omega = R(p.omega), one_m = R(p.one_m_omega);
+    static_for<L::Q>([&](auto I) {
+        constexpr int i = I;
+        out[i] = (fl & kEquilibrium) ? fe[i] : omega * fe[i] + one_m * v[i];
+    });
+    if (fl & kBounce) {
+        // F(REFLECTED) = BOUNCEDBACK; w_opp(i) = w_i, so deviations bounce like populations
+        static_for<L::Q - 1>([&](auto I) {
+            constexpr int i = I + 1;
+            out[L::opp(i)] = v[i];
+        });
+    }
+}
+
+// One cell of a BGK step read from and written to global memory.  P supplies mask, cls, nx, ny,
+// nz, N, omega, one_m_omega, scale and inv_scale (StepParams for one lattice, BatchLattice for one
+// member of an ensemble).
 template <class L, class S, bool ABS, class P>
 __device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, S* __restrict__ fout, int x, int y,
                                          int z) {
@@ -215,24 +269,8 @@ __device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, 
     uint32_t fl;
     cell_class(p.mask, p.cls, c, cls, fl);
     if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
-    R rho, drho, ux, uy, uz;
-    moments<L, ABS>(v, rho, drho, ux, uy, uz);
-    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
     R out[L::Q];
-    const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
-    const R omega = R(p.omega), one_m = R(p.one_m_omega);
-    static_for<L::Q>([&](auto I) {
-        constexpr int i = I;
-        const R fe = feq_i<L, i, ABS>(rho, drho, usq15, ux, uy, uz);
-        out[i] = (fl & kEquilibrium) ? fe : omega * fe + one_m * v[i];
-    });
-    if (fl & kBounce) {
-        // F(REFLECTED) = BOUNCEDBACK (cpp/d2q9_bgk_lid.cpp:155); w_opp(i) = w_i
-        static_for<L::Q - 1>([&](auto I) {
-            constexpr int i = I + 1;
-            out[L::opp(i)] = v[i];
-        });
-    }
+    bgk_collide<L, ABS>(p, cls, fl, v, out);
     store_cell<L, S, ABS>(fout, p, c, out);
 }
 
@@ -244,10 +282,43 @@ __global__ void __launch_bounds__(512) k_step_bgk(StepParams<typename Codec<S>::
 }
 
 // ---- MRT (D3Q27) -------------------------------------------------------------------------
-// With deviation arithmetic the transform acts on d = f - w: M d = M f - M w, and M w = meq(rho = 1,
-// u = 0) for both bases, so the relaxation m* = m - S (m - meq) carries over with every equilibrium
-// moment replaced by its deviation from rest, i.e. the cell quantity rho replaced by rho - 1.
-template <int BASIS, class S, bool ABS>
+// Collision of one cell in deviation arithmetic.  T enters with the streamed deviations in tensor
+// slot order (T[slot(i)] = f_i - w_i) and leaves with the post-collision deviations in direction
+// order in out[].  The transform acts on d = f - w: M d = M f - M w, and M w = meq(rho = 1, u = 0) for
+// both bases, so m* = m - S (m - meq) carries over with every equilibrium moment replaced by its
+// deviation from rest, i.e. the cell quantity rho replaced by rho - 1 (mrt.cuh).  Bounce-back is left
+// to the caller (it needs the streamed values, which the transform overwrote).
+template <int BASIS, class P, class R>
+__device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R (&T)[27], R (&out)[27]) {
+    using L = D3Q27;
+    mrt_forward<BASIS>(T);
+    R drho = T[0];
+    R rho = R(1) + drho;
+    const R inv = R(1) / rho;
+    R ux = T[1] * inv, uy = T[3] * inv, uz = T[9] * inv;
+    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 3);
+    R q[11];
+    q[0] = drho;
+    q[1] = rho * ux;
+    q[2] = rho * uy;
+    q[3] = rho * uz;
+    q[4] = q[1] * ux;
+    q[5] = q[2] * uy;
+    q[6] = q[3] * uz;
+    q[7] = q[1] * uy;
+    q[8] = q[1] * uz;
+    q[9] = q[2] * uz;
+    q[10] = ux * ux + uy * uy + uz * uz;
+    mrt_relax<BASIS>(T, q, p.mrt);
+    mrt_inverse<BASIS>(T);
+    static_for<27>([&](auto I) {
+        constexpr int i = I;
+        out[i] = T[L::slot(i)];
+    });
+    if (fl & kEquilibrium) equilibrium_dev<L, R>(rho, drho, ux, uy, uz, out);
+}
+
+template <int BASIS, class S>
 __global__ void __launch_bounds__(256) k_step_mrt(StepParams<typename Codec<S>::Real> p) {
     using L = D3Q27;
     using R = typename Codec<S>::Real;
@@ -262,54 +333,27 @@ __global__ void __launch_bounds__(256) k_step_mrt(StepParams<typename Codec<S>::
     uint32_t fl;
     {
         R v[27];
-        pull<L, S, ABS>(fin, p, rows, x, v);
+        pull<L, S, false>(fin, p, rows, x, v);
         cell_class(p.mask, p.cls, c, cls, fl);
-        if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
-        // populations -> tensor slots (a register renaming)
+        if (fl & kZeroGradXp) pull_zerograd<L, S, false>(fin, p, rows, x, v);
         static_for<27>([&](auto I) {
             constexpr int i = I;
             T[L::slot(i)] = v[i];
         });
     }
-    mrt_forward<BASIS>(T);
-    R rho = ABS ? T[0] : R(1) + T[0];
-    R drho = ABS ? T[0] - R(1) : T[0];
-    const R inv = R(1) / rho;
-    R ux = T[1] * inv, uy = T[3] * inv, uz = T[9] * inv;
-    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 3);
-    R q[11];
-    q[0] = ABS ? rho : drho;
-    q[1] = rho * ux;
-    q[2] = rho * uy;
-    q[3] = rho * uz;
-    q[4] = q[1] * ux;
-    q[5] = q[2] * uy;
-    q[6] = q[3] * uz;
-    q[7] = q[1] * uy;
-    q[8] = q[1] * uz;
-    q[9] = q[2] * uz;
-    q[10] = ux * ux + uy * uy + uz * uz;
-    mrt_relax<BASIS>(T, q, p.mrt);
-    mrt_inverse<BASIS>(T);
     R out[27];
-    static_for<27>([&](auto I) {
-        constexpr int i = I;
-        out[i] = T[L::slot(i)];
-    });
-    if (fl & (kEquilibrium | kBounce)) {
-        if (fl & kEquilibrium) equilibrium_v<L, ABS>(rho, drho, ux, uy, uz, out);
-        if (fl & kBounce) {
-            // reload the streamed populations (the transform overwrote them in place)
-            R v[27];
-            pull<L, S, ABS>(fin, p, rows, x, v);
-            if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
-            static_for<26>([&](auto I) {
-                constexpr int i = I + 1;
-                out[L::opp(i)] = v[i];
-            });
-        }
+    mrt_collide<BASIS>(p, cls, fl, T, out);
+    if (fl & kBounce) {
+        // reload the streamed deviations (the transform overwrote them in place)
+        R v[27];
+        pull<L, S, false>(fin, p, rows, x, v);
+        if (fl & kZeroGradXp) pull_zerograd<L, S, false>(fin, p, rows, x, v);
+        static_for<26>([&](auto I) {
+            constexpr int i = I + 1;
+            out[L::opp(i)] = v[i];
+        });
     }
-    store_cell<L, S, ABS>(static_cast<S*>(p.fout), p, c, out);
+    store_cell<L, S, false>(static_cast<S*>(p.fout), p, c, out);
 }
 
 // ---- Shan-Chen (D2Q9) --------------------------------------------------------------------
@@ -389,12 +433,12 @@ __global__ void __launch_bounds__(512) k_step_sc(StepParams<typename Codec<S>::R
         vx = ux + Fx * k;
         vy = uy + Fy * k;
     }
+    R fe[9];
+    equilibrium_v<L, ABS>(rho, drho, vx, vy, R(0), fe);
     R out[9];
-    const R usq15 = R(1.5) * (vx * vx + vy * vy);
     static_for<9>([&](auto I) {
         constexpr int i = I;
-        const R fe = feq_i<L, i, ABS>(rho, drho, usq15, vx, vy, R(0));
-        out[i] = (fl & kEquilibrium) ? fe : p.omega * fe + p.one_m_omega * v[i];
+        out[i] = (fl & kEquilibrium) ? fe[i] : p.omega * fe[i] + p.one_m_omega * v[i];
     });
     if (fl & kBounce) {
         static_for<8>([&](auto I) {

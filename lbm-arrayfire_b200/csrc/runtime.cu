@@ -11,6 +11,7 @@
 
 #include "internal.h"
 #include "kernels.cuh"
+#include "rowpipe.cuh"
 
 namespace lbm {
 
@@ -120,6 +121,10 @@ struct lbm_ctx {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     bool timed = false;
     int block = 0;
+    int kernel = LBM_KERNEL_AUTO;  // requested family
+    int kernel_used = 0;           // family chosen (PLAIN or ROWS); 0 before the first step
+    int rows_grid = 0;             // persistent grid of the row pipeline
+    int* err = nullptr;            // device error word of the row pipeline
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int gsteps = 0;
     bool has_prev = false;
@@ -180,8 +185,81 @@ StepParams<double>& params_of<double>(lbm_ctx* c) {
     return c->pd;
 }
 
+// ---- row pipeline (rowpipe.cuh) ------------------------------------------------------------
+static bool rows_eligible(const lbm_ctx* c) {
+    const lbm_desc& d = c->d;
+    return d.lattice == LBM_D3Q27 && (d.collision == LBM_BGK || d.collision == LBM_MRT) &&
+           d.arithmetic == LBM_ARITH_DEVIATION && d.storage != LBM_F64 &&
+           (d.nx == 128 || d.nx == 256 || d.nx == 512);
+}
+
+template <class S, int PITCH, int COLL>
+static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s) {
+    auto kern = k_step_rows<D3Q27, S, PITCH, COLL>;
+    constexpr size_t smem = rowpipe_smem_bytes<D3Q27, S, PITCH>();
+    kern<<<c->rows_grid, PITCH, smem, s>>>(p, c->err);
+}
+
+template <class S, int PITCH, int COLL>
+static int prepare_rows_t(lbm_ctx* c) {
+    auto kern = k_step_rows<D3Q27, S, PITCH, COLL>;
+    constexpr size_t smem = rowpipe_smem_bytes<D3Q27, S, PITCH>();
+    LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, sms = 0;
+    LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PITCH, smem));
+    LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->d.device));
+    if (per_sm < 1) return set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
+    const long long rows = c->d.ny * c->d.nz;
+    c->rows_grid = (int)std::min<long long>(rows, (long long)per_sm * sms);
+    return LBM_OK;
+}
+
+template <class F>
+static void dispatch_rows(const lbm_ctx* c, F&& f) {
+    const int coll = c->d.collision == LBM_BGK ? 0 : (c->d.mrt_basis == LBM_MRT_REF ? 1 : 2);
+    auto by_pitch = [&](auto st, auto co) {
+        switch (c->d.nx) {
+            case 128: f(st, co, std::integral_constant<int, 128>{}); break;
+            case 256: f(st, co, std::integral_constant<int, 256>{}); break;
+            default: f(st, co, std::integral_constant<int, 512>{}); break;
+        }
+    };
+    auto by_coll = [&](auto st) {
+        switch (coll) {
+            case 0: by_pitch(st, std::integral_constant<int, 0>{}); break;
+            case 1: by_pitch(st, std::integral_constant<int, 1>{}); break;
+            default: by_pitch(st, std::integral_constant<int, 2>{}); break;
+        }
+    };
+    switch (c->d.storage) {
+        case LBM_F32: by_coll(Tag<float>{}); break;
+        case LBM_F16S: by_coll(Tag<__half>{}); break;
+        default: by_coll(Tag<__nv_bfloat16>{}); break;
+    }
+}
+
+static int prepare_rows(lbm_ctx* c) {
+    int rc = LBM_OK;
+    dispatch_rows(c, [&](auto st, auto co, auto pi) {
+        using S = typename decltype(st)::type;
+        rc = prepare_rows_t<S, decltype(pi)::value, decltype(co)::value>(c);
+    });
+    return rc;
+}
+
 // Launch one time step reading buffer `from` and writing the other one.
 static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
+    if (c->kernel_used == LBM_KERNEL_ROWS) {
+        dispatch_rows(c, [&](auto st, auto co, auto pi) {
+            using S = typename decltype(st)::type;
+            using R = typename Codec<S>::Real;
+            StepParams<R> p = params_of<R>(c);
+            p.fin = c->f[from];
+            p.fout = c->f[from ^ 1];
+            launch_rows_t<S, decltype(pi)::value, decltype(co)::value>(c, p, s);
+        });
+        return;
+    }
     const dim3 blk(block), grid((unsigned)((c->d.nx + block - 1) / block), (unsigned)c->d.ny, (unsigned)c->d.nz);
     dispatch_storage(c->d.storage, [&](auto tag) {
         using S = typename decltype(tag)::type;
@@ -206,9 +284,9 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
                 break;
             case LBM_MRT:  // deviation arithmetic only (validate_desc)
                 if (c->d.mrt_basis == LBM_MRT_REF)
-                    k_step_mrt<kMrtRef, S, false><<<grid, blk, 0, s>>>(p);
+                    k_step_mrt<kMrtRef, S><<<grid, blk, 0, s>>>(p);
                 else
-                    k_step_mrt<kMrtGramSchmidt, S, false><<<grid, blk, 0, s>>>(p);
+                    k_step_mrt<kMrtGramSchmidt, S><<<grid, blk, 0, s>>>(p);
                 break;
             default:
                 if (abs_arith) {
@@ -238,32 +316,57 @@ static std::string tune_key(const lbm_ctx* c) {
 
 // Pick the block width by timing candidates on the real buffers: each trial reads the current
 // buffer and writes the other one, which the next step overwrites anyway.
+// Choose the kernel family and, for the plain kernel, the block width.  An explicit block width or
+// LBM_KERNEL_PLAIN selects the plain kernel, LBM_KERNEL_ROWS the row pipeline; otherwise every
+// eligible candidate is timed (cached per problem shape).
 static int autotune(lbm_ctx* c) {
-    const std::string key = tune_key(c);
+    if (c->kernel == LBM_KERNEL_ROWS) {
+        c->kernel_used = LBM_KERNEL_ROWS;
+        return prepare_rows(c);
+    }
+    if (c->kernel == LBM_KERNEL_PLAIN && c->block) {
+        c->kernel_used = LBM_KERNEL_PLAIN;
+        return LBM_OK;
+    }
+    if (c->block) {
+        c->kernel_used = LBM_KERNEL_PLAIN;
+        return LBM_OK;
+    }
+    const bool try_rows = c->kernel == LBM_KERNEL_AUTO && rows_eligible(c);
+    const std::string key = tune_key(c) + (try_rows ? "/rows" : "/plain");
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
+            if (it->second < 0) {
+                c->kernel_used = LBM_KERNEL_ROWS;
+                return prepare_rows(c);
+            }
+            c->kernel_used = LBM_KERNEL_PLAIN;
             c->block = it->second;
             return LBM_OK;
         }
     }
     const int maxb = max_block(c);
     const long long nxr = ((c->d.nx + 31) / 32) * 32;
-    std::vector<int> cands;
+    std::vector<int> cands;  // block widths of the plain kernel; -1 = row pipeline
     for (int b : {32, 64, 128, 256, 512})
         if (b <= maxb && (b <= nxr || b == 32)) cands.push_back(b);
-    if (cands.size() == 1) {
-        c->block = cands[0];
-    } else {
+    if (try_rows) {
+        int rc = prepare_rows(c);
+        if (rc) return rc;
+        cands.push_back(-1);
+    }
+    int best_b = cands[0];
+    if (cands.size() > 1) {
         cudaEvent_t a, b;
         LBM_CK(cudaEventCreate(&a));
         LBM_CK(cudaEventCreate(&b));
         float best = 1e30f;
-        int best_b = cands[0];
         const long long bytes = c->N * c->q * (long long)c->sbytes * 2;
         const int reps = bytes > (256LL << 20) ? 2 : 6;
         for (int blk : cands) {
+            c->kernel_used = blk < 0 ? LBM_KERNEL_ROWS : LBM_KERNEL_PLAIN;
             launch_step(c, c->cur, c->stream, blk);
             LBM_CK(cudaEventRecord(a, c->stream));
             for (int r = 0; r < reps; ++r) launch_step(c, c->cur, c->stream, blk);
@@ -279,10 +382,11 @@ static int autotune(lbm_ctx* c) {
         cudaEventDestroy(a);
         cudaEventDestroy(b);
         LBM_CK(cudaGetLastError());
-        c->block = best_b;
     }
+    c->kernel_used = best_b < 0 ? LBM_KERNEL_ROWS : LBM_KERNEL_PLAIN;
+    c->block = best_b < 0 ? 0 : best_b;
     std::lock_guard<std::mutex> g(g_tune_mu);
-    g_tune_cache[key] = c->block;
+    g_tune_cache[key] = best_b;
     return LBM_OK;
 }
 
@@ -341,6 +445,7 @@ static void destroy_ctx(lbm_ctx* c) {
     cudaFree(c->staging);
     cudaFree(c->partial);
     cudaFree(c->sums_out);
+    cudaFree(c->err);
     if (c->e0) cudaEventDestroy(c->e0);
     if (c->e1) cudaEventDestroy(c->e1);
     if (c->own) cudaStreamDestroy(c->own);
@@ -399,7 +504,8 @@ int lbm_create(const lbm_desc* d, lbm_ctx** out) {
     c->reduce_blocks = grid_blocks(c->N, 256);
     bool ok = cudaMalloc(&c->f[0], fbytes) == cudaSuccess && cudaMalloc(&c->f[1], fbytes) == cudaSuccess &&
               cudaMalloc(&c->partial, sizeof(Sums) * c->reduce_blocks) == cudaSuccess &&
-              cudaMalloc(&c->sums_out, sizeof(Sums)) == cudaSuccess;
+              cudaMalloc(&c->sums_out, sizeof(Sums)) == cudaSuccess &&
+              cudaMalloc(&c->err, sizeof(int)) == cudaSuccess && cudaMemset(c->err, 0, sizeof(int)) == cudaSuccess;
     if (ok && d->mask) ok = cudaMalloc(&c->mask, (size_t)c->N) == cudaSuccess;
     if (ok && d->collision == LBM_SHANCHEN)
         ok = cudaMalloc(&c->psi, (size_t)c->N * (d->storage == LBM_F64 ? 8 : 4)) == cudaSuccess;
@@ -553,7 +659,7 @@ int lbm_step(lbm_ctx* c, int64_t nsteps) {
     if (nsteps < 0) return set_error(LBM_ERR_INVALID, "nsteps must be >= 0");
     if (nsteps == 0) return LBM_OK;
     LBM_CK(cudaSetDevice(c->d.device));
-    if (c->block == 0) {
+    if (!c->kernel_used) {
         int rc = autotune(c);
         if (rc) return rc;
     }
@@ -586,6 +692,12 @@ int lbm_sync(lbm_ctx* c) {
     if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
     LBM_CK(cudaSetDevice(c->d.device));
     LBM_CK(cudaStreamSynchronize(c->stream));
+    int err = 0;
+    LBM_CK(cudaMemcpy(&err, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+        LBM_CK(cudaMemset(c->err, 0, sizeof(int)));
+        return set_error(LBM_ERR_TIMEOUT, "a row-pipeline wait on a shared-memory stage gave up; results are invalid");
+    }
     return LBM_OK;
 }
 
@@ -720,9 +832,28 @@ int lbm_set_block(lbm_ctx* c, int threads_x) {
     LBM_CK(cudaStreamSynchronize(c->stream));
     drop_graphs(c);
     c->block = threads_x;
+    c->kernel_used = 0;
     return LBM_OK;
 }
 
 int lbm_get_block(const lbm_ctx* c) { return c ? c->block : 0; }
+
+int lbm_set_kernel(lbm_ctx* c, int kind) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    if (kind != LBM_KERNEL_AUTO && kind != LBM_KERNEL_PLAIN && kind != LBM_KERNEL_ROWS)
+        return set_error(LBM_ERR_INVALID, "unknown kernel family");
+    if (kind == LBM_KERNEL_ROWS && !rows_eligible(c))
+        return set_error(LBM_ERR_UNSUPPORTED,
+                         "the row pipeline needs D3Q27 BGK/MRT, deviation arithmetic, F32/F16S/BF16S and nx in {128,256,512}");
+    LBM_CK(cudaSetDevice(c->d.device));
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->kernel = kind;
+    c->kernel_used = 0;
+    if (kind == LBM_KERNEL_ROWS) c->block = 0;
+    return LBM_OK;
+}
+
+int lbm_get_kernel(const lbm_ctx* c) { return c ? c->kernel_used : 0; }
 
 }  // extern "C"

@@ -137,6 +137,7 @@ const char* lbm_strerror(int status) {
         case LBM_ERR_UNSUPPORTED: return "unsupported combination";
         case LBM_ERR_NO_DEVICE: return "no usable CUDA device";
         case LBM_ERR_STATE: return "invalid state for this call";
+        case LBM_ERR_TIMEOUT: return "a bounded device-side wait timed out";
         default: return "unknown status";
     }
 }

@@ -33,13 +33,14 @@ BGK, MRT, SHANCHEN = 0, 1, 2
 F32, F16S, BF16S, F64 = 0, 1, 2, 3
 MRT_REF, MRT_GRAM_SCHMIDT = 0, 1
 ARITH_DEVIATION, ARITH_ABSOLUTE = 0, 1
+KERNEL_AUTO, KERNEL_PLAIN, KERNEL_ROWS = 0, 1, 2
 DTYPE_F32, DTYPE_F64 = 0, 1
 HOST, DEVICE = 0, 1
 BOUNCE, SET_RHO, SET_UX, SET_UY, SET_UZ, EQUILIBRIUM, ZEROGRAD_XP = 1, 2, 4, 8, 16, 32, 64
 MAX_CLASSES = 16
 
 ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "diverged",
-          -5: "unsupported", -6: "no device", -7: "invalid state"}
+          -5: "unsupported", -6: "no device", -7: "invalid state", -8: "device wait timed out"}
 
 
 class LbmError(RuntimeError):
@@ -108,6 +109,8 @@ _SIGS = {
     "lbm_get_desc": (C.c_int, [_P, _DP]),
     "lbm_set_block": (C.c_int, [_P, C.c_int]),
     "lbm_get_block": (C.c_int, [_P]),
+    "lbm_set_kernel": (C.c_int, [_P, C.c_int]),
+    "lbm_get_kernel": (C.c_int, [_P]),
     "lbm_sums_fp64_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_double, _P, _P]),
     "lbm_batch_create": (C.c_int, [_DP, C.c_int, C.POINTER(_P)]),
     "lbm_batch_destroy": (None, [_P]),
@@ -333,6 +336,13 @@ class Lattice:
 
     def block(self) -> int:
         return lib().lbm_get_block(self._h)
+
+    def set_kernel(self, kind: int):
+        """KERNEL_AUTO, KERNEL_PLAIN or KERNEL_ROWS (bulk-copy row pipeline)."""
+        _check(lib().lbm_set_kernel(self._h, kind))
+
+    def kernel(self) -> int:
+        return lib().lbm_get_kernel(self._h)
 
     def device_populations(self):
         nbytes = C.c_size_t()

@@ -205,3 +205,47 @@ def test_duct3d_config_mode_parity():
         F = lat.get_populations(np.float64)
     Fo, _, _ = O.run(oracle_problem(dd, mm), F0, 200, dtype=np.float32)
     assert rel_l2(F, Fo) < 1e-5
+
+
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.BF16S])
+@pytest.mark.parametrize("coll", ["bgk_cavity", "bgk_duct", "mrt_ref", "mrt_gs"])
+def test_row_pipeline_equals_plain_kernel(storage, coll):
+    """The bulk-copy row pipeline and the one-cell-per-thread kernel run the same collision code on
+    the same inputs: results must be bit-identical (lid, solid, equilibrium-inlet, zero-gradient)."""
+    if coll == "bgk_cavity":
+        d, m, F0 = cavity3d(n=(128, 10, 9), u_lid=0.08, omega=1.6, storage=storage)
+    elif coll == "bgk_duct":
+        d = lb.make_desc(lb.D3Q27, lb.BGK, storage, (128, 12, 12), omega=1.7)
+        m = lb.setup_duct3d(d, 0.04, 30, 6, 6, 3)
+        solid = m == 1
+        F0 = O.init_equilibrium(oracle_problem(d, m), rho=np.where(solid, 0.0, 1.0),
+                                u=np.concatenate([np.where(solid, 0.0, 0.04), np.zeros(2 * m.size)]))
+    else:
+        basis = lb.MRT_REF if coll == "mrt_ref" else lb.MRT_GRAM_SCHMIDT
+        d = lb.make_desc(lb.D3Q27, lb.MRT, storage, (256, 9, 8), mrt_s=lb.mrt_rates(1.8, 1.2), mrt_basis=basis)
+        m = lb.setup_cavity3d(d, 0.05)
+        F0 = np.repeat(lb.velocities(lb.D3Q27)[3], d.cells)
+    out = {}
+    for kind in (lb.KERNEL_PLAIN, lb.KERNEL_ROWS):
+        with lb.Lattice(d, m) as lat:
+            lat.set_kernel(kind)
+            lat.set_populations(np.asarray(F0, dtype=np.float64))
+            lat.step(25)
+            lat.sync()
+            assert lat.kernel() == kind
+            out[kind] = lat.get_populations(np.float32)
+    assert np.array_equal(out[lb.KERNEL_PLAIN], out[lb.KERNEL_ROWS])
+
+
+def test_row_pipeline_needs_eligible_shape():
+    d, m, F0 = cavity2d(n=64)
+    with lb.Lattice(d, m) as lat:
+        with pytest.raises(lb.LbmError) as e:
+            lat.set_kernel(lb.KERNEL_ROWS)
+        assert e.value.code == -5
+    d, m, F0 = cavity3d(n=(100, 8, 8))
+    with lb.Lattice(d, m) as lat:
+        with pytest.raises(lb.LbmError):
+            lat.set_kernel(lb.KERNEL_ROWS)
+        lat.step(3)
+        assert lat.kernel() == lb.KERNEL_PLAIN
