@@ -38,10 +38,14 @@ FALLBACK_HBM_GBS = 6650.0
 # ---------------------------------------------------------------------------------------------
 
 
+def cube(n):
+    return tuple(n) if isinstance(n, (tuple, list)) else (n, n, n)
+
+
 def wl_mrt256(lb, storage, n=256):
-    """D3Q27 MRT lid cavity n^3, Gram-Schmidt basis, lid 0.05, sv from Re 1000 at L=256."""
+    """D3Q27 MRT lid cavity n^3 (or nx x ny x nz), Gram-Schmidt basis, lid 0.05, sv from Re 1000 at L=256."""
     sv = 1.0 / (3.0 * (0.05 * 256 / 1000.0) + 0.5)
-    d = lb.make_desc(lb.D3Q27, lb.MRT, storage, (n, n, n), mrt_s=lb.mrt_rates(sv, 1.2),
+    d = lb.make_desc(lb.D3Q27, lb.MRT, storage, cube(n), mrt_s=lb.mrt_rates(sv, 1.2),
                      mrt_basis=lb.MRT_GRAM_SCHMIDT)
     m = lb.setup_cavity3d(d, 0.05)
     return d, m
@@ -67,7 +71,7 @@ def wl_sc1024(lb, storage, n=None):
 
 
 def wl_bgk3d(lb, storage, n=256):
-    d = lb.make_desc(lb.D3Q27, lb.BGK, storage, (n, n, n), omega=lb.omega_from_re(0.05, n, 1000.0, 0))
+    d = lb.make_desc(lb.D3Q27, lb.BGK, storage, cube(n), omega=lb.omega_from_re(0.05, cube(n)[0], 1000.0, 0))
     m = lb.setup_cavity3d(d, 0.05)
     return d, m
 
@@ -282,17 +286,28 @@ def timed_steps(torch, lat, steps, dev):
 
 def build_workload(lb, args, storage):
     fn = WORKLOADS[args.workload][0]
+    if args.dims and args.workload.startswith("d3q27"):
+        return fn(lb, storage, tuple(int(v) for v in args.dims.lower().split("x")))
     if args.size and args.workload.startswith("d3q27"):
         return fn(lb, storage, args.size)
     return fn(lb, storage)
+
+
+def apply_kernel_choice(lb, lat, args):
+    if args.kernel != "auto":
+        lat.set_kernel({"plain": lb.KERNEL_PLAIN, "rows": lb.KERNEL_ROWS}[args.kernel])
+    if args.block:
+        lat.set_block(args.block)
+
+
+KERNEL_NAMES = {1: "plain", 2: "rows"}
 
 
 def measure(torch, lb, args, storage, dev, world, sample_clocks=False):
     d, m = build_workload(lb, args, storage)
     d.device = dev
     lat = lb.Lattice(d, m)
-    if args.block:
-        lat.set_block(args.block)
+    apply_kernel_choice(lb, lat, args)
     lat.step(args.warmup if args.warmup > 0 else 1)   # includes the block-width autotune
     lat.sync()
     torch.cuda.synchronize(dev)
@@ -314,8 +329,7 @@ def e2e_measure(torch, lb, args, storage, dev, world):
     d, m = build_workload(lb, args, storage)
     d.device = dev
     lat = lb.Lattice(d, m)
-    if args.block:
-        lat.set_block(args.block)
+    apply_kernel_choice(lb, lat, args)
     N, Q = d.cells, d.q
     _, _, _, w, _ = lb.velocities(d.lattice)
     F_host = torch.empty(N * Q, dtype=torch.float32, pin_memory=True)
@@ -400,6 +414,8 @@ def run_ours(args, rank, world, local_rank):
     avg_launch_s = el / (args.steps * launches_per_step)
     achieved = bytes_cell * N / launches_per_step / avg_launch_s / 1e9
     traffic = dram_traffic(args.workload, head_storage)
+    kernel_family = KERNEL_NAMES.get(lat.kernel(), "unknown")
+    block_used = lat.block()
     lat.close()
     del lat
 
@@ -412,11 +428,13 @@ def run_ours(args, rank, world, local_rank):
                    "bytes_per_cell_update": bytes_cell,
                    "l2": f"inputs larger than L2: {N * d.q * storage_bytes(head_storage) / 1e9:.2f} GB per population buffer"
                    if N * d.q * storage_bytes(head_storage) > 126e6 else "lattice is L2-resident (no flush)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "kernel_family": kernel_family, "block": block_used},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_kind == "measured" else "fallback 6.65 TB/s",
-                     "kernel": {0: "k_step_bgk", 1: "k_step_mrt", 2: "k_step_sc + k_sc_psi"}[d.collision],
+                     "kernel": "k_step_rows" if kernel_family == "rows" else
+                     {0: "k_step_bgk", 1: "k_step_mrt", 2: "k_step_sc + k_sc_psi"}[d.collision],
                      "bytes_per_launch": bytes_cell * N / launches_per_step},
         "gpu_launches": args.steps * launches_per_step,
         "clocks": clocks,
@@ -466,6 +484,8 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--size", type=int, default=0, help="cube side for D3Q27 workloads (default: the config's)")
+    ap.add_argument("--dims", default="", help="NXxNYxNZ for D3Q27 workloads (small cases for profiling)")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "rows"], help="step-kernel family")
     ap.add_argument("--block", type=int, default=0, help="fixed block width (default: autotune)")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:

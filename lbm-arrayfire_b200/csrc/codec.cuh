@@ -13,6 +13,11 @@
 // transforms; for the 16-bit codecs the stored word already is the deviation.
 // load/load_dev read global memory through the read-only path (__ldg); dev() decodes a value that
 // was read by other means (e.g. from shared memory, which __ldg must not be given).
+//
+// The BGK and MRT step kernels use the "raw" interface: raw() gives the deviation in storage units,
+// i.e. (f - w) * scale for the 16-bit codecs (no multiply) and f - w for F32/F64 (scale 1), and enc()
+// stores a value given in the same units.  The collision folds `scale` (a power of two, so every
+// rescaling is exact) into its per-cell constants instead of rescaling 2*Q populations.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -31,6 +36,9 @@ struct Codec<float> {
     static constexpr int kBytes = 4;
     __device__ __forceinline__ static float load(const float* p, float, float) { return __ldg(p); }
     __device__ __forceinline__ static void store(float* p, float v, float, float) { *p = v; }
+    static constexpr bool kScaled = false;
+    __device__ __forceinline__ static float raw(float v, float w) { return v - w; }
+    __device__ __forceinline__ static float enc(float d, float w) { return w + d; }
     __device__ __forceinline__ static float dev(float raw, float w, float) { return raw - w; }
     __device__ __forceinline__ static float load_dev(const float* p, float w, float) { return __ldg(p) - w; }
     __device__ __forceinline__ static void store_dev(float* p, float d, float w, float) { *p = w + d; }
@@ -42,6 +50,9 @@ struct Codec<double> {
     static constexpr int kBytes = 8;
     __device__ __forceinline__ static double load(const double* p, double, double) { return __ldg(p); }
     __device__ __forceinline__ static void store(double* p, double v, double, double) { *p = v; }
+    static constexpr bool kScaled = false;
+    __device__ __forceinline__ static double raw(double v, double w) { return v - w; }
+    __device__ __forceinline__ static double enc(double d, double w) { return w + d; }
     __device__ __forceinline__ static double dev(double raw, double w, double) { return raw - w; }
     __device__ __forceinline__ static double load_dev(const double* p, double w, double) { return __ldg(p) - w; }
     __device__ __forceinline__ static void store_dev(double* p, double d, double w, double) { *p = w + d; }
@@ -57,6 +68,9 @@ struct Codec<__half> {
     __device__ __forceinline__ static void store(__half* p, float v, float w, float scale) {
         *p = __float2half_rn((v - w) * scale);
     }
+    static constexpr bool kScaled = true;
+    __device__ __forceinline__ static float raw(__half v, float) { return __half2float(v); }
+    __device__ __forceinline__ static __half enc(float d, float) { return __float2half_rn(d); }
     __device__ __forceinline__ static float dev(__half raw, float, float inv_scale) {
         return __half2float(raw) * inv_scale;
     }
@@ -78,6 +92,9 @@ struct Codec<__nv_bfloat16> {
     __device__ __forceinline__ static void store(__nv_bfloat16* p, float v, float w, float scale) {
         *p = __float2bfloat16_rn((v - w) * scale);
     }
+    static constexpr bool kScaled = true;
+    __device__ __forceinline__ static float raw(__nv_bfloat16 v, float) { return __bfloat162float(v); }
+    __device__ __forceinline__ static __nv_bfloat16 enc(float d, float) { return __float2bfloat16_rn(d); }
     __device__ __forceinline__ static float dev(__nv_bfloat16 raw, float, float inv_scale) {
         return __bfloat162float(raw) * inv_scale;
     }

@@ -63,8 +63,8 @@ struct Rows {
     __device__ __forceinline__ long long src(int cy, int cz) const { return base[1 - cy][1 - cz]; }
 };
 
-// Pull gather of one cell.  ABS = false: deviations d_i = f_i - w_i; ABS = true: the populations
-// themselves.  x-wrap per thread; the source x of c_x = +1 is x-1 and of c_x = -1 is x+1
+// Pull gather of one cell.  ABS = false: deviations in storage units (Codec::raw: f_i - w_i, times
+// the storage scale for the 16-bit codecs); ABS = true: the populations themselves.  x-wrap per thread; the source x of c_x = +1 is x-1 and of c_x = -1 is x+1
 // (af::shift: out[x] = in[x - c]).
 template <class L, class S, bool ABS, class P, class R>
 __device__ __forceinline__ void pull(const S* __restrict__ fin, const P& p, const Rows<L>& rows, int x,
@@ -79,7 +79,7 @@ __device__ __forceinline__ void pull(const S* __restrict__ fin, const P& p, cons
         if constexpr (ABS)
             d[i] = Codec<S>::load(fin + idx, R(L::w(i)), R(p.inv_scale));
         else
-            d[i] = Codec<S>::load_dev(fin + idx, R(L::w(i)), R(p.inv_scale));
+            d[i] = Codec<S>::raw(__ldg(fin + idx), R(L::w(i)));
     });
 }
 
@@ -95,15 +95,16 @@ __device__ __forceinline__ void pull_zerograd(const S* __restrict__ fin, const P
             if constexpr (ABS)
                 d[i] = Codec<S>::load(fin + idx, R(L::w(i)), R(p.inv_scale));
             else
-                d[i] = Codec<S>::load_dev(fin + idx, R(L::w(i)), R(p.inv_scale));
+                d[i] = Codec<S>::raw(__ldg(fin + idx), R(L::w(i)));
         }
     });
 }
 
 // Moments (cpp/d2q9_bgk_lid.cpp:131-138): rho = sum f, j = sum c f, u = j / rho.  On deviations
 // sum d = rho - 1 and sum c d = j (sum c w = 0).  Both rho and drho = rho - 1 are returned.
+// isc: 1 / storage scale of raw deviations (a power of two, so the rescaled sums are exact).
 template <class L, bool ABS, class R>
-__device__ __forceinline__ void moments(const R (&v)[L::Q], R& rho, R& drho, R& ux, R& uy, R& uz) {
+__device__ __forceinline__ void moments(const R (&v)[L::Q], R isc, R& rho, R& drho, R& ux, R& uy, R& uz) {
     R r = R(0), jx = R(0), jy = R(0), jz = R(0);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
@@ -119,8 +120,11 @@ __device__ __forceinline__ void moments(const R (&v)[L::Q], R& rho, R& drho, R& 
         rho = r;
         drho = r - R(1);
     } else {
-        drho = r;
-        rho = R(1) + r;
+        drho = r * isc;
+        rho = R(1) + drho;
+        jx = jx * isc;
+        jy = jy * isc;
+        jz = jz * isc;
     }
     ux = jx / rho;
     uy = jy / rho;
@@ -157,9 +161,9 @@ __device__ __forceinline__ R feq_abs_i(R rho, R usq15, R ux, R uy, R uz) {
 
 // Deviation equilibrium feq_i - w_i = w_i ((rho - 1) + rho (4.5 eu^2 - 1.5 u^2)) +- w_i rho 3 eu,
 // evaluated once per pair of opposite directions: the symmetric part is shared and the
-// momentum-carrying part is exactly antisymmetric.
+// momentum-carrying part is exactly antisymmetric.  sc: storage scale of the result (power of two).
 template <class L, class R>
-__device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz, R (&fe)[L::Q]) {
+__device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz, R sc, R (&fe)[L::Q]) {
     const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
     const R rho3 = R(3) * rho;
     const R rho45 = R(4.5) * rho;
@@ -168,7 +172,7 @@ __device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz,
         constexpr int i = I;
         constexpr int o = L::opp(i);
         if constexpr (i == 0) {
-            fe[0] = R(L::w(0)) * base;
+            fe[0] = (R(L::w(0)) * sc) * base;
         } else if constexpr (i < o) {
             constexpr int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
             R eu = R(0);
@@ -178,7 +182,7 @@ __device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz,
             if constexpr (cy == -1) eu = eu - uy;
             if constexpr (cz == 1) eu = eu + uz;
             if constexpr (cz == -1) eu = eu - uz;
-            const R w = R(L::w(i));
+            const R w = R(L::w(i)) * sc;
             const R sym = w * (base + rho45 * (eu * eu));
             const R anti = w * (rho3 * eu);
             fe[i] = sym + anti;
@@ -188,7 +192,7 @@ __device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz,
 }
 
 template <class L, bool ABS, class R>
-__device__ __forceinline__ void equilibrium_v(R rho, R drho, R ux, R uy, R uz, R (&feq)[L::Q]) {
+__device__ __forceinline__ void equilibrium_v(R rho, R drho, R ux, R uy, R uz, R sc, R (&feq)[L::Q]) {
     if constexpr (ABS) {
         const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
         static_for<L::Q>([&](auto I) {
@@ -196,7 +200,7 @@ __device__ __forceinline__ void equilibrium_v(R rho, R drho, R ux, R uy, R uz, R
             feq[i] = feq_abs_i<L, i>(rho, usq15, ux, uy, uz);
         });
     } else {
-        equilibrium_dev<L, R>(rho, drho, ux, uy, uz, feq);
+        equilibrium_dev<L, R>(rho, drho, ux, uy, uz, sc, feq);
     }
 }
 
@@ -204,7 +208,7 @@ __device__ __forceinline__ void equilibrium_v(R rho, R drho, R ux, R uy, R uz, R
 template <class L, class R>
 __device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R (&feq)[L::Q]) {
     R dev[L::Q];
-    equilibrium_dev<L, R>(rho, rho - R(1), ux, uy, uz, dev);
+    equilibrium_dev<L, R>(rho, rho - R(1), ux, uy, uz, R(1), dev);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
         feq[i] = R(L::w(i)) + dev[i];
@@ -218,8 +222,21 @@ __device__ __forceinline__ void store_cell(S* __restrict__ fout, const P& p, lon
         if constexpr (ABS)
             Codec<S>::store(fout + (long long)i * p.N + c, out[i], R(L::w(i)), R(p.scale));
         else
-            Codec<S>::store_dev(fout + (long long)i * p.N + c, out[i], R(L::w(i)), R(p.scale));
+            fout[(long long)i * p.N + c] = Codec<S>::enc(out[i], R(L::w(i)));
     });
+}
+
+// Storage scale and its inverse for raw deviations: the codec's scale for the 16-bit codecs,
+// compile-time 1 otherwise.
+template <class S, class P, class R>
+__device__ __forceinline__ void storage_scale(const P& p, R& sc, R& isc) {
+    if constexpr (Codec<S>::kScaled) {
+        sc = R(p.scale);
+        isc = R(p.inv_scale);
+    } else {
+        sc = R(1);
+        isc = R(1);
+    }
 }
 
 template <class T>
@@ -232,14 +249,16 @@ __device__ __forceinline__ void cell_class(const uint8_t* __restrict__ mask, con
 // ---- BGK ---------------------------------------------------------------------------------
 // Collision of one cell from its streamed populations v (ABS) or deviations v = f - w:
 // F = omega FEQ + (1 - omega) F_streamed (cpp/d2q9_bgk_lid.cpp:153), the class overwrites before it
-// and the full-way bounce-back after it (:155).  P supplies cls, omega, one_m_omega.
+// and the full-way bounce-back after it (:155).  P supplies cls, omega, one_m_omega.  Deviations
+// are in storage units: sc / isc are the storage scale and its inverse (1 for ABS).
 template <class L, bool ABS, class P, class R>
-__device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, const R (&v)[L::Q], R (&out)[L::Q]) {
+__device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, const R (&v)[L::Q], R sc, R isc,
+                                            R (&out)[L::Q]) {
     R rho, drho, ux, uy, uz;
-    moments<L, ABS>(v, rho, drho, ux, uy, uz);
+    moments<L, ABS>(v, isc, rho, drho, ux, uy, uz);
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
     R fe[L::Q];
-    equilibrium_v<L, ABS>(rho, drho, ux, uy, uz, fe);
+    equilibrium_v<L, ABS>(rho, drho, ux, uy, uz, sc, fe);
     const R omega = R(p.omega), one_m = R(p.one_m_omega);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
@@ -269,13 +288,15 @@ __device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, 
     uint32_t fl;
     cell_class(p.mask, p.cls, c, cls, fl);
     if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+    R sc, isc;
+    storage_scale<S>(p, sc, isc);
     R out[L::Q];
-    bgk_collide<L, ABS>(p, cls, fl, v, out);
+    bgk_collide<L, ABS>(p, cls, fl, v, sc, isc, out);
     store_cell<L, S, ABS>(fout, p, c, out);
 }
 
 template <class L, class S, bool ABS>
-__global__ void __launch_bounds__(512) k_step_bgk(StepParams<typename Codec<S>::Real> p) {
+__global__ void __launch_bounds__(512) k_step_bgk(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
     bgk_cell<L, S, ABS>(p, static_cast<const S*>(p.fin), static_cast<S*>(p.fout), x, blockIdx.y, blockIdx.z);
@@ -287,14 +308,17 @@ __global__ void __launch_bounds__(512) k_step_bgk(StepParams<typename Codec<S>::
 // order in out[].  The transform acts on d = f - w: M d = M f - M w, and M w = meq(rho = 1, u = 0) for
 // both bases, so m* = m - S (m - meq) carries over with every equilibrium moment replaced by its
 // deviation from rest, i.e. the cell quantity rho replaced by rho - 1 (mrt.cuh).  Bounce-back is left
-// to the caller (it needs the streamed values, which the transform overwrote).
+// to the caller (it needs the streamed values, which the transform overwrote).  The deviations are in
+// storage units (times sc); the transform is linear, so the scale rides along and enters only through
+// isc here and through the equilibrium coefficients (beta and B carry sc, set on the host).
 template <int BASIS, class P, class R>
-__device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R (&T)[27], R (&out)[27]) {
+__device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R (&T)[27], R sc, R isc,
+                                            R (&out)[27]) {
     using L = D3Q27;
     mrt_forward<BASIS>(T);
-    R drho = T[0];
+    R drho = T[0] * isc;
     R rho = R(1) + drho;
-    const R inv = R(1) / rho;
+    const R inv = isc / rho;
     R ux = T[1] * inv, uy = T[3] * inv, uz = T[9] * inv;
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 3);
     R q[11];
@@ -315,11 +339,11 @@ __device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R 
         constexpr int i = I;
         out[i] = T[L::slot(i)];
     });
-    if (fl & kEquilibrium) equilibrium_dev<L, R>(rho, drho, ux, uy, uz, out);
+    if (fl & kEquilibrium) equilibrium_dev<L, R>(rho, drho, ux, uy, uz, sc, out);
 }
 
 template <int BASIS, class S>
-__global__ void __launch_bounds__(256) k_step_mrt(StepParams<typename Codec<S>::Real> p) {
+__global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D3Q27;
     using R = typename Codec<S>::Real;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -341,8 +365,10 @@ __global__ void __launch_bounds__(256) k_step_mrt(StepParams<typename Codec<S>::
             T[L::slot(i)] = v[i];
         });
     }
+    R sc, isc;
+    storage_scale<S>(p, sc, isc);
     R out[27];
-    mrt_collide<BASIS>(p, cls, fl, T, out);
+    mrt_collide<BASIS>(p, cls, fl, T, sc, isc, out);
     if (fl & kBounce) {
         // reload the streamed deviations (the transform overwrote them in place)
         R v[27];
@@ -359,7 +385,7 @@ __global__ void __launch_bounds__(256) k_step_mrt(StepParams<typename Codec<S>::
 // ---- Shan-Chen (D2Q9) --------------------------------------------------------------------
 // Pass 1: psi = 1 - exp(-rho) of the streamed density of every cell.
 template <class S, bool ABS>
-__global__ void __launch_bounds__(512) k_sc_psi(StepParams<typename Codec<S>::Real> p) {
+__global__ void __launch_bounds__(512) k_sc_psi(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D2Q9;
     using R = typename Codec<S>::Real;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -374,9 +400,11 @@ __global__ void __launch_bounds__(512) k_sc_psi(StepParams<typename Codec<S>::Re
     uint32_t fl;
     cell_class(p.mask, p.cls, c, cls, fl);
     if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+    R sc, isc;
+    storage_scale<S>(p, sc, isc);
     R sum = R(0);
     static_for<9>([&](auto I) { sum += v[I]; });
-    R rho = ABS ? sum : R(1) + sum;
+    R rho = ABS ? sum : R(1) + sum * isc;
     if (fl & kSetRho) rho = R(p.cls.rho[cls]);
     p.psi[c] = R(1) - exp(-rho);
 }
@@ -406,7 +434,7 @@ __device__ __forceinline__ void sc_force(const StepParams<R>& p, const Rows<D2Q9
 }
 
 template <class S, bool ABS>
-__global__ void __launch_bounds__(512) k_step_sc(StepParams<typename Codec<S>::Real> p) {
+__global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D2Q9;
     using R = typename Codec<S>::Real;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -421,8 +449,10 @@ __global__ void __launch_bounds__(512) k_step_sc(StepParams<typename Codec<S>::R
     uint32_t fl;
     cell_class(p.mask, p.cls, c, cls, fl);
     if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+    R sc, isc;
+    storage_scale<S>(p, sc, isc);
     R rho, drho, ux, uy, uz;
-    moments<L, ABS>(v, rho, drho, ux, uy, uz);
+    moments<L, ABS>(v, isc, rho, drho, ux, uy, uz);
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 2);
     R Fx, Fy;
     sc_force(p, rows, x, c, Fx, Fy);
@@ -434,7 +464,7 @@ __global__ void __launch_bounds__(512) k_step_sc(StepParams<typename Codec<S>::R
         vy = uy + Fy * k;
     }
     R fe[9];
-    equilibrium_v<L, ABS>(rho, drho, vx, vy, R(0), fe);
+    equilibrium_v<L, ABS>(rho, drho, vx, vy, R(0), sc, fe);
     R out[9];
     static_for<9>([&](auto I) {
         constexpr int i = I;
@@ -453,7 +483,7 @@ __global__ void __launch_bounds__(512) k_step_sc(StepParams<typename Codec<S>::R
 // pulled = 1: the fields the last step's collision used (pull from the previous buffer, class
 // overwrites, Shan-Chen velocity u + F/(2 rho)).  pulled = 0: local moments of p.fin.
 template <class L, class S, class O>
-__global__ void k_macros(StepParams<typename Codec<S>::Real> p, int pulled, int collision, O* rho_out,
+__global__ void k_macros(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int pulled, int collision, O* rho_out,
                          O* u_out) {
     using R = typename Codec<S>::Real;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -472,11 +502,13 @@ __global__ void k_macros(StepParams<typename Codec<S>::Real> p, int pulled, int 
     } else {
         static_for<L::Q>([&](auto I) {
             constexpr int i = I;
-            d[i] = Codec<S>::load_dev(fin + (long long)i * p.N + c, R(L::w(i)), p.inv_scale);
+            d[i] = Codec<S>::raw(__ldg(fin + (long long)i * p.N + c), R(L::w(i)));
         });
     }
+    R sc, isc;
+    storage_scale<S>(p, sc, isc);
     R rho, drho, ux, uy, uz;
-    moments<L, false>(d, rho, drho, ux, uy, uz);
+    moments<L, false>(d, isc, rho, drho, ux, uy, uz);
     if (pulled && fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
     if constexpr (L::DIM == 2) {
         if (pulled && collision == 2) {

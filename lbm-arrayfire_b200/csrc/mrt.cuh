@@ -16,6 +16,8 @@
 // (cx+1) + 3(cy+1) + 9(cz+1) before the transform.
 #pragma once
 
+#include <cmath>
+
 #include "lattice.cuh"
 
 namespace lbm {
@@ -94,12 +96,20 @@ LBM_HD constexpr double mrt_meq_coef(int basis, int t, int k) {
     }
 }
 
+// s - 2v as one fused multiply-add: 2v is exact, so this rounds exactly like the two-operation
+// form, but stays one instruction (the compiler turns 2v into v + v otherwise).
+template <class R>
+LBM_HD R minus_twice(R s, R v) {
+    using std::fma;
+    return fma(R(-2), v, s);
+}
+
 template <int BASIS, class R>
 LBM_HD void mrt_fwd3(R& v0, R& v1, R& v2) {
     // v0, v1, v2 = populations at c = -1, 0, +1 along one axis
     const R s = v0 + v2, d = v2 - v0;
     const R m0 = s + v1;
-    const R m2 = BASIS == kMrtRef ? s : s - R(2) * v1;
+    const R m2 = BASIS == kMrtRef ? s : minus_twice(s, v1);
     v0 = m0;
     v1 = d;
     v2 = m2;
@@ -108,7 +118,7 @@ LBM_HD void mrt_fwd3(R& v0, R& v1, R& v2) {
 template <int BASIS, class R>
 LBM_HD void mrt_inv3(R& m0, R& m1, R& m2) {
     // inverse of mrt_fwd3 after the per-axis scale has been applied
-    const R v1 = m0 - R(2) * m2;
+    const R v1 = minus_twice(m0, m2);
     const R t = BASIS == kMrtRef ? m2 : m0 + m2;
     const R v0 = t - m1, v2 = t + m1;
     m0 = v0;

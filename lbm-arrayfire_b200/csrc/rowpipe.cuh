@@ -1,18 +1,24 @@
-// rowpipe.cuh — D3Q27 step kernel with bulk-copy (TMA) staging of whole lattice rows.
+// rowpipe.cuh — D3Q27 step kernel with bulk-copy (TMA) staging of lattice rows.
 //
-// A CTA of nx threads owns one lattice row (y, z) at a time and walks a strided list of rows.  For
-// each row it needs, per direction i, the full source row (y - cy_i, z - cz_i) of plane i; the x
-// shift of the pull (af::shift semantics, periodic in x) then becomes an index offset inside that
-// staged row.  Warp 0 issues one `cp.async.bulk` global->shared copy per direction into a ring of NS
-// shared-memory stages (completion counted in bytes on one mbarrier per stage), so NS rows of loads
-// are in flight per CTA without holding registers.  The collision reads the staged populations with
-// immediate-offset shared loads, writes its results into one of two output stages, and warp 0 sends
-// each output row back with `cp.async.bulk` shared->global copies.  Compared with the one-cell-per-
-// thread kernel this removes the per-population 64-bit address arithmetic (the issue bottleneck of
-// 16-bit storage) and decouples memory latency from occupancy.
+// A CTA owns a group of up to B consecutive lattice rows (y0..y0+nb-1, z) at a time — one thread per
+// x, each handling the nb cells of its column — and walks a strided list of row groups.  For each
+// group it needs, per direction i, the source rows (y0+b - cy_i, z - cz_i) of plane i: one contiguous
+// run of memory, split in two where the group wraps around y.  The x shift of the pull (af::shift
+// semantics, periodic in x) becomes an index offset inside the staged rows.
 //
-// Every wait on an mbarrier is bounded (about two seconds); a CTA that times out records
-// kRowPipeTimeout in *err, drains the copies it issued with bounded waits and returns.
+// The rows arrive by `cp.async.bulk` global->shared copies (one or two per direction per group, plus
+// the mask rows) into a ring of NS shared-memory stages; each stage's completion is counted in bytes
+// on an mbarrier (full[s]).  The warps wait on full[s], read the staged populations with
+// immediate-offset shared loads, collide and store their cells straight to global memory (coalesced
+// along x).  There is no producer warp: every warp bumps a shared counter when it is done with a
+// stage, and the warp that empties it issues the refill for the group NS steps ahead.  (Measured on
+// B200: a dedicated producer warp spent ~13% of the SM's issue slots polling its barrier, and staging
+// the outputs for bulk stores was slower than direct stores, 25 vs 29 GLUPS for FP32 MRT at 256^3,
+// because the copy engine's request rate, not the bytes, was the limit.)  For the same reason a group
+// spans 1-2 KB per direction (B rows) so each bulk load moves a useful amount.
+//
+// Every wait on an mbarrier is bounded (about two seconds); a warp that times out records
+// kRowPipeTimeout in *err, waits (bounded) for the copies into this CTA's stages and returns.
 // No multicast: every copy moves data of this GPU's own memory into this CTA's shared memory.
 #pragma once
 
@@ -37,23 +43,24 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
 }
+// try_wait with a suspend-time hint (1 ms): the warp may be parked until the phase completes.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(smem_addr(bar)), "r"(parity)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(1000000u)
         : "memory");
     return done != 0;
 }
-// Bounded wait: false after ~2^32 clocks (about two seconds) without completion.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Bounded wait: false after `limit` clocks (2^32 is about two seconds) without completion.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit = 1LL << 32) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > (1LL << 32)) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src_gmem, uint32_t bytes, uint64_t* bar) {
@@ -62,14 +69,6 @@ __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src_gmem, 
                  "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
                  : "memory");
 }
-__device__ __forceinline__ void bulk_store(void* dst_gmem, const void* src_smem, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem), "r"(smem_addr(src_smem)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -82,148 +81,183 @@ constexpr unsigned long long pack_c(bool z) {
     return v;
 }
 
-// Stage counts: input stages NS (loads in flight per CTA) and two output stages.
-template <class S>
-struct RowPipeStages {
-    static constexpr int NS = sizeof(S) <= 2 ? 4 : 2;
-    static constexpr int NO = 2;
+#ifndef LBM_ROWPIPE_GROUP_BYTES
+#define LBM_ROWPIPE_GROUP_BYTES 0  // bytes per direction per row group (sets B); 0 = per storage type
+#endif
+#ifndef LBM_ROWPIPE_NS
+#define LBM_ROWPIPE_NS 0  // stages; 0 = as many as the shared-memory budget holds
+#endif
+
+// Rows per group B, stage bytes and stages NS.  Measured on B200 (MRT, 256^3): 16-bit storage is
+// limited by the bulk-copy request rate and gains from the largest copies (2 KB per direction: 43 vs
+// 33 GLUPS at 512 B); FP32 runs at ~0.9 of the copy bandwidth and does best with 1 KB copies and
+// three stages (~83 KB) per CTA.  Two CTAs share an SM for nx <= 256, one CTA has it for nx = 512.
+template <class S, int PITCH>
+struct RowPipeShape {
+    static constexpr bool k16 = sizeof(S) == 2;
+    static constexpr int kRowBytes = PITCH * (int)sizeof(S);
+    static constexpr int kGroupBytes = LBM_ROWPIPE_GROUP_BYTES > 0 ? LBM_ROWPIPE_GROUP_BYTES : (k16 ? 2048 : 1024);
+    static constexpr int B0 = kGroupBytes / kRowBytes;
+    static constexpr int B = B0 < 1 ? 1 : (B0 > 4 ? 4 : B0);
+    static constexpr int CTAS = PITCH <= 256 ? 2 : 1;
+    static constexpr int STAGE = 27 * B * kRowBytes;
+    static constexpr int kBudget = (CTAS == 2 ? (k16 ? 110 : 83) : (k16 ? 216 : 166)) * 1024;
+    static constexpr int NS0 = LBM_ROWPIPE_NS > 0 ? LBM_ROWPIPE_NS : kBudget / STAGE;
+    static constexpr int NS = NS0 < 2 ? 2 : (NS0 > 8 ? 8 : NS0);
+    static_assert((size_t)NS * (STAGE + B * PITCH) + 128 <= (CTAS == 2 ? 112 : 224) * 1024,
+                  "row pipeline stages exceed the shared-memory budget");
 };
 
+// barriers and counters | NS population stages | NS mask stages
 template <class L, class S, int PITCH>
 constexpr size_t rowpipe_smem_bytes() {
-    return 128 + (size_t)(RowPipeStages<S>::NS + RowPipeStages<S>::NO) * L::Q * PITCH * sizeof(S);
+    using Sh = RowPipeShape<S, PITCH>;
+    return 128 + (size_t)Sh::NS * L::Q * Sh::B * PITCH * sizeof(S) + (size_t)Sh::NS * Sh::B * PITCH;
 }
 
 // COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt).  Deviation arithmetic.
-// Requires nx == PITCH (one thread per cell of the row).
+// Requires nx == PITCH; block = PITCH threads (PITCH / 32 warps).
+//   full[s]  tx-count barrier, completed by the bulk loads of stage s
+//   done[s]  warps finished with stage s in its current use; the last one resets it and refills
 template <class L, class S, int PITCH, int COLL>
-__global__ void __launch_bounds__(PITCH, PITCH <= 256 ? 2 : 1)
-    k_step_rows(StepParams<typename Codec<S>::Real> p, int* __restrict__ err) {
+__global__ void __launch_bounds__(PITCH, RowPipeShape<S, PITCH>::CTAS)
+    k_step_rows(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int* __restrict__ err) {
     using R = typename Codec<S>::Real;
+    using Sh = RowPipeShape<S, PITCH>;
     constexpr int Q = L::Q;
-    constexpr int NS = RowPipeStages<S>::NS;
-    constexpr int NO = RowPipeStages<S>::NO;
+    constexpr int NS = Sh::NS;
+    constexpr int B = Sh::B;
+    constexpr int SB = B * PITCH;  // elements per direction in a stage
+    constexpr int W = PITCH / 32;  // warps
+    static_assert(NS <= 8, "barriers and counters occupy the first 128 bytes");
     constexpr unsigned long long kCy = pack_c<L>(false), kCz = pack_c<L>(true);
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-    S* in = reinterpret_cast<S*>(smem + 128);
-    S* outs = in + NS * Q * PITCH;
+    unsigned int* done = reinterpret_cast<unsigned int*>(full + NS);
+    S* in = reinterpret_cast<S*>(smem + 128);                                 // [NS][Q][B][PITCH]
+    uint8_t* mask_st = reinterpret_cast<uint8_t*>(in + (size_t)NS * Q * SB);  // [NS][B][PITCH]
+    const bool has_mask = p.mask != nullptr;
 
-    const int x = threadIdx.x;
-    const int lane = x & 31, warp = x >> 5;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
-    const long long rows = (long long)ny * nz;
+    const int gy = (ny + B - 1) / B;  // row groups per z plane; the last one may be short
+    const long long groups = (long long)gy * nz;
     const uint32_t row_bytes = (uint32_t)(nx * sizeof(S));
+    const long long first = blockIdx.x, stride = gridDim.x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
-    S* __restrict__ fout = static_cast<S*>(p.fout);
 
-    if (x == 0) {
-        for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
-        mbar_init_fence();
-    }
-    __syncthreads();
-
-    // warp 0: stage the Q source rows of destination row r into input stage s
-    auto issue = [&](long long r, int s) {
-        const int y = (int)(r % ny), z = (int)(r / ny);
-        if (lane == 0) mbar_arrive_expect_tx(&full[s], (uint32_t)Q * row_bytes);
+    // Issue the bulk loads of group g into stage s (one warp; lanes 0..Q-1 one direction each).
+    auto issue = [&](long long g, int s) {
+        const int y0 = (int)(g % gy) * B, z = (int)(g / gy);
+        const int nb = ny - y0 < B ? ny - y0 : B;
+        if (lane == 0)
+            mbar_arrive_expect_tx(&full[s], (uint32_t)(Q * nb) * row_bytes + (has_mask ? (uint32_t)(nb * nx) : 0u));
         __syncwarp();
         if (lane < Q) {
             const int cy = (int)((kCy >> (2 * lane)) & 3) - 1, cz = (int)((kCz >> (2 * lane)) & 3) - 1;
-            int ys = y - cy, zs = z - cz;
-            ys = ys < 0 ? ys + ny : (ys >= ny ? ys - ny : ys);
+            int zs = z - cz;
             zs = zs < 0 ? zs + nz : (zs >= nz ? zs - nz : zs);
-            const S* src = fin + (long long)lane * p.N + ((long long)zs * ny + ys) * nx;
-            bulk_load(in + (lane * PITCH) + (long long)s * Q * PITCH, src, row_bytes, &full[s]);
+            int ys = y0 - cy;  // first source row; the nb rows wrap around y at most once
+            ys = ys < 0 ? ys + ny : (ys >= ny ? ys - ny : ys);
+            const int run = ny - ys < nb ? ny - ys : nb;  // rows before the wrap
+            const S* plane = fin + (long long)lane * p.N + (long long)zs * ny * nx;
+            S* dst = in + ((long long)s * Q + lane) * SB;
+            bulk_load(dst, plane + (long long)ys * nx, (uint32_t)run * row_bytes, &full[s]);
+            if (run < nb) bulk_load(dst + run * PITCH, plane, (uint32_t)(nb - run) * row_bytes, &full[s]);
+        } else if (lane == Q && has_mask) {
+            bulk_load(mask_st + s * SB, p.mask + ((long long)z * ny + y0) * nx, (uint32_t)(nb * nx), &full[s]);
         }
     };
 
-    const long long first = blockIdx.x, stride = gridDim.x;
-    if (warp == 0)
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            done[s] = 0;
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid < 32)
         for (int s = 0; s < NS; ++s)
-            if (first + s * stride < rows) issue(first + s * stride, s);
+            if (first + s * stride < groups) issue(first + s * stride, s);
 
+    const int x = tid;
     const int xm = x == 0 ? nx - 1 : x - 1;
     const int xp = x == nx - 1 ? 0 : x + 1;
-    long long k = 0;
-    bool dead = false;
-    for (;; ++k) {
-        const long long r = first + k * stride;
-        if (r >= rows) break;
-        const int s = (int)(k % NS), o = (int)(k % NO);
-        const uint32_t parity = (uint32_t)((k / NS) & 1);
-        const bool ok = mbar_wait_bounded(&full[s], parity);
-        const S* st = in + (long long)s * Q * PITCH;
-
-        // gather the streamed deviations from the staged rows
-        R v[Q];
-        static_for<Q>([&](auto I) {
-            constexpr int i = I;
-            constexpr int cx = L::cx(i);
-            const int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
-            v[i] = Codec<S>::dev(st[i * PITCH + xs], R(L::w(i)), R(p.inv_scale));
-        });
-        const long long c = r * nx + x;
-        int cls;
-        uint32_t fl;
-        cell_class(p.mask, p.cls, c, cls, fl);
-        if (fl & kZeroGradXp) {
+    R sc, isc;
+    storage_scale<S>(p, sc, isc);
+    for (long long k = 0; first + k * stride < groups; ++k) {
+        const long long g = first + k * stride;
+        const int s = (int)(k % NS);
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1))) {
+            if (lane == 0) atomicExch(err, kRowPipeTimeout);
+            // wait, briefly and bounded, for copies that may still land in this CTA's stages
+            for (int j = 1; j < NS && first + (k + j) * stride < groups; ++j)
+                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1), 1LL << 28)) break;
+            return;
+        }
+        const int y0 = (int)(g % gy) * B, z = (int)(g / gy);
+        const int nb = ny - y0 < B ? ny - y0 : B;
+#pragma unroll 1
+        for (int b = 0; b < nb; ++b) {
+            const S* st = in + (long long)s * Q * SB + b * PITCH;  // direction i at st[i * SB]
+            R v[Q];
             static_for<Q>([&](auto I) {
                 constexpr int i = I;
-                if constexpr (L::cx(i) == -1) v[i] = Codec<S>::dev(st[i * PITCH + x], R(L::w(i)), R(p.inv_scale));
+                constexpr int cx = L::cx(i);
+                const int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
+                v[i] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
             });
-        }
-        R out[Q];
-        if constexpr (COLL == 0) {
-            bgk_collide<L, false>(p, cls, fl, v, out);
-        } else {
-            R T[27];
-            static_for<27>([&](auto I) {
-                constexpr int i = I;
-                T[L::slot(i)] = v[i];
-            });
-            mrt_collide<COLL == 1 ? kMrtRef : kMrtGramSchmidt>(p, cls, fl, T, out);
-            if (fl & kBounce) {
-                static_for<Q - 1>([&](auto I) {
-                    constexpr int i = I + 1;
-                    constexpr int cx = L::cx(i);
-                    int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
-                    if (cx == -1 && (fl & kZeroGradXp)) xs = x;
-                    out[L::opp(i)] = Codec<S>::dev(st[i * PITCH + xs], R(L::w(i)), R(p.inv_scale));
+            const int cls = has_mask ? (int)mask_st[s * SB + b * PITCH + x] : 0;
+            const uint32_t fl = p.cls.flags[cls];
+            if (fl & kZeroGradXp) {
+                static_for<Q>([&](auto I) {
+                    constexpr int i = I;
+                    if constexpr (L::cx(i) == -1) v[i] = Codec<S>::raw(st[i * SB + x], R(L::w(i)));
                 });
             }
+            R out[Q];
+            if constexpr (COLL == 0) {
+                bgk_collide<L, false>(p, cls, fl, v, sc, isc, out);
+            } else {
+                R T[27];
+                static_for<27>([&](auto I) {
+                    constexpr int i = I;
+                    T[L::slot(i)] = v[i];
+                });
+                mrt_collide<COLL == 1 ? kMrtRef : kMrtGramSchmidt>(p, cls, fl, T, sc, isc, out);
+                if (fl & kBounce) {
+                    static_for<Q - 1>([&](auto I) {
+                        constexpr int i = I + 1;
+                        constexpr int cx = L::cx(i);
+                        int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
+                        if (cx == -1 && (fl & kZeroGradXp)) xs = x;
+                        out[L::opp(i)] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
+                    });
+                }
+            }
+            S* __restrict__ fo = static_cast<S*>(p.fout) + ((long long)z * ny + y0 + b) * nx + x;
+            static_for<Q>([&](auto I) {
+                constexpr int i = I;
+                fo[(long long)i * p.N] = Codec<S>::enc(out[i], R(L::w(i)));
+            });
         }
-
-        // (B) every thread is done with input stage s; warp 0's wait on output stage o is visible
-        if (__syncthreads_or(!ok)) {
-            dead = true;
-            break;
+        // This warp is done reading stage s.  The last warp out refills it with group k + NS.
+        __syncwarp();
+        unsigned int before = 0;
+        if (lane == 0) {
+            __threadfence_block();
+            before = atomicAdd(&done[s], 1u);
         }
-        if (warp == 0 && r + NS * stride < rows) issue(r + NS * stride, s);
-
-        S* so = outs + (long long)o * Q * PITCH;
-        static_for<Q>([&](auto I) {
-            constexpr int i = I;
-            Codec<S>::store_dev(so + i * PITCH + x, out[i], R(L::w(i)), R(p.scale));
-        });
-        fence_proxy_async_smem();
-        __syncthreads();  // (C) output stage o complete
-        if (warp == 0) {
-            if (lane < Q) bulk_store(fout + (long long)lane * p.N + r * nx, so + lane * PITCH, row_bytes);
-            bulk_commit();
-            bulk_wait_read_1();  // output stage o^1 is free for the next row (NO == 2)
+        before = __shfl_sync(0xffffffffu, before, 0);
+        if (before == W - 1) {
+            __threadfence_block();
+            if (lane == 0) done[s] = 0;
+            fence_proxy_async_smem();  // order the warps' shared reads before the async-proxy writes
+            if (g + NS * stride < groups) issue(g + NS * stride, s);
         }
     }
-    if (dead) {
-        if (x == 0) atomicExch(err, kRowPipeTimeout);
-        // drain the loads this CTA issued (iterations k .. k+NS-1) with bounded waits
-        for (int j = 0; j < NS; ++j) {
-            const long long kk = k + j;
-            if (first + kk * stride >= rows) break;
-            if (!mbar_wait_bounded(&full[kk % NS], (uint32_t)((kk / NS) & 1))) break;
-        }
-    }
-    if (warp == 0) bulk_wait_all();
 }
 
 }  // namespace lbm

@@ -162,13 +162,16 @@ static StepParams<R> make_params(const lbm_ctx* c) {
     if (d.collision == LBM_MRT) {
         MrtCoef<double> k;
         mrt_coefficients(d.mrt_basis, d.mrt_s, k);
+        // 16-bit storages carry (f - w) * scale through the (linear) transform; the equilibrium
+        // moments are formed unscaled, so their coefficients take the scale (a power of two: exact).
+        const double es = (d.storage == LBM_F16S || d.storage == LBM_BF16S) ? c->scale : 1.0;
         for (int t = 0; t < 27; ++t) {
             p.mrt.alpha[t] = R(k.alpha[t]);
-            p.mrt.beta[t] = R(k.beta[t]);
+            p.mrt.beta[t] = R(k.beta[t] * es);
         }
         for (int t = 0; t < 9; ++t) {
             p.mrt.A[t] = R(k.A[t]);
-            p.mrt.B[t] = R(k.B[t]);
+            p.mrt.B[t] = R(k.B[t] * es);
         }
     }
     return p;
@@ -197,7 +200,7 @@ template <class S, int PITCH, int COLL>
 static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s) {
     auto kern = k_step_rows<D3Q27, S, PITCH, COLL>;
     constexpr size_t smem = rowpipe_smem_bytes<D3Q27, S, PITCH>();
-    kern<<<c->rows_grid, PITCH, smem, s>>>(p, c->err);
+    kern<<<c->rows_grid, PITCH, smem, s>>>(p, c->err);  // one thread per x
 }
 
 template <class S, int PITCH, int COLL>
@@ -209,8 +212,9 @@ static int prepare_rows_t(lbm_ctx* c) {
     LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PITCH, smem));
     LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->d.device));
     if (per_sm < 1) return set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
-    const long long rows = c->d.ny * c->d.nz;
-    c->rows_grid = (int)std::min<long long>(rows, (long long)per_sm * sms);
+    constexpr int B = RowPipeShape<S, PITCH>::B;
+    const long long groups = (c->d.ny + B - 1) / B * c->d.nz;
+    c->rows_grid = (int)std::min<long long>(groups, (long long)per_sm * sms);
     return LBM_OK;
 }
 
