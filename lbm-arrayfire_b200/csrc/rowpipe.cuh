@@ -6,19 +6,21 @@
 // run of memory, split in two where the group wraps around y.  The x shift of the pull (af::shift
 // semantics, periodic in x) becomes an index offset inside the staged rows.
 //
-// The rows arrive by `cp.async.bulk` global->shared copies (one or two per direction per group, plus
-// the mask rows) into a ring of NS shared-memory stages; each stage's completion is counted in bytes
-// on an mbarrier (full[s]).  The warps wait on full[s], read the staged populations with
-// immediate-offset shared loads, collide and store their cells straight to global memory (coalesced
-// along x).  There is no producer warp: every warp bumps a shared counter when it is done with a
-// stage, and the warp that empties it issues the refill for the group NS steps ahead.  (Measured on
-// B200: a dedicated producer warp spent ~13% of the SM's issue slots polling its barrier, and staging
-// the outputs for bulk stores was slower than direct stores, 25 vs 29 GLUPS for FP32 MRT at 256^3,
-// because the copy engine's request rate, not the bytes, was the limit.)  For the same reason a group
-// spans 1-2 KB per direction (B rows) so each bulk load moves a useful amount.
+// Warp specialisation: one producer warp issues `cp.async.bulk` global->shared copies (one or two per
+// direction per group, plus the mask rows) into a ring of NS shared-memory stages; each stage's
+// completion is counted in bytes on an mbarrier (full[s]).  The consumer warps wait on full[s], read
+// the staged populations with immediate-offset shared loads, collide, store their cells straight to
+// global memory (coalesced along x) and release the stage on empty[s]; the producer refills a stage as
+// soon as empty[s] completes.  Measured on B200 (MRT, 256^3), against the alternatives:
+//   - staging the outputs for bulk stores too: 25 vs 29 GLUPS (FP32) — the copy engine's request
+//     rate, not the bytes, was the limit; for the same reason a group spans 1-2 KB per direction;
+//   - no producer warp, the last consumer warp out of a stage refilling it: 40 vs 44 GLUPS (F16S),
+//     25 vs 28 GLUPS (FP32) — the refill then waits for the slowest warp of the CTA.
+// Compared with the one-cell-per-thread kernel this removes the per-population 64-bit load-address
+// arithmetic and decouples memory latency from occupancy.
 //
 // Every wait on an mbarrier is bounded (about two seconds); a warp that times out records
-// kRowPipeTimeout in *err, waits (bounded) for the copies into this CTA's stages and returns.
+// kRowPipeTimeout in *err and returns (consumers after a bounded wait for copies into their stages).
 // No multicast: every copy moves data of this GPU's own memory into this CTA's shared memory.
 #pragma once
 
@@ -69,8 +71,8 @@ __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src_gmem, 
                  "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
                  : "memory");
 }
-__device__ __forceinline__ void fence_proxy_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
 // (cy, cz) of direction i packed two bits each, so a lane can look its own up at run time.
@@ -108,7 +110,7 @@ struct RowPipeShape {
                   "row pipeline stages exceed the shared-memory budget");
 };
 
-// barriers and counters | NS population stages | NS mask stages
+// barriers | NS population stages | NS mask stages
 template <class L, class S, int PITCH>
 constexpr size_t rowpipe_smem_bytes() {
     using Sh = RowPipeShape<S, PITCH>;
@@ -116,11 +118,11 @@ constexpr size_t rowpipe_smem_bytes() {
 }
 
 // COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt).  Deviation arithmetic.
-// Requires nx == PITCH; block = PITCH threads (PITCH / 32 warps).
-//   full[s]  tx-count barrier, completed by the bulk loads of stage s
-//   done[s]  warps finished with stage s in its current use; the last one resets it and refills
+// Requires nx == PITCH; block = PITCH consumer threads (one per x) + one producer warp.
+//   full[s]   tx-count barrier, completed by the bulk loads of stage s
+//   empty[s]  every consumer warp has finished reading stage s
 template <class L, class S, int PITCH, int COLL>
-__global__ void __launch_bounds__(PITCH, RowPipeShape<S, PITCH>::CTAS)
+__global__ void __launch_bounds__(PITCH + 32, RowPipeShape<S, PITCH>::CTAS)
     k_step_rows(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int* __restrict__ err) {
     using R = typename Codec<S>::Real;
     using Sh = RowPipeShape<S, PITCH>;
@@ -128,12 +130,12 @@ __global__ void __launch_bounds__(PITCH, RowPipeShape<S, PITCH>::CTAS)
     constexpr int NS = Sh::NS;
     constexpr int B = Sh::B;
     constexpr int SB = B * PITCH;  // elements per direction in a stage
-    constexpr int W = PITCH / 32;  // warps
-    static_assert(NS <= 8, "barriers and counters occupy the first 128 bytes");
+    constexpr int W = PITCH / 32;  // consumer warps
+    static_assert(NS <= 8, "barriers occupy the first 128 bytes");
     constexpr unsigned long long kCy = pack_c<L>(false), kCz = pack_c<L>(true);
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-    unsigned int* done = reinterpret_cast<unsigned int*>(full + NS);
+    uint64_t* empty = full + NS;
     S* in = reinterpret_cast<S*>(smem + 128);                                 // [NS][Q][B][PITCH]
     uint8_t* mask_st = reinterpret_cast<uint8_t*>(in + (size_t)NS * Q * SB);  // [NS][B][PITCH]
     const bool has_mask = p.mask != nullptr;
@@ -173,14 +175,24 @@ __global__ void __launch_bounds__(PITCH, RowPipeShape<S, PITCH>::CTAS)
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) {
             mbar_init(&full[s], 1);
-            done[s] = 0;
+            mbar_init(&empty[s], W);
         }
         mbar_init_fence();
     }
     __syncthreads();
-    if (tid < 32)
+    if (tid >= PITCH) {  // producer warp
         for (int s = 0; s < NS; ++s)
             if (first + s * stride < groups) issue(first + s * stride, s);
+        for (long long k = 0; first + (k + NS) * stride < groups; ++k) {
+            const int s = (int)(k % NS);
+            if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1))) {
+                if (lane == 0) atomicExch(err, kRowPipeTimeout);
+                return;
+            }
+            issue(first + (k + NS) * stride, s);
+        }
+        return;
+    }
 
     const int x = tid;
     const int xm = x == 0 ? nx - 1 : x - 1;
@@ -245,18 +257,7 @@ __global__ void __launch_bounds__(PITCH, RowPipeShape<S, PITCH>::CTAS)
         }
         // This warp is done reading stage s.  The last warp out refills it with group k + NS.
         __syncwarp();
-        unsigned int before = 0;
-        if (lane == 0) {
-            __threadfence_block();
-            before = atomicAdd(&done[s], 1u);
-        }
-        before = __shfl_sync(0xffffffffu, before, 0);
-        if (before == W - 1) {
-            __threadfence_block();
-            if (lane == 0) done[s] = 0;
-            fence_proxy_async_smem();  // order the warps' shared reads before the async-proxy writes
-            if (g + NS * stride < groups) issue(g + NS * stride, s);
-        }
+        if (lane == 0) mbar_arrive(&empty[s]);
     }
 }
 

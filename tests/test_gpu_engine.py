@@ -237,6 +237,30 @@ def test_row_pipeline_equals_plain_kernel(storage, coll):
     assert np.array_equal(out[lb.KERNEL_PLAIN], out[lb.KERNEL_ROWS])
 
 
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S])
+@pytest.mark.parametrize("coll", ["bgk", "mrt_gs"])
+def test_row_pipeline_ring_wraps_equal_plain_kernel(storage, coll):
+    """A lattice with ~20x more row groups than resident CTAs, so every CTA cycles through its
+    shared-memory stage ring many times (refills, barrier phases, short last group of each plane):
+    still bit-identical to the one-cell-per-thread kernel."""
+    shape = (256, 126, 48)  # 126 = 31 groups of 4 + one of 2 (16-bit), 126 groups of 1 (F32)
+    if coll == "bgk":
+        d = lb.make_desc(lb.D3Q27, lb.BGK, storage, shape, omega=1.7)
+    else:
+        d = lb.make_desc(lb.D3Q27, lb.MRT, storage, shape, mrt_s=lb.mrt_rates(1.8, 1.2),
+                         mrt_basis=lb.MRT_GRAM_SCHMIDT)
+    m = lb.setup_cavity3d(d, 0.08)
+    out = {}
+    for kind in (lb.KERNEL_PLAIN, lb.KERNEL_ROWS):
+        with lb.Lattice(d, m) as lat:
+            lat.set_kernel(kind)
+            lat.step(12)
+            lat.sync()
+            out[kind] = lat.get_populations(np.float32)
+    assert np.isfinite(out[lb.KERNEL_ROWS]).all()
+    assert np.array_equal(out[lb.KERNEL_PLAIN], out[lb.KERNEL_ROWS])
+
+
 def test_row_pipeline_needs_eligible_shape():
     d, m, F0 = cavity2d(n=64)
     with lb.Lattice(d, m) as lat:
