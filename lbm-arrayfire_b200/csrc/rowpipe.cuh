@@ -58,6 +58,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return done != 0;
 }
 // Bounded wait: false after `limit` clocks (2^32 is about two seconds) without completion.
+// (An explicit __nanosleep back-off between polls was measured: no change in throughput.)
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit = 1LL << 32) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
@@ -89,24 +90,40 @@ constexpr unsigned long long pack_c(bool z) {
 #ifndef LBM_ROWPIPE_NS
 #define LBM_ROWPIPE_NS 0  // stages; 0 = as many as the shared-memory budget holds
 #endif
+#ifndef LBM_ROWPIPE_CR
+#define LBM_ROWPIPE_CR 0  // consumer row sets per CTA (CR x PITCH consumer threads); 0 = per storage type
+#endif
 
-// Rows per group B, stage bytes and stages NS.  Measured on B200 (MRT, 256^3): 16-bit storage is
-// limited by the bulk-copy request rate and gains from the largest copies (2 KB per direction: 43 vs
-// 33 GLUPS at 512 B); FP32 runs at ~0.9 of the copy bandwidth and does best with 1 KB copies and
-// three stages (~83 KB) per CTA.  Two CTAs share an SM for nx <= 256, one CTA has it for nx = 512.
+// Rows per group B, consumer row sets CR, stage bytes and stages NS.  Measured on B200 (MRT, 256^3):
+// the size of each per-direction bulk copy matters most — every copy is a separate DRAM stream, so
+// small copies lose row-buffer locality (F16S: 512 B 33 GLUPS, 1 KB 34-42, 2 KB 44, 4 KB 44.5).
+// FP32 reaches 0.97 of the measured copy bandwidth with 2 KB copies (2 rows), two consumer row sets
+// and three stages in one CTA per SM (28.0 -> 29.0 GLUPS against one row set and 1 KB copies);
+// 16-bit storage keeps one row set, 4-row groups and two stages in each of two CTAs per SM.
 template <class S, int PITCH>
 struct RowPipeShape {
     static constexpr bool k16 = sizeof(S) == 2;
     static constexpr int kRowBytes = PITCH * (int)sizeof(S);
     static constexpr int kGroupBytes = LBM_ROWPIPE_GROUP_BYTES > 0 ? LBM_ROWPIPE_GROUP_BYTES : (k16 ? 2048 : 1024);
-    static constexpr int B0 = kGroupBytes / kRowBytes;
-    static constexpr int B = B0 < 1 ? 1 : (B0 > 4 ? 4 : B0);
-    static constexpr int CTAS = PITCH <= 256 ? 2 : 1;
-    static constexpr int STAGE = 27 * B * kRowBytes;
+    // consumer row sets: CR groups of PITCH threads take rows b = r, r + CR, ... of a group
+    static constexpr int CRQ = LBM_ROWPIPE_CR > 0 ? LBM_ROWPIPE_CR : (k16 ? 1 : 2);
+    static constexpr int CR0 = CRQ * PITCH > 512 ? 512 / PITCH : CRQ;
+    static constexpr int CR = CR0 < 1 ? 1 : CR0;
+    static constexpr int CONSUMERS = CR * PITCH;
+    static constexpr int CTAS = CONSUMERS <= 256 ? 2 : 1;
+    static constexpr int kLimit = (CTAS == 2 ? 112 : 224) * 1024;  // shared memory per CTA
     static constexpr int kBudget = (CTAS == 2 ? (k16 ? 110 : 83) : (k16 ? 216 : 166)) * 1024;
+    // rows per group: the requested copy size, at least one row per row set, two stages must fit
+    static constexpr int B0 = kGroupBytes / kRowBytes;
+    static constexpr int B1 = B0 < CR ? CR : B0;
+    static constexpr int BMAX0 = (kLimit - 128) / (2 * (27 * kRowBytes + PITCH));
+    static constexpr int BMAX = BMAX0 > 8 ? 8 : BMAX0;
+    static constexpr int B = B1 > BMAX ? BMAX : (B1 < 1 ? 1 : B1);
+    static constexpr int STAGE = 27 * B * kRowBytes;
     static constexpr int NS0 = LBM_ROWPIPE_NS > 0 ? LBM_ROWPIPE_NS : kBudget / STAGE;
     static constexpr int NS = NS0 < 2 ? 2 : (NS0 > 8 ? 8 : NS0);
-    static_assert((size_t)NS * (STAGE + B * PITCH) + 128 <= (CTAS == 2 ? 112 : 224) * 1024,
+    static_assert(B >= 1, "a row group must fit twice into shared memory");
+    static_assert((size_t)NS * (STAGE + B * PITCH) + 128 <= (size_t)kLimit,
                   "row pipeline stages exceed the shared-memory budget");
 };
 
@@ -118,11 +135,11 @@ constexpr size_t rowpipe_smem_bytes() {
 }
 
 // COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt).  Deviation arithmetic.
-// Requires nx == PITCH; block = PITCH consumer threads (one per x) + one producer warp.
+// Requires nx == PITCH; block = CR x PITCH consumer threads (one per x and row set) + one producer warp.
 //   full[s]   tx-count barrier, completed by the bulk loads of stage s
 //   empty[s]  every consumer warp has finished reading stage s
 template <class L, class S, int PITCH, int COLL>
-__global__ void __launch_bounds__(PITCH + 32, RowPipeShape<S, PITCH>::CTAS)
+__global__ void __launch_bounds__(RowPipeShape<S, PITCH>::CONSUMERS + 32, RowPipeShape<S, PITCH>::CTAS)
     k_step_rows(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int* __restrict__ err) {
     using R = typename Codec<S>::Real;
     using Sh = RowPipeShape<S, PITCH>;
@@ -130,7 +147,8 @@ __global__ void __launch_bounds__(PITCH + 32, RowPipeShape<S, PITCH>::CTAS)
     constexpr int NS = Sh::NS;
     constexpr int B = Sh::B;
     constexpr int SB = B * PITCH;  // elements per direction in a stage
-    constexpr int W = PITCH / 32;  // consumer warps
+    constexpr int CR = Sh::CR;
+    constexpr int W = Sh::CONSUMERS / 32;  // consumer warps
     static_assert(NS <= 8, "barriers occupy the first 128 bytes");
     constexpr unsigned long long kCy = pack_c<L>(false), kCz = pack_c<L>(true);
     extern __shared__ __align__(128) unsigned char smem[];
@@ -180,7 +198,7 @@ __global__ void __launch_bounds__(PITCH + 32, RowPipeShape<S, PITCH>::CTAS)
         mbar_init_fence();
     }
     __syncthreads();
-    if (tid >= PITCH) {  // producer warp
+    if (tid >= Sh::CONSUMERS) {  // producer warp
         for (int s = 0; s < NS; ++s)
             if (first + s * stride < groups) issue(first + s * stride, s);
         for (long long k = 0; first + (k + NS) * stride < groups; ++k) {
@@ -194,7 +212,7 @@ __global__ void __launch_bounds__(PITCH + 32, RowPipeShape<S, PITCH>::CTAS)
         return;
     }
 
-    const int x = tid;
+    const int x = tid % PITCH, rset = tid / PITCH;
     const int xm = x == 0 ? nx - 1 : x - 1;
     const int xp = x == nx - 1 ? 0 : x + 1;
     R sc, isc;
@@ -212,7 +230,7 @@ __global__ void __launch_bounds__(PITCH + 32, RowPipeShape<S, PITCH>::CTAS)
         const int y0 = (int)(g % gy) * B, z = (int)(g / gy);
         const int nb = ny - y0 < B ? ny - y0 : B;
 #pragma unroll 1
-        for (int b = 0; b < nb; ++b) {
+        for (int b = rset; b < nb; b += CR) {
             const S* st = in + (long long)s * Q * SB + b * PITCH;  // direction i at st[i * SB]
             R v[Q];
             static_for<Q>([&](auto I) {

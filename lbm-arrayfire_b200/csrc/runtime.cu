@@ -200,7 +200,8 @@ template <class S, int PITCH, int COLL>
 static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s) {
     auto kern = k_step_rows<D3Q27, S, PITCH, COLL>;
     constexpr size_t smem = rowpipe_smem_bytes<D3Q27, S, PITCH>();
-    kern<<<c->rows_grid, PITCH + 32, smem, s>>>(p, c->err);  // one thread per x
+    constexpr int threads = RowPipeShape<S, PITCH>::CONSUMERS + 32;  // consumers + one producer warp
+    kern<<<c->rows_grid, threads, smem, s>>>(p, c->err);
 }
 
 template <class S, int PITCH, int COLL>
@@ -209,7 +210,7 @@ static int prepare_rows_t(lbm_ctx* c) {
     constexpr size_t smem = rowpipe_smem_bytes<D3Q27, S, PITCH>();
     LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0, sms = 0;
-    LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PITCH + 32, smem));
+    LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RowPipeShape<S, PITCH>::CONSUMERS + 32, smem));
     LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->d.device));
     if (per_sm < 1) return set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
     constexpr int B = RowPipeShape<S, PITCH>::B;
