@@ -447,13 +447,15 @@ def run_ours(args, rank, world, local_rank):
     }
     # FP32 plain beside the 16-bit headline
     if head_storage != lb.F32 and not args.no_compare:
-        d32, lat32, el32, _ = measure(torch, lb, args, lb.F32, dev, world)
+        d32, lat32, el32, clocks32 = measure(torch, lb, args, lb.F32, dev, world, sample_clocks=(rank == 0))
+        family32 = KERNEL_NAMES.get(lat32.kernel(), "unknown")
         lat32.close()
         del lat32
         v32 = world * N * args.steps / el32 / 1e6
         b32 = algorithmic_bytes_per_cell(d32)
         a32 = b32 * N / launches_per_step / (el32 / (args.steps * launches_per_step)) / 1e9
         out["fp32_plain"] = {"value": v32, "unit": "MLUPS", "ms_per_step": el32 * 1e3 / args.steps,
+                             "kernel_family": family32, "clocks": clocks32,
                              "roofline": {"achieved": a32, "peak": peak, "frac": a32 / peak,
                                           "traffic": dram_traffic(args.workload, lb.F32)}}
         out[f"speedup_{STORAGE_NAMES[head_storage]}_vs_f32"] = value / v32

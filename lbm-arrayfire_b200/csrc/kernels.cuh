@@ -13,6 +13,7 @@
 
 #include <cstdint>
 
+#include "arith.cuh"
 #include "codec.cuh"
 #include "lattice.cuh"
 #include "mrt.cuh"
@@ -103,19 +104,37 @@ __device__ __forceinline__ void pull_zerograd(const S* __restrict__ fin, const P
 // Moments (cpp/d2q9_bgk_lid.cpp:131-138): rho = sum f, j = sum c f, u = j / rho.  On deviations
 // sum d = rho - 1 and sum c d = j (sum c w = 0).  Both rho and drho = rho - 1 are returned.
 // isc: 1 / storage scale of raw deviations (a power of two, so the rescaled sums are exact).
+// The sums start from their first term (not from zero): no 0 + x whose folding could depend on the
+// compiler's context.
+template <class L, int AXIS>
+LBM_HD constexpr int first_moving(int) {
+    for (int i = 0; i < L::Q; ++i)
+        if ((AXIS == 0 ? L::cx(i) : AXIS == 1 ? L::cy(i) : L::cz(i)) != 0) return i;
+    return L::Q;
+}
+template <class L, int AXIS, class R>
+__device__ __forceinline__ R momentum_sum(const R (&v)[L::Q]) {
+    constexpr int f = first_moving<L, AXIS>(0);
+    if constexpr (f == L::Q) {
+        return R(0);
+    } else {
+        constexpr int cf = AXIS == 0 ? L::cx(f) : AXIS == 1 ? L::cy(f) : L::cz(f);
+        R j = cf == 1 ? v[f] : -v[f];
+        static_for<L::Q>([&](auto I) {
+            constexpr int i = I;
+            constexpr int c = AXIS == 0 ? L::cx(i) : AXIS == 1 ? L::cy(i) : L::cz(i);
+            if constexpr (i > f && c == 1) j = j + v[i];
+            if constexpr (i > f && c == -1) j = j - v[i];
+        });
+        return j;
+    }
+}
+
 template <class L, bool ABS, class R>
 __device__ __forceinline__ void moments(const R (&v)[L::Q], R isc, R& rho, R& drho, R& ux, R& uy, R& uz) {
-    R r = R(0), jx = R(0), jy = R(0), jz = R(0);
-    static_for<L::Q>([&](auto I) {
-        constexpr int i = I;
-        r += v[i];
-        if constexpr (L::cx(i) == 1) jx += v[i];
-        if constexpr (L::cx(i) == -1) jx -= v[i];
-        if constexpr (L::cy(i) == 1) jy += v[i];
-        if constexpr (L::cy(i) == -1) jy -= v[i];
-        if constexpr (L::cz(i) == 1) jz += v[i];
-        if constexpr (L::cz(i) == -1) jz -= v[i];
-    });
+    R r = v[0];
+    static_for<L::Q - 1>([&](auto I) { r = r + v[I + 1]; });
+    R jx = momentum_sum<L, 0>(v), jy = momentum_sum<L, 1>(v), jz = momentum_sum<L, 2>(v);
     if constexpr (ABS) {
         rho = r;
         drho = r - R(1);
@@ -162,12 +181,13 @@ __device__ __forceinline__ R feq_abs_i(R rho, R usq15, R ux, R uy, R uz) {
 // Deviation equilibrium feq_i - w_i = w_i ((rho - 1) + rho (4.5 eu^2 - 1.5 u^2)) +- w_i rho 3 eu,
 // evaluated once per pair of opposite directions: the symmetric part is shared and the
 // momentum-carrying part is exactly antisymmetric.  sc: storage scale of the result (power of two).
+// Every multiply-add is explicit (mad): the rounding is fixed by the source (arith.cuh).
 template <class L, class R>
 __device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz, R sc, R (&fe)[L::Q]) {
-    const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
+    const R nusq15 = R(-1.5) * mad(uz, uz, mad(uy, uy, ux * ux));
     const R rho3 = R(3) * rho;
     const R rho45 = R(4.5) * rho;
-    const R base = drho - rho * usq15;
+    const R base = mad(rho, nusq15, drho);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
         constexpr int o = L::opp(i);
@@ -175,15 +195,14 @@ __device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz,
             fe[0] = (R(L::w(0)) * sc) * base;
         } else if constexpr (i < o) {
             constexpr int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
-            R eu = R(0);
-            if constexpr (cx == 1) eu = eu + ux;
-            if constexpr (cx == -1) eu = eu - ux;
-            if constexpr (cy == 1) eu = eu + uy;
-            if constexpr (cy == -1) eu = eu - uy;
-            if constexpr (cz == 1) eu = eu + uz;
-            if constexpr (cz == -1) eu = eu - uz;
+            // c.u from its first nonzero term (no 0 + x)
+            R eu = cx != 0 ? (cx == 1 ? ux : -ux) : (cy != 0 ? (cy == 1 ? uy : -uy) : (cz == 1 ? uz : -uz));
+            if constexpr (cx != 0 && cy == 1) eu = eu + uy;
+            if constexpr (cx != 0 && cy == -1) eu = eu - uy;
+            if constexpr ((cx != 0 || cy != 0) && cz == 1) eu = eu + uz;
+            if constexpr ((cx != 0 || cy != 0) && cz == -1) eu = eu - uz;
             const R w = R(L::w(i)) * sc;
-            const R sym = w * (base + rho45 * (eu * eu));
+            const R sym = w * mad(rho45, eu * eu, base);
             const R anti = w * (rho3 * eu);
             fe[i] = sym + anti;
             fe[o] = sym - anti;
@@ -262,7 +281,7 @@ __device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, co
     const R omega = R(p.omega), one_m = R(p.one_m_omega);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
-        out[i] = (fl & kEquilibrium) ? fe[i] : omega * fe[i] + one_m * v[i];
+        out[i] = (fl & kEquilibrium) ? fe[i] : mad(omega, fe[i], one_m * v[i]);
     });
     if (fl & kBounce) {
         // F(REFLECTED) = BOUNCEDBACK; w_opp(i) = w_i, so deviations bounce like populations
@@ -311,16 +330,23 @@ __global__ void __launch_bounds__(512) k_step_bgk(const __grid_constant__ StepPa
 // to the caller (it needs the streamed values, which the transform overwrote).  The deviations are in
 // storage units (times sc); the transform is linear, so the scale rides along and enters only through
 // isc here and through the equilibrium coefficients (beta and B carry sc, set on the host).
-template <int BASIS, class P, class R>
-__device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R (&T)[27], R sc, R isc,
-                                            R (&out)[27]) {
-    using L = D3Q27;
+// Forward transform and the cell quantities: rho, rho - 1 and u from the moments of slots 0, 1, 3, 9.
+template <int BASIS, class R>
+__device__ __forceinline__ void mrt_pre(R (&T)[27], R isc, R& rho, R& drho, R& ux, R& uy, R& uz) {
     mrt_forward<BASIS>(T);
-    R drho = T[0] * isc;
-    R rho = R(1) + drho;
+    drho = T[0] * isc;
+    rho = R(1) + drho;
     const R inv = isc / rho;
-    R ux = T[1] * inv, uy = T[3] * inv, uz = T[9] * inv;
-    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 3);
+    ux = T[1] * inv;
+    uy = T[3] * inv;
+    uz = T[9] * inv;
+}
+
+// Relaxation towards the equilibrium moments of (rho, u), inverse transform, direction order.
+template <int BASIS, class R, class K>
+__device__ __forceinline__ void mrt_post(R (&T)[27], R rho, R drho, R ux, R uy, R uz, const MrtCoef<K>& k,
+                                         R (&out)[27]) {
+    using L = D3Q27;
     R q[11];
     q[0] = drho;
     q[1] = rho * ux;
@@ -332,13 +358,23 @@ __device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R 
     q[7] = q[1] * uy;
     q[8] = q[1] * uz;
     q[9] = q[2] * uz;
-    q[10] = ux * ux + uy * uy + uz * uz;
-    mrt_relax<BASIS>(T, q, p.mrt);
+    q[10] = mad(uz, uz, mad(uy, uy, ux * ux));
+    mrt_relax<BASIS>(T, q, k);
     mrt_inverse<BASIS>(T);
     static_for<27>([&](auto I) {
         constexpr int i = I;
         out[i] = T[L::slot(i)];
     });
+}
+
+template <int BASIS, class P, class R>
+__device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R (&T)[27], R sc, R isc,
+                                            R (&out)[27]) {
+    using L = D3Q27;
+    R rho, drho, ux, uy, uz;
+    mrt_pre<BASIS>(T, isc, rho, drho, ux, uy, uz);
+    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 3);
+    mrt_post<BASIS>(T, rho, drho, ux, uy, uz, p.mrt, out);
     if (fl & kEquilibrium) equilibrium_dev<L, R>(rho, drho, ux, uy, uz, sc, out);
 }
 

@@ -18,6 +18,7 @@
 
 #include <cmath>
 
+#include "arith.cuh"
 #include "lattice.cuh"
 
 namespace lbm {
@@ -100,8 +101,7 @@ LBM_HD constexpr double mrt_meq_coef(int basis, int t, int k) {
 // form, but stays one instruction (the compiler turns 2v into v + v otherwise).
 template <class R>
 LBM_HD R minus_twice(R s, R v) {
-    using std::fma;
-    return fma(R(-2), v, s);
+    return mad(R(-2), v, s);
 }
 
 template <int BASIS, class R>
@@ -166,32 +166,70 @@ struct MrtCoef {
     R alpha[27], beta[27], A[9], B[9];
 };
 
-// Equilibrium moment of slot T from the cell quantities q[0..10].
-template <int BASIS, int T, class R>
-LBM_HD R mrt_meq(const R (&q)[11]) {
-    R acc = R(0);
-    static_for<11>([&](auto K) {
-        constexpr double c = mrt_meq_coef(BASIS, T, K);
-        if constexpr (c != 0.0) acc = acc + R(c) * q[K];
-    });
-    return acc;
+// First quantity with a nonzero coefficient in the equilibrium moment of slot t (11: none).
+LBM_HD constexpr int mrt_meq_first(int basis, int t) {
+    for (int k = 0; k < 11; ++k)
+        if (mrt_meq_coef(basis, t, k) != 0.0) return k;
+    return 11;
 }
 
-// m* = relaxed, scaled moments.  q: cell quantities for the equilibrium.
-template <int BASIS, class R>
-LBM_HD void mrt_relax(R (&T)[27], const R (&q)[11], const MrtCoef<R>& k) {
+// Equilibrium moment of slot T from the cell quantities q[0..10]: a chain of explicit multiply-adds
+// (unit coefficients as plain adds), the same IEEE operations for every real type.
+template <int BASIS, int T, class R>
+LBM_HD R mrt_meq(const R (&q)[11]) {
+    constexpr int k0 = mrt_meq_first(BASIS, T);
+    if constexpr (k0 == 11) {
+        return R(0);
+    } else {
+        constexpr double c0 = mrt_meq_coef(BASIS, T, k0);
+        R acc;
+        if constexpr (c0 == 1.0)
+            acc = q[k0];
+        else if constexpr (c0 == -1.0)
+            acc = -q[k0];
+        else
+            acc = R(c0) * q[k0];
+        static_for<11>([&](auto K) {
+            constexpr int kk = K;
+            constexpr double c = mrt_meq_coef(BASIS, T, kk);
+            if constexpr (kk > k0 && c != 0.0) {
+                if constexpr (c == 1.0)
+                    acc = acc + q[kk];
+                else if constexpr (c == -1.0)
+                    acc = acc - q[kk];
+                else
+                    acc = mad(R(c), q[kk], acc);
+            }
+        });
+        return acc;
+    }
+}
+
+// m* = relaxed, scaled moments.  q: cell quantities for the equilibrium.  K: coefficient type (the
+// scalar of R).
+template <int BASIS, class R, class K>
+LBM_HD void mrt_relax(R (&T)[27], const R (&q)[11], const MrtCoef<K>& k) {
     static_for<27>([&](auto TI) {
         constexpr int t = TI;
         if constexpr (mrt_slot_row(t) >= 0) {
             const R e = mrt_meq<BASIS, t>(q);
-            T[t] = k.alpha[t] * T[t] + k.beta[t] * e;
+            T[t] = mad(R(k.alpha[t]), T[t], R(k.beta[t]) * e);
         }
     });
     const R a = T[2], b = T[6], c = T[18];
     const R ea = mrt_meq<BASIS, 2>(q), eb = mrt_meq<BASIS, 6>(q), ec = mrt_meq<BASIS, 18>(q);
-    T[2] = k.A[0] * a + k.A[1] * b + k.A[2] * c + k.B[0] * ea + k.B[1] * eb + k.B[2] * ec;
-    T[6] = k.A[3] * a + k.A[4] * b + k.A[5] * c + k.B[3] * ea + k.B[4] * eb + k.B[5] * ec;
-    T[18] = k.A[6] * a + k.A[7] * b + k.A[8] * c + k.B[6] * ea + k.B[7] * eb + k.B[8] * ec;
+    auto mix = [&](int r) {
+        R acc = R(k.A[3 * r]) * a;
+        acc = mad(R(k.A[3 * r + 1]), b, acc);
+        acc = mad(R(k.A[3 * r + 2]), c, acc);
+        acc = mad(R(k.B[3 * r]), ea, acc);
+        acc = mad(R(k.B[3 * r + 1]), eb, acc);
+        return mad(R(k.B[3 * r + 2]), ec, acc);
+    };
+    const R n2 = mix(0), n6 = mix(1), n18 = mix(2);
+    T[2] = n2;
+    T[6] = n6;
+    T[18] = n18;
 }
 
 }  // namespace lbm

@@ -105,7 +105,7 @@ struct RowPipeShape {
     static constexpr bool k16 = sizeof(S) == 2;
     static constexpr int kRowBytes = PITCH * (int)sizeof(S);
     static constexpr int kGroupBytes = LBM_ROWPIPE_GROUP_BYTES > 0 ? LBM_ROWPIPE_GROUP_BYTES : (k16 ? 2048 : 1024);
-    // consumer row sets: CR groups of PITCH threads take rows b = r, r + CR, ... of a group
+    // consumer row sets: CR sets of PITCH threads take rows b = r, r + CR, ... of a group
     static constexpr int CRQ = LBM_ROWPIPE_CR > 0 ? LBM_ROWPIPE_CR : (k16 ? 1 : 2);
     static constexpr int CR0 = CRQ * PITCH > 512 ? 512 / PITCH : CRQ;
     static constexpr int CR = CR0 < 1 ? 1 : CR0;
