@@ -89,6 +89,8 @@ WORKLOADS = {
     "d2q9_shanchen_1024": (wl_sc1024, "D2Q9 Shan-Chen 1024^2 periodic, G=-5.5, tau=1"),
     "d3q27_bgk_lid_256": (wl_bgk3d, "D3Q27 BGK lid cavity 256^3"),
     "d2q9_lid_8192": (wl_cavity2d_big, "D2Q9 BGK lid cavity 8192^2"),
+    "ensemble_config5": (None, "48 D2Q9 BGK lids L in {64..1024} Re in [100,1000] + 16 D3Q27 BGK channels "
+                               "(4L,L,L) L in {64..192} with sphere d=L/4, inlet 0.04, seed 3"),
 }
 
 STORAGE_NAMES = {0: "f32", 1: "f16s", 2: "bf16s", 3: "f64"}
@@ -241,9 +243,11 @@ def run_reference(args, rank, world):
     import oracle as O
 
     O.lib()
-    # calibrate, then pick a sample lattice so that W + K steps end within ~150 s
+    if args.workload == "ensemble_config5":
+        return run_reference_ensemble(args, world, O)
+    # calibrate, then pick a sample lattice so that W + K steps end within the budget (default 150 s)
     mlups0, _, _, _ = oracle_mlups(args.workload, 1.0)
-    budget_cells = mlups0 * 1e6 * 150.0 / max(1, args.steps + args.warmup)
+    budget_cells = mlups0 * 1e6 * args.ref_seconds / max(1, args.steps + args.warmup)
     if args.workload.startswith("d3q27"):
         side = int(max(8, min(256, math.floor(budget_cells ** (1 / 3)))))
         p, d = oracle_problem_for(args.workload, side)
@@ -263,6 +267,42 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "description": WORKLOADS[args.workload][1], "sample_shape": list(p.shape)},
+        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": threads(), "kind": "port", "sample": sample,
+                         "note": "ArrayFire CPU backend unavailable on this box; C restatement of the reference loop"},
+        "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def run_reference_ensemble(args, world, O):
+    """Reference arm of config 5: the CPU restatement on the smallest member of each lattice family
+    (a D2Q9 lid and a D3Q27 channel of the ensemble), K steps each; MLUPS = cells x steps / time."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import lbm_b200 as lb
+    from helpers import oracle_problem
+
+    members = ensemble_members(lb, lb.F32)
+    picks = []
+    for lat in (lb.D2Q9, lb.D3Q27):
+        d, m, name = min((x for x in members if x[0].lattice == lat), key=lambda x: x[0].cells)
+        picks.append((oracle_problem(d, m), name, d.shape))
+    cells = steps_done = 0
+    dt = 0.0
+    for p, _, _ in picks:
+        F = O.init_equilibrium(p)
+        if args.warmup:
+            F, _, _ = O.run(p, F, args.warmup, dtype=np.float32)
+        t = time.perf_counter()
+        O.run(p, F, args.steps, dtype=np.float32)
+        dt += time.perf_counter() - t
+        cells += p.n
+    value = cells * args.steps / dt / 1e6
+    sample = " + ".join(f"{name} {'x'.join(map(str, shp))}" for _, name, shp in picks) + \
+        f", {args.steps} timed steps each, FP32, {threads()} threads on {cpu_model()}"
+    return {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload][1]},
         "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": threads(), "kind": "port", "sample": sample,
                          "note": "ArrayFire CPU backend unavailable on this box; C restatement of the reference loop"},
         "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -395,11 +435,123 @@ def barrier(torch, world):
 
 
 def reduce_max(torch, value, dev, world):
+    """Max over ranks (the job takes as long as its slowest rank)."""
+    from lbm_b200.shard import max_over_ranks
+
     if world <= 1:
         return value
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{dev}")
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return float(t.item())
+    return max_over_ranks(value, device=f"cuda:{dev}")
+
+
+# ---------------------------------------------------------------------------------------------
+# config 5: batched ensemble
+# ---------------------------------------------------------------------------------------------
+def ensemble_members(lb, storage, seed=3):
+    """48 D2Q9 BGK lid cavities (L uniform in {64, 128, ..., 1024}, Re uniform in [100, 1000], lid 0.1,
+    C++ viscosity rule nu = u L / Re) and 16 D3Q27 BGK channels (4L, L, L), L uniform in
+    {64, 96, 128, 160, 192}, sphere of diameter L/4 centred in the channel, equilibrium inlet 0.04,
+    zero-gradient outlet, nu from Re = 100 on the sphere diameter.  numpy PCG64 seeded with `seed`."""
+    rng = np.random.default_rng(seed)
+    members = []
+    for _ in range(48):
+        L = int(rng.integers(1, 17)) * 64
+        re = float(rng.uniform(100.0, 1000.0))
+        d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (L, L), omega=lb.omega_from_re(0.1, L, re, 0))
+        members.append((d, lb.setup_cavity2d(d, 0.1), f"d2q9_lid_{L}"))
+    for _ in range(16):
+        L = int(rng.choice([64, 96, 128, 160, 192]))
+        diam = L / 4.0
+        nu = 0.04 * diam / 100.0
+        d = lb.make_desc(lb.D3Q27, lb.BGK, storage, (4 * L, L, L), omega=1.0 / (3.0 * nu + 0.5))
+        members.append((d, lb.setup_duct3d(d, 0.04, 2.0 * L, L / 2.0, L / 2.0, diam / 2.0), f"d3q27_channel_{L}"))
+    return members
+
+
+def run_ensemble(args, rank, world, local_rank):
+    """Config 5: every rank advances its LPT share of the ensemble as one batch (one launch per lattice
+    family per step, CUDA graphs); aggregate MLUPS = all cells x steps / max-over-ranks time.  Beside it,
+    the same members stepped one lattice at a time with the plain single-lattice path."""
+    import torch
+
+    import lbm_b200 as lb
+    from lbm_b200.shard import lpt_assign
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    storage = {"f16s": lb.F16S, "f32": lb.F32, "bf16s": lb.BF16S, "f64": lb.F64}[args.storage]
+    peak, peak_kind = peaks()
+    members = ensemble_members(lb, storage)
+    bytes_upd = [algorithmic_bytes_per_cell(d) * d.cells for d, _, _ in members]
+    parts = lpt_assign(bytes_upd, world)
+    mine = [members[k] for k in parts[rank]]
+    total_cells = sum(d.cells for d, _, _ in members)
+    total_bytes = sum(bytes_upd)
+    my_cells = sum(d.cells for d, _, _ in mine)
+
+    def events_time(stream_handle, fn):
+        st = torch.cuda.ExternalStream(stream_handle, device=dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    batch = lb.Batch([d for d, _, _ in mine], [m for _, m, _ in mine])
+    batch.step(max(args.warmup, 1))  # tile autotune + graph capture
+    batch.sync()
+    torch.cuda.synchronize(dev)
+    barrier(torch, world)
+    sampler = ClockSampler(gpu_id_for_smi(torch, dev)) if rank == 0 else None
+    if sampler:
+        time.sleep(0.3)
+    el = events_time(batch.stream(), lambda: batch.step(args.steps))
+    clocks = sampler.stop() if sampler else None
+    torch.cuda.synchronize(dev)
+    barrier(torch, world)
+    el_max = reduce_max(torch, el, dev, world)
+    tile = batch.tile_info()
+    families = len({d.lattice for d, _, _ in mine})
+    batch.close()
+    del batch
+
+    # the same members one lattice at a time (plain single-lattice path, autotuned, graphs)
+    seq = 0.0
+    if not args.no_compare:
+        for d, m, _ in mine:
+            d.device = dev
+            with lb.Lattice(d, m) as lat:
+                lat.step(max(args.warmup, 1))
+                lat.sync()
+                seq += events_time(lat.stream(), lambda: lat.step(args.steps))
+        seq = reduce_max(torch, seq, dev, world)
+
+    value = total_cells * args.steps / el_max / 1e6
+    achieved = total_bytes * args.steps / el_max / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el_max * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "ensemble_config5", "description": WORKLOADS["ensemble_config5"][1],
+                   "members": len(members), "cells": total_cells, "storage": STORAGE_NAMES[storage],
+                   "l2": f"inputs larger than L2: {total_bytes / 2 / 1e9:.2f} GB of populations per buffer set",
+                   "parallelism": f"LPT shards x{world}" if world > 1 else "single GPU",
+                   "members_per_rank": [len(p) for p in parts], "cells_this_rank": my_cells,
+                   "tile_width": tile[0], "tiles": tile[1]},
+        "roofline": {"bound": "hbm", "achieved": achieved / world, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / world / peak, "traffic": None,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6.65 TB/s", "kernel": "k_batch_bgk<D2Q9> + k_batch_bgk<D3Q27>",
+                     "note": "achieved per GPU: algorithmic bytes of all members / max-over-ranks time / ranks"},
+        "gpu_launches": args.steps * families,
+        "clocks": clocks,
+    }
+    if seq > 0:
+        out["sequential_plain"] = {"value": total_cells * args.steps / seq / 1e6, "unit": "MLUPS",
+                                   "seconds": seq, "note": "each member alone through lbm_step, summed"}
+        out["speedup_batched_vs_sequential"] = seq / el_max
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -491,6 +643,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=150.0, help="time budget of the reference arm")
     ap.add_argument("--size", type=int, default=0, help="cube side for D3Q27 workloads (default: the config's)")
     ap.add_argument("--dims", default="", help="NXxNYxNZ for D3Q27 workloads (small cases for profiling)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "rows"], help="step-kernel family")
@@ -516,7 +669,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device(f"cuda:{local_rank}"))
     try:
-        out = run_ours(args, rank, world, local_rank)
+        out = (run_ensemble if args.workload == "ensemble_config5" else run_ours)(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)
     finally:

@@ -85,68 +85,133 @@ constexpr unsigned long long pack_c(bool z) {
 }
 
 #ifndef LBM_ROWPIPE_GROUP_BYTES
-#define LBM_ROWPIPE_GROUP_BYTES 0  // bytes per direction per row group (sets B); 0 = per storage type
+#define LBM_ROWPIPE_GROUP_BYTES 0  // target bytes per direction per row group; 0 = per storage type
 #endif
 #ifndef LBM_ROWPIPE_NS
 #define LBM_ROWPIPE_NS 0  // stages; 0 = as many as the shared-memory budget holds
 #endif
 #ifndef LBM_ROWPIPE_CR
-#define LBM_ROWPIPE_CR 0  // consumer row sets per CTA (CR x PITCH consumer threads); 0 = per storage type
+#define LBM_ROWPIPE_CR 0  // consumer row sets per CTA; 0 = per lattice and storage type
 #endif
 
-// Rows per group B, consumer row sets CR, stage bytes and stages NS.  Measured on B200 (MRT, 256^3):
-// the size of each per-direction bulk copy matters most — every copy is a separate DRAM stream, so
-// small copies lose row-buffer locality (F16S: 512 B 33 GLUPS, 1 KB 34-42, 2 KB 44, 4 KB 44.5).
-// FP32 reaches 0.97 of the measured copy bandwidth with 2 KB copies (2 rows), two consumer row sets
-// and three stages in one CTA per SM (28.0 -> 29.0 GLUPS against one row set and 1 KB copies);
-// 16-bit storage keeps one row set, 4-row groups and two stages in each of two CTAs per SM.
-template <class S, int PITCH>
+// Shape of the row pipeline for lattice L, storage S and shared-memory row pitch PITCH (elements; the
+// lattice's nx is at most PITCH).  Measured on B200 (D3Q27 MRT, 256^3): the size of each
+// per-direction bulk copy matters most — every copy is a separate DRAM stream, so small copies lose
+// row-buffer locality (F16S: 512 B 33 GLUPS, 1 KB 34-42, 2 KB 44, 4 KB 44.5).  FP32 reaches 0.97 of
+// the measured copy bandwidth with 2 KB copies, two consumer row sets and three stages in one CTA per
+// SM; 16-bit storage keeps one row set and two stages in each of two CTAs per SM.
+//   THREADS   consumer threads per row set (one x each; XPT = 2 x positions each for PITCH 1024)
+//   CR        row sets: set r takes rows b = r, r + CR, ... of a group
+//   B         rows per group at nx == PITCH; the host may put more rows of a narrower lattice into
+//             the same stage (runtime rows per group, at most B * PITCH / nx)
+//   NS        stages
+template <class L, class S, int PITCH>
 struct RowPipeShape {
+    static constexpr int Q = L::Q;
     static constexpr bool k16 = sizeof(S) == 2;
+    static constexpr bool k3 = L::DIM == 3;
+    static constexpr int THREADS = PITCH > 512 ? 512 : PITCH;
+    static constexpr int XPT = PITCH / THREADS;
     static constexpr int kRowBytes = PITCH * (int)sizeof(S);
     static constexpr int kGroupBytes = LBM_ROWPIPE_GROUP_BYTES > 0 ? LBM_ROWPIPE_GROUP_BYTES : (k16 ? 2048 : 1024);
-    // consumer row sets: CR sets of PITCH threads take rows b = r, r + CR, ... of a group
-    static constexpr int CRQ = LBM_ROWPIPE_CR > 0 ? LBM_ROWPIPE_CR : (k16 ? 1 : 2);
-    static constexpr int CR0 = CRQ * PITCH > 512 ? 512 / PITCH : CRQ;
+    static constexpr int CRQ = LBM_ROWPIPE_CR > 0 ? LBM_ROWPIPE_CR : (k3 && !k16 ? 2 : 1);
+    static constexpr int CR0 = CRQ * THREADS > 512 ? 512 / THREADS : CRQ;
     static constexpr int CR = CR0 < 1 ? 1 : CR0;
-    static constexpr int CONSUMERS = CR * PITCH;
-    static constexpr int CTAS = CONSUMERS <= 256 ? 2 : 1;
-    static constexpr int kLimit = (CTAS == 2 ? 112 : 224) * 1024;  // shared memory per CTA
-    static constexpr int kBudget = (CTAS == 2 ? (k16 ? 110 : 83) : (k16 ? 216 : 166)) * 1024;
-    // rows per group: the requested copy size, at least one row per row set, two stages must fit
+    static constexpr int CONSUMERS = CR * THREADS;
+    // CTAs per SM: D3Q27 collisions need ~90-120 registers per thread, D2Q9 far fewer
+    static constexpr int CTAS = k3 ? (CONSUMERS <= 256 ? 2 : 1) : (CONSUMERS <= 256 ? 3 : 2);
+    static constexpr int kLimit = (CTAS == 1 ? 224 : CTAS == 2 ? 112 : 74) * 1024;  // smem per CTA
+    static constexpr int kBudget = (CTAS == 1 ? (k16 ? 216 : 166) : CTAS == 2 ? (k16 ? 110 : 83) : 72) * 1024;
     static constexpr int B0 = kGroupBytes / kRowBytes;
     static constexpr int B1 = B0 < CR ? CR : B0;
-    static constexpr int BMAX0 = (kLimit - 128) / (2 * (27 * kRowBytes + PITCH));
+    static constexpr int BMAX0 = (kLimit - 128) / (2 * (Q * kRowBytes + PITCH));
     static constexpr int BMAX = BMAX0 > 8 ? 8 : BMAX0;
     static constexpr int B = B1 > BMAX ? BMAX : (B1 < 1 ? 1 : B1);
-    static constexpr int STAGE = 27 * B * kRowBytes;
-    static constexpr int NS0 = LBM_ROWPIPE_NS > 0 ? LBM_ROWPIPE_NS : kBudget / STAGE;
+    static constexpr int SB = B * PITCH;  // elements per direction in a stage
+    static constexpr int STAGE = Q * SB * (int)sizeof(S) + SB;  // populations + mask bytes
+    static constexpr int NSB = (kBudget < kLimit - 128 ? kBudget : kLimit - 128) / STAGE;
+    static constexpr int NS0 = LBM_ROWPIPE_NS > 0 ? LBM_ROWPIPE_NS : NSB;
     static constexpr int NS = NS0 < 2 ? 2 : (NS0 > 8 ? 8 : NS0);
     static_assert(B >= 1, "a row group must fit twice into shared memory");
-    static_assert((size_t)NS * (STAGE + B * PITCH) + 128 <= (size_t)kLimit,
-                  "row pipeline stages exceed the shared-memory budget");
+    static_assert((size_t)NS * STAGE + 128 <= (size_t)kLimit, "row pipeline stages exceed the shared-memory budget");
+
+    static constexpr size_t smem_bytes() { return 128 + (size_t)NS * STAGE; }
+    // rows per group for a lattice of width nx (host side): the target copy size, at least one row
+    // per row set, within the stage
+    static int rows_per_group(int nx) {
+        const int cap = B * PITCH / nx;
+        int b = kGroupBytes / (nx * (int)sizeof(S));
+        if (b < CR) b = CR;
+        if (b > cap) b = cap;
+        return b < 1 ? 1 : b;
+    }
 };
 
-// barriers | NS population stages | NS mask stages
-template <class L, class S, int PITCH>
-constexpr size_t rowpipe_smem_bytes() {
-    using Sh = RowPipeShape<S, PITCH>;
-    return 128 + (size_t)Sh::NS * L::Q * Sh::B * PITCH * sizeof(S) + (size_t)Sh::NS * Sh::B * PITCH;
+// One cell of the row pipeline: st points at the staged row of direction 0 (direction i at
+// st[i * SB]), mrow at the cell classes of the row, orow at the row's first cell in the output buffer.
+template <class L, class S, int SB, int COLL, class P>
+__device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t* mrow, int x, int nx,
+                                         typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow) {
+    using R = typename Codec<S>::Real;
+    constexpr int Q = L::Q;
+    const int xm = x == 0 ? nx - 1 : x - 1;
+    const int xp = x == nx - 1 ? 0 : x + 1;
+    R v[Q];
+    static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = L::cx(i);
+        const int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
+        v[i] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
+    });
+    const int cls = mrow ? (int)mrow[x] : 0;
+    const uint32_t fl = p.cls.flags[cls];
+    if (fl & kZeroGradXp) {
+        static_for<Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (L::cx(i) == -1) v[i] = Codec<S>::raw(st[i * SB + x], R(L::w(i)));
+        });
+    }
+    R out[Q];
+    if constexpr (COLL == 0) {
+        bgk_collide<L, false>(p, cls, fl, v, sc, isc, out);
+    } else {
+        R T[27];
+        static_for<27>([&](auto I) {
+            constexpr int i = I;
+            T[L::slot(i)] = v[i];
+        });
+        mrt_collide<COLL == 1 ? kMrtRef : kMrtGramSchmidt>(p, cls, fl, T, sc, isc, out);
+        if (fl & kBounce) {
+            static_for<Q - 1>([&](auto I) {
+                constexpr int i = I + 1;
+                constexpr int cx = L::cx(i);
+                int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
+                if (cx == -1 && (fl & kZeroGradXp)) xs = x;
+                out[L::opp(i)] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
+            });
+        }
+    }
+    S* __restrict__ fo = orow + x;
+    static_for<Q>([&](auto I) {
+        constexpr int i = I;
+        fo[(long long)i * p.N] = Codec<S>::enc(out[i], R(L::w(i)));
+    });
 }
 
 // COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt).  Deviation arithmetic.
-// Requires nx == PITCH; block = CR x PITCH consumer threads (one per x and row set) + one producer warp.
+// Requires nx <= PITCH with nx * sizeof(S) a multiple of 16 bytes; `rows` = rows per group
+// (RowPipeShape::rows_per_group).  Block = CR x THREADS consumer threads + one producer warp.
 //   full[s]   tx-count barrier, completed by the bulk loads of stage s
 //   empty[s]  every consumer warp has finished reading stage s
+// Stage s holds, for direction i, the group's source rows at in[(s * Q + i) * SB + b * nx].
 template <class L, class S, int PITCH, int COLL>
-__global__ void __launch_bounds__(RowPipeShape<S, PITCH>::CONSUMERS + 32, RowPipeShape<S, PITCH>::CTAS)
-    k_step_rows(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int* __restrict__ err) {
+__global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, RowPipeShape<L, S, PITCH>::CTAS)
+    k_step_rows(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int rows, int* __restrict__ err) {
     using R = typename Codec<S>::Real;
-    using Sh = RowPipeShape<S, PITCH>;
+    using Sh = RowPipeShape<L, S, PITCH>;
     constexpr int Q = L::Q;
     constexpr int NS = Sh::NS;
-    constexpr int B = Sh::B;
-    constexpr int SB = B * PITCH;  // elements per direction in a stage
+    constexpr int SB = Sh::SB;
     constexpr int CR = Sh::CR;
     constexpr int W = Sh::CONSUMERS / 32;  // consumer warps
     static_assert(NS <= 8, "barriers occupy the first 128 bytes");
@@ -154,13 +219,14 @@ __global__ void __launch_bounds__(RowPipeShape<S, PITCH>::CONSUMERS + 32, RowPip
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
     uint64_t* empty = full + NS;
-    S* in = reinterpret_cast<S*>(smem + 128);                                 // [NS][Q][B][PITCH]
-    uint8_t* mask_st = reinterpret_cast<uint8_t*>(in + (size_t)NS * Q * SB);  // [NS][B][PITCH]
+    S* in = reinterpret_cast<S*>(smem + 128);                                 // [NS][Q][SB]
+    uint8_t* mask_st = reinterpret_cast<uint8_t*>(in + (size_t)NS * Q * SB);  // [NS][SB]
     const bool has_mask = p.mask != nullptr;
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
+    const int B = rows;
     const int gy = (ny + B - 1) / B;  // row groups per z plane; the last one may be short
     const long long groups = (long long)gy * nz;
     const uint32_t row_bytes = (uint32_t)(nx * sizeof(S));
@@ -184,7 +250,7 @@ __global__ void __launch_bounds__(RowPipeShape<S, PITCH>::CONSUMERS + 32, RowPip
             const S* plane = fin + (long long)lane * p.N + (long long)zs * ny * nx;
             S* dst = in + ((long long)s * Q + lane) * SB;
             bulk_load(dst, plane + (long long)ys * nx, (uint32_t)run * row_bytes, &full[s]);
-            if (run < nb) bulk_load(dst + run * PITCH, plane, (uint32_t)(nb - run) * row_bytes, &full[s]);
+            if (run < nb) bulk_load(dst + run * nx, plane, (uint32_t)(nb - run) * row_bytes, &full[s]);
         } else if (lane == Q && has_mask) {
             bulk_load(mask_st + s * SB, p.mask + ((long long)z * ny + y0) * nx, (uint32_t)(nb * nx), &full[s]);
         }
@@ -212,9 +278,7 @@ __global__ void __launch_bounds__(RowPipeShape<S, PITCH>::CONSUMERS + 32, RowPip
         return;
     }
 
-    const int x = tid % PITCH, rset = tid / PITCH;
-    const int xm = x == 0 ? nx - 1 : x - 1;
-    const int xp = x == nx - 1 ? 0 : x + 1;
+    const int tx = tid % Sh::THREADS, rset = tid / Sh::THREADS;
     R sc, isc;
     storage_scale<S>(p, sc, isc);
     for (long long k = 0; first + k * stride < groups; ++k) {
@@ -231,51 +295,17 @@ __global__ void __launch_bounds__(RowPipeShape<S, PITCH>::CONSUMERS + 32, RowPip
         const int nb = ny - y0 < B ? ny - y0 : B;
 #pragma unroll 1
         for (int b = rset; b < nb; b += CR) {
-            const S* st = in + (long long)s * Q * SB + b * PITCH;  // direction i at st[i * SB]
-            R v[Q];
-            static_for<Q>([&](auto I) {
-                constexpr int i = I;
-                constexpr int cx = L::cx(i);
-                const int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
-                v[i] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
-            });
-            const int cls = has_mask ? (int)mask_st[s * SB + b * PITCH + x] : 0;
-            const uint32_t fl = p.cls.flags[cls];
-            if (fl & kZeroGradXp) {
-                static_for<Q>([&](auto I) {
-                    constexpr int i = I;
-                    if constexpr (L::cx(i) == -1) v[i] = Codec<S>::raw(st[i * SB + x], R(L::w(i)));
-                });
+            const S* st = in + (long long)s * Q * SB + b * nx;
+            const uint8_t* mrow = has_mask ? mask_st + s * SB + b * nx : nullptr;
+            S* orow = static_cast<S*>(p.fout) + ((long long)z * ny + y0 + b) * nx;
+#pragma unroll 1
+            for (int xx = 0; xx < Sh::XPT; ++xx) {
+                const int x = tx + xx * Sh::THREADS;
+                if (x < nx) row_cell<L, S, SB, COLL>(p, st, mrow, x, nx, sc, isc, orow);
             }
-            R out[Q];
-            if constexpr (COLL == 0) {
-                bgk_collide<L, false>(p, cls, fl, v, sc, isc, out);
-            } else {
-                R T[27];
-                static_for<27>([&](auto I) {
-                    constexpr int i = I;
-                    T[L::slot(i)] = v[i];
-                });
-                mrt_collide<COLL == 1 ? kMrtRef : kMrtGramSchmidt>(p, cls, fl, T, sc, isc, out);
-                if (fl & kBounce) {
-                    static_for<Q - 1>([&](auto I) {
-                        constexpr int i = I + 1;
-                        constexpr int cx = L::cx(i);
-                        int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
-                        if (cx == -1 && (fl & kZeroGradXp)) xs = x;
-                        out[L::opp(i)] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
-                    });
-                }
-            }
-            S* __restrict__ fo = static_cast<S*>(p.fout) + ((long long)z * ny + y0 + b) * nx + x;
-            static_for<Q>([&](auto I) {
-                constexpr int i = I;
-                fo[(long long)i * p.N] = Codec<S>::enc(out[i], R(L::w(i)));
-            });
         }
-        // This warp is done reading stage s.  The last warp out refills it with group k + NS.
         __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
+        if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
     }
 }
 

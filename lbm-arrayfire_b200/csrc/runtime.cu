@@ -7,6 +7,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "internal.h"
@@ -124,6 +125,7 @@ struct lbm_ctx {
     int kernel = LBM_KERNEL_AUTO;  // requested family
     int kernel_used = 0;           // family chosen (PLAIN or ROWS); 0 before the first step
     int rows_grid = 0;             // persistent grid of the row pipeline
+    int rows_rpg = 1;              // its rows per group
     int* err = nullptr;            // device error word of the row pipeline
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int gsteps = 0;
@@ -189,65 +191,84 @@ StepParams<double>& params_of<double>(lbm_ctx* c) {
 }
 
 // ---- row pipeline (rowpipe.cuh) ------------------------------------------------------------
+// D3Q27 BGK/MRT or D2Q9 BGK, deviation arithmetic, F32/F16S/BF16S, 32 <= nx <= 1024 and nx a
+// multiple of 16: every bulk copy (population rows of nx * s bytes, mask rows of nx bytes) must start
+// on a 16-byte boundary and move a multiple of 16 bytes.
 static bool rows_eligible(const lbm_ctx* c) {
     const lbm_desc& d = c->d;
-    return d.lattice == LBM_D3Q27 && (d.collision == LBM_BGK || d.collision == LBM_MRT) &&
-           d.arithmetic == LBM_ARITH_DEVIATION && d.storage != LBM_F64 &&
-           (d.nx == 128 || d.nx == 256 || d.nx == 512);
+    const bool coll_ok = d.lattice == LBM_D3Q27 ? (d.collision == LBM_BGK || d.collision == LBM_MRT)
+                                               : d.collision == LBM_BGK;
+    return coll_ok && d.arithmetic == LBM_ARITH_DEVIATION && d.storage != LBM_F64 && d.nx >= 32 &&
+           d.nx <= 1024 && d.nx % 16 == 0;
 }
 
-template <class S, int PITCH, int COLL>
+template <class L, class S, int PITCH, int COLL>
 static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s) {
-    auto kern = k_step_rows<D3Q27, S, PITCH, COLL>;
-    constexpr size_t smem = rowpipe_smem_bytes<D3Q27, S, PITCH>();
-    constexpr int threads = RowPipeShape<S, PITCH>::CONSUMERS + 32;  // consumers + one producer warp
-    kern<<<c->rows_grid, threads, smem, s>>>(p, c->err);
+    using Sh = RowPipeShape<L, S, PITCH>;
+    auto kern = k_step_rows<L, S, PITCH, COLL>;
+    kern<<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err);  // + producer warp
 }
 
-template <class S, int PITCH, int COLL>
+template <class L, class S, int PITCH, int COLL>
 static int prepare_rows_t(lbm_ctx* c) {
-    auto kern = k_step_rows<D3Q27, S, PITCH, COLL>;
-    constexpr size_t smem = rowpipe_smem_bytes<D3Q27, S, PITCH>();
-    LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    using Sh = RowPipeShape<L, S, PITCH>;
+    auto kern = k_step_rows<L, S, PITCH, COLL>;
+    LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
     int per_sm = 0, sms = 0;
-    LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RowPipeShape<S, PITCH>::CONSUMERS + 32, smem));
+    LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
     LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->d.device));
     if (per_sm < 1) return set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
-    constexpr int B = RowPipeShape<S, PITCH>::B;
-    const long long groups = (c->d.ny + B - 1) / B * c->d.nz;
+    c->rows_rpg = Sh::rows_per_group((int)c->d.nx);
+    const long long groups = (c->d.ny + c->rows_rpg - 1) / c->rows_rpg * c->d.nz;
     c->rows_grid = (int)std::min<long long>(groups, (long long)per_sm * sms);
     return LBM_OK;
 }
 
+// f(lattice tag, storage tag, collision constant, pitch constant)
 template <class F>
 static void dispatch_rows(const lbm_ctx* c, F&& f) {
     const int coll = c->d.collision == LBM_BGK ? 0 : (c->d.mrt_basis == LBM_MRT_REF ? 1 : 2);
-    auto by_pitch = [&](auto st, auto co) {
-        switch (c->d.nx) {
-            case 128: f(st, co, std::integral_constant<int, 128>{}); break;
-            case 256: f(st, co, std::integral_constant<int, 256>{}); break;
-            default: f(st, co, std::integral_constant<int, 512>{}); break;
+    auto by_pitch = [&](auto lt, auto st, auto co) {
+        const long long nx = c->d.nx;
+        if (nx <= 128)
+            f(lt, st, co, std::integral_constant<int, 128>{});
+        else if (nx <= 256)
+            f(lt, st, co, std::integral_constant<int, 256>{});
+        else if (nx <= 512)
+            f(lt, st, co, std::integral_constant<int, 512>{});
+        else
+            f(lt, st, co, std::integral_constant<int, 1024>{});
+    };
+    auto by_coll = [&](auto lt, auto st) {
+        if constexpr (std::is_same_v<typename decltype(lt)::type, D2Q9>) {
+            by_pitch(lt, st, std::integral_constant<int, 0>{});
+        } else {
+            switch (coll) {
+                case 0: by_pitch(lt, st, std::integral_constant<int, 0>{}); break;
+                case 1: by_pitch(lt, st, std::integral_constant<int, 1>{}); break;
+                default: by_pitch(lt, st, std::integral_constant<int, 2>{}); break;
+            }
         }
     };
-    auto by_coll = [&](auto st) {
-        switch (coll) {
-            case 0: by_pitch(st, std::integral_constant<int, 0>{}); break;
-            case 1: by_pitch(st, std::integral_constant<int, 1>{}); break;
-            default: by_pitch(st, std::integral_constant<int, 2>{}); break;
+    auto by_storage = [&](auto lt) {
+        switch (c->d.storage) {
+            case LBM_F32: by_coll(lt, Tag<float>{}); break;
+            case LBM_F16S: by_coll(lt, Tag<__half>{}); break;
+            default: by_coll(lt, Tag<__nv_bfloat16>{}); break;
         }
     };
-    switch (c->d.storage) {
-        case LBM_F32: by_coll(Tag<float>{}); break;
-        case LBM_F16S: by_coll(Tag<__half>{}); break;
-        default: by_coll(Tag<__nv_bfloat16>{}); break;
-    }
+    if (c->d.lattice == LBM_D2Q9)
+        by_storage(Tag<D2Q9>{});
+    else
+        by_storage(Tag<D3Q27>{});
 }
 
 static int prepare_rows(lbm_ctx* c) {
     int rc = LBM_OK;
-    dispatch_rows(c, [&](auto st, auto co, auto pi) {
+    dispatch_rows(c, [&](auto lt, auto st, auto co, auto pi) {
+        using L = typename decltype(lt)::type;
         using S = typename decltype(st)::type;
-        rc = prepare_rows_t<S, decltype(pi)::value, decltype(co)::value>(c);
+        rc = prepare_rows_t<L, S, decltype(pi)::value, decltype(co)::value>(c);
     });
     return rc;
 }
@@ -255,13 +276,14 @@ static int prepare_rows(lbm_ctx* c) {
 // Launch one time step reading buffer `from` and writing the other one.
 static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
     if (c->kernel_used == LBM_KERNEL_ROWS) {
-        dispatch_rows(c, [&](auto st, auto co, auto pi) {
+        dispatch_rows(c, [&](auto lt, auto st, auto co, auto pi) {
+            using L = typename decltype(lt)::type;
             using S = typename decltype(st)::type;
             using R = typename Codec<S>::Real;
             StepParams<R> p = params_of<R>(c);
             p.fin = c->f[from];
             p.fout = c->f[from ^ 1];
-            launch_rows_t<S, decltype(pi)::value, decltype(co)::value>(c, p, s);
+            launch_rows_t<L, S, decltype(pi)::value, decltype(co)::value>(c, p, s);
         });
         return;
     }
@@ -849,7 +871,8 @@ int lbm_set_kernel(lbm_ctx* c, int kind) {
         return set_error(LBM_ERR_INVALID, "unknown kernel family");
     if (kind == LBM_KERNEL_ROWS && !rows_eligible(c))
         return set_error(LBM_ERR_UNSUPPORTED,
-                         "the row pipeline needs D3Q27 BGK/MRT, deviation arithmetic, F32/F16S/BF16S and nx in {128,256,512}");
+                         "the row pipeline needs D3Q27 BGK/MRT or D2Q9 BGK, deviation arithmetic, F32/F16S/BF16S "
+                         "and 32 <= nx <= 1024 with nx a multiple of 16");
     LBM_CK(cudaSetDevice(c->d.device));
     LBM_CK(cudaStreamSynchronize(c->stream));
     drop_graphs(c);

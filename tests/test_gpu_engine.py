@@ -261,15 +261,64 @@ def test_row_pipeline_ring_wraps_equal_plain_kernel(storage, coll):
     assert np.array_equal(out[lb.KERNEL_PLAIN], out[lb.KERNEL_ROWS])
 
 
+def _rows_vs_plain(d, m, F0, steps):
+    out = {}
+    for kind in (lb.KERNEL_PLAIN, lb.KERNEL_ROWS):
+        with lb.Lattice(d, m) as lat:
+            lat.set_kernel(kind)
+            if F0 is not None:
+                lat.set_populations(np.asarray(F0, dtype=np.float64))
+            lat.step(steps)
+            lat.sync()
+            assert lat.kernel() == kind
+            out[kind] = lat.get_populations(np.float32)
+    assert np.isfinite(out[lb.KERNEL_ROWS]).all()
+    return out[lb.KERNEL_PLAIN], out[lb.KERNEL_ROWS]
+
+
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.BF16S])
+@pytest.mark.parametrize("case", ["d2q9_lid_128", "d2q9_lid_64", "d2q9_channel_1024", "d3q27_duct_384",
+                                  "d3q27_duct_640", "d3q27_mrt_96"])
+def test_row_pipeline_other_widths_and_d2q9_equal_plain(storage, case):
+    """Widths below the shared-memory row pitch (idle threads), above 512 (two x per thread), D2Q9,
+    equilibrium inlets and zero-gradient outlets: bit-identical to the one-cell-per-thread kernel."""
+    if case == "d2q9_lid_128":
+        d, m, F0 = cavity2d(n=128, storage=storage)
+    elif case == "d2q9_lid_64":
+        d, m, F0 = cavity2d(n=64, re=400.0, storage=storage)
+    elif case == "d2q9_channel_1024":
+        d, m, F0 = channel2d(1024, 64, 0.04, 100.0, 200, 32, 10, storage=storage, config_mode=True, seed=1,
+                             noise=1e-4)
+    elif case in ("d3q27_duct_384", "d3q27_duct_640"):
+        nx = int(case.split("_")[-1])
+        d = lb.make_desc(lb.D3Q27, lb.BGK, storage, (nx, 14, 10), omega=1.7)
+        m = lb.setup_duct3d(d, 0.04, nx / 3, 7, 5, 3)
+        F0 = None
+    else:
+        d = lb.make_desc(lb.D3Q27, lb.MRT, storage, (96, 20, 9), mrt_s=lb.mrt_rates(1.8, 1.2),
+                         mrt_basis=lb.MRT_GRAM_SCHMIDT)
+        m = lb.setup_cavity3d(d, 0.05)
+        F0 = None
+    a, b = _rows_vs_plain(d, m, F0, 30)
+    assert np.array_equal(a, b)
+
+
 def test_row_pipeline_needs_eligible_shape():
-    d, m, F0 = cavity2d(n=64)
-    with lb.Lattice(d, m) as lat:
-        with pytest.raises(lb.LbmError) as e:
-            lat.set_kernel(lb.KERNEL_ROWS)
-        assert e.value.code == -5
-    d, m, F0 = cavity3d(n=(100, 8, 8))
-    with lb.Lattice(d, m) as lat:
-        with pytest.raises(lb.LbmError):
-            lat.set_kernel(lb.KERNEL_ROWS)
-        lat.step(3)
-        assert lat.kernel() == lb.KERNEL_PLAIN
+    rejected = [
+        lb.make_desc(lb.D2Q9, lb.SHANCHEN, lb.F32, (128, 128), omega=1.0, sc_G=-5.0),  # two-pass model
+        lb.make_desc(lb.D3Q27, lb.BGK, lb.F32, (100, 8, 8), omega=1.3),  # 100-byte mask rows
+        lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (2048, 8), omega=1.3),  # wider than 1024
+        lb.make_desc(lb.D3Q27, lb.BGK, lb.F64, (128, 8, 8), omega=1.3),  # FP64 storage
+        lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (128, 8), omega=1.3, arithmetic=lb.ARITH_ABSOLUTE),
+    ]
+    for d in rejected:
+        with lb.Lattice(d, None) as lat:
+            with pytest.raises(lb.LbmError) as e:
+                lat.set_kernel(lb.KERNEL_ROWS)
+            assert e.value.code == -5
+            lat.step(3)
+            assert lat.kernel() == lb.KERNEL_PLAIN
+    # nx = 112 (a multiple of 16 below the 128-cell row pitch): eligible, and equal to the plain kernel
+    d, m, F0 = cavity3d(n=(112, 8, 8), storage=lb.F16S)
+    a, b = _rows_vs_plain(d, m, F0, 7)
+    assert np.array_equal(a, b)
