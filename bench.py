@@ -512,6 +512,7 @@ def run_ensemble(args, rank, world, local_rank):
     barrier(torch, world)
     el_max = reduce_max(torch, el, dev, world)
     tile = batch.tile_info()
+    mode = {lb.BATCH_TILES: "tiles", lb.BATCH_ROWS: "rows+tiles"}.get(batch.mode(), "auto")
     families = len({d.lattice for d, _, _ in mine})
     batch.close()
     del batch
@@ -527,6 +528,18 @@ def run_ensemble(args, rank, world, local_rank):
                 seq += events_time(lat.stream(), lambda: lat.step(args.steps))
         seq = reduce_max(torch, seq, dev, world)
 
+    # the same ensemble in FP32 storage, batched the same way
+    el32 = 0.0
+    if not args.no_compare and storage != lb.F32:
+        mem32 = ensemble_members(lb, lb.F32)
+        mine32 = [mem32[k] for k in parts[rank]]
+        b32 = lb.Batch([d for d, _, _ in mine32], [m for _, m, _ in mine32])
+        b32.step(max(args.warmup, 1))
+        b32.sync()
+        el32 = reduce_max(torch, events_time(b32.stream(), lambda: b32.step(args.steps)), dev, world)
+        b32.close()
+        del b32
+
     value = total_cells * args.steps / el_max / 1e6
     achieved = total_bytes * args.steps / el_max / 1e9
     out = {
@@ -538,15 +551,21 @@ def run_ensemble(args, rank, world, local_rank):
                    "l2": f"inputs larger than L2: {total_bytes / 2 / 1e9:.2f} GB of populations per buffer set",
                    "parallelism": f"LPT shards x{world}" if world > 1 else "single GPU",
                    "members_per_rank": [len(p) for p in parts], "cells_this_rank": my_cells,
-                   "tile_width": tile[0], "tiles": tile[1]},
+                   "batch_mode": mode, "tile_width": tile[0], "tiles": tile[1]},
         "roofline": {"bound": "hbm", "achieved": achieved / world, "peak": peak, "unit": "GB/s",
                      "frac": achieved / world / peak, "traffic": None,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                     else "fallback 6.65 TB/s", "kernel": "k_batch_bgk<D2Q9> + k_batch_bgk<D3Q27>",
+                     else "fallback 6.65 TB/s",
+                     "kernel": "k_batch_rows<D2Q9/D3Q27> (+ k_batch_bgk tiles)" if mode == "rows+tiles"
+                     else "k_batch_bgk<D2Q9> + k_batch_bgk<D3Q27>",
                      "note": "achieved per GPU: algorithmic bytes of all members / max-over-ranks time / ranks"},
         "gpu_launches": args.steps * families,
         "clocks": clocks,
     }
+    if el32 > 0:
+        out["fp32_batched"] = {"value": total_cells * args.steps / el32 / 1e6, "unit": "MLUPS",
+                               "ms_per_step": el32 * 1e3 / args.steps}
+        out[f"speedup_{STORAGE_NAMES[storage]}_vs_f32"] = el32 / el_max
     if seq > 0:
         out["sequential_plain"] = {"value": total_cells * args.steps / seq / 1e6, "unit": "MLUPS",
                                    "seconds": seq, "note": "each member alone through lbm_step, summed"}

@@ -197,8 +197,10 @@ int  lbm_sums_fp64_noalloc(const void* populations, int lattice, int storage, in
 
 /* ---- batched ensemble -------------------------------------------------------------------
  * Many independent lattices (any mix of D2Q9/D3Q27 BGK, sizes and rates, one storage type)
- * advanced by one kernel launch per step over a tile table; nsteps of those are captured in a
- * CUDA graph and replayed.                                                                      */
+ * advanced by one persistent kernel launch per lattice family and step over a work table (row
+ * groups staged by bulk copies for members with nx a multiple of 16 up to 1024, one-thread-per-cell
+ * tiles for the others); nsteps of those are captured in a CUDA graph and replayed.  Every member
+ * gives the same populations as stepping it alone.                                               */
 int  lbm_batch_create(const lbm_desc* descs, int n, lbm_batch** out);
 void lbm_batch_destroy(lbm_batch* b);
 int  lbm_batch_size(const lbm_batch* b);
@@ -212,6 +214,12 @@ int64_t lbm_batch_cells(const lbm_batch* b);
 void* lbm_batch_stream(lbm_batch* b);
 /* Tile shape chosen by the autotuner (cells per tile along x, tiles launched per step). */
 int  lbm_batch_tile_info(const lbm_batch* b, int* tile_x, int64_t* n_tiles);
+/* Work distribution: AUTO (default) times both on the first step; TILES steps every member with
+ * the one-thread-per-cell tile kernel; ROWS uses the row pipeline for every eligible member.
+ * lbm_batch_get_mode reports the choice in use (AUTO before the first step).                     */
+enum lbm_batch_mode { LBM_BATCH_AUTO = 0, LBM_BATCH_TILES = 1, LBM_BATCH_ROWS = 2 };
+int  lbm_batch_set_mode(lbm_batch* b, int mode);
+int  lbm_batch_get_mode(const lbm_batch* b);
 
 /* ---- problem set-up helpers (the reference's loop-invariant state, layer L3) --------------
  * Each fills mask[N] (column-major) and the descriptor's class table so that the per-cell

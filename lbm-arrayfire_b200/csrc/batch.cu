@@ -1,8 +1,14 @@
 // batch.cu — an ensemble of independent BGK lattices (any mix of D2Q9 and D3Q27 extents and
-// rates, one storage type) advanced together.  Each step is one kernel per lattice family over a
-// tile table: a tile is one row segment (lattice, y, z, x0) of `tile_x` cells, so lattices of very
-// different sizes share the SMs without per-lattice launches.  Chunks of steps are captured in a
-// CUDA graph and replayed.  The tile width is picked by timing candidates on the real buffers.
+// rates, one storage type) advanced together.  Each step is one persistent kernel per lattice family
+// over a work table, so lattices of very different sizes share the SMs without per-lattice launches:
+//   - row pipeline (k_batch_rows): items are (lattice, first row, z, rows) groups staged in shared
+//     memory by bulk copies, for members whose rows the copies can move (nx a multiple of 16, at most
+//     1024); the shared-memory row pitch is the family's widest such row, narrower members put more
+//     rows into a stage and every consumer thread takes cells of the flattened group;
+//   - tile kernel (k_batch_bgk): a tile is one row segment (lattice, y, z, x0) of `tile_x` cells, one
+//     thread per cell, for the other members (or all of them, if the autotuner finds that faster).
+// Chunks of steps are captured in a CUDA graph and replayed.  The autotuner times the tile widths and
+// the row pipeline on the real buffers.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -11,6 +17,7 @@
 
 #include "internal.h"
 #include "kernels.cuh"
+#include "rowpipe.cuh"
 
 namespace lbm {
 
@@ -39,6 +46,112 @@ __global__ void __launch_bounds__(256) k_batch_bgk(const BatchLattice<typename C
     const int x = t.x0 + threadIdx.x;
     if (x >= p.nx) return;
     bgk_cell<L, S, false>(p, static_cast<const S*>(p.f[parity]), static_cast<S*>(p.f[parity ^ 1]), x, t.y, t.z);
+}
+
+// One row group of one member: rows y0 .. y0 + nb - 1 at z.
+struct RowItem {
+    int lat, y0, z, nb;
+};
+
+// The row pipeline of rowpipe.cuh over a work table of row groups of several lattices (BGK).
+template <class L, class S, int PITCH>
+__global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, RowPipeShape<L, S, PITCH>::CTAS)
+    k_batch_rows(const BatchLattice<typename Codec<S>::Real>* __restrict__ lats, const RowItem* __restrict__ items,
+                 long long n_items, int parity, int* __restrict__ err) {
+    using R = typename Codec<S>::Real;
+    using Sh = RowPipeShape<L, S, PITCH>;
+    constexpr int Q = L::Q;
+    constexpr int NS = Sh::NS;
+    constexpr int SB = Sh::SB;
+    constexpr int CONS = Sh::CONSUMERS;
+    constexpr int W = CONS / 32;
+    static_assert(NS <= 8, "barriers occupy the first 128 bytes");
+    constexpr unsigned long long kCy = pack_c<L>(false), kCz = pack_c<L>(true);
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* empty = full + NS;
+    S* in = reinterpret_cast<S*>(smem + 128);                                 // [NS][Q][SB]
+    uint8_t* mask_st = reinterpret_cast<uint8_t*>(in + (size_t)NS * Q * SB);  // [NS][SB]
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const long long first = blockIdx.x, stride = gridDim.x;
+
+    auto issue = [&](long long g, int s) {
+        const RowItem it = items[g];
+        const BatchLattice<R>& m = lats[it.lat];
+        const int nx = m.nx, ny = m.ny, nz = m.nz, nb = it.nb;
+        const uint32_t row_bytes = (uint32_t)(nx * sizeof(S));
+        if (lane == 0)
+            mbar_arrive_expect_tx(&full[s], (uint32_t)(Q * nb) * row_bytes + (m.mask ? (uint32_t)(nb * nx) : 0u));
+        __syncwarp();
+        if (lane < Q) {
+            const int cy = (int)((kCy >> (2 * lane)) & 3) - 1, cz = (int)((kCz >> (2 * lane)) & 3) - 1;
+            int zs = it.z - cz;
+            zs = zs < 0 ? zs + nz : (zs >= nz ? zs - nz : zs);
+            int ys = it.y0 - cy;
+            ys = ys < 0 ? ys + ny : (ys >= ny ? ys - ny : ys);
+            const int run = ny - ys < nb ? ny - ys : nb;
+            const S* plane = static_cast<const S*>(m.f[parity]) + (long long)lane * m.N + (long long)zs * ny * nx;
+            S* dst = in + ((long long)s * Q + lane) * SB;
+            bulk_load(dst, plane + (long long)ys * nx, (uint32_t)run * row_bytes, &full[s]);
+            if (run < nb) bulk_load(dst + run * nx, plane, (uint32_t)(nb - run) * row_bytes, &full[s]);
+        } else if (lane == Q && m.mask) {
+            bulk_load(mask_st + s * SB, m.mask + ((long long)it.z * ny + it.y0) * nx, (uint32_t)(nb * nx), &full[s]);
+        }
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], W);
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid >= CONS) {  // producer warp
+        for (int s = 0; s < NS; ++s)
+            if (first + s * stride < n_items) issue(first + s * stride, s);
+        for (long long k = 0; first + (k + NS) * stride < n_items; ++k) {
+            const int s = (int)(k % NS);
+            if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1))) {
+                if (lane == 0) atomicExch(err, kRowPipeTimeout);
+                return;
+            }
+            issue(first + (k + NS) * stride, s);
+        }
+        return;
+    }
+    for (long long k = 0; first + k * stride < n_items; ++k) {
+        const long long g = first + k * stride;
+        const int s = (int)(k % NS);
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1))) {
+            if (lane == 0) atomicExch(err, kRowPipeTimeout);
+            for (int j = 1; j < NS && first + (k + j) * stride < n_items; ++j)
+                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1), 1LL << 28)) break;
+            return;
+        }
+        const RowItem it = items[g];
+        const BatchLattice<R>& m = lats[it.lat];
+        const int nx = m.nx;
+        R sc, isc;
+        storage_scale<S>(m, sc, isc);
+        const S* st = in + (long long)s * Q * SB;
+        const uint8_t* ms = m.mask ? mask_st + s * SB : nullptr;
+        S* out0 = static_cast<S*>(m.f[parity ^ 1]) + ((long long)it.z * m.ny + it.y0) * nx;
+        // cells of the group, flattened (row b, column x), CONS apart
+        int b = tid / nx, x = tid - b * nx;
+#pragma unroll 1
+        for (int c = tid; c < it.nb * nx; c += CONS) {
+            row_cell<L, S, SB, 0>(m, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc, out0 + (long long)b * nx);
+            x += CONS;
+            while (x >= nx) {
+                x -= nx;
+                ++b;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
 }
 
 template <class T>
@@ -73,6 +186,13 @@ struct lbm_batch {
     int gsteps = 0;
     long long cells = 0;
     double bytes_per_step = 0;
+    int mode = 0;                    // LBM_BATCH_AUTO / TILES / ROWS
+    bool use_rows = false;           // row pipeline for the eligible members
+    int rows_pitch[2] = {0, 0};      // shared-memory row pitch per family
+    RowItem* items_d[2] = {nullptr, nullptr};
+    long long n_items[2] = {0, 0};
+    int rows_grid[2] = {0, 0};
+    int* err = nullptr;              // device error word of the row pipeline
 };
 
 namespace lbm {
@@ -86,11 +206,97 @@ static void batch_drop_graphs(lbm_batch* b) {
     b->gsteps = 0;
 }
 
+// Row pipeline eligibility of one member: bulk copies move whole rows (nx a multiple of 16, <= 1024).
+static bool batch_row_member(const lbm_batch* b, int k) {
+    const lbm_desc& d = b->descs[k];
+    return b->storage != LBM_F64 && d.nx >= 32 && d.nx <= 1024 && d.nx % 16 == 0;
+}
+
+static int pitch_for(long long nx) { return nx <= 128 ? 128 : nx <= 256 ? 256 : nx <= 512 ? 512 : 1024; }
+
+// f(lattice tag, storage tag, pitch constant) for family fam (0 = D2Q9, 1 = D3Q27)
+template <class F>
+static void batch_rows_dispatch(const lbm_batch* b, int fam, F&& f) {
+    auto by_pitch = [&](auto lt, auto st) {
+        switch (b->rows_pitch[fam]) {
+            case 128: f(lt, st, std::integral_constant<int, 128>{}); break;
+            case 256: f(lt, st, std::integral_constant<int, 256>{}); break;
+            case 512: f(lt, st, std::integral_constant<int, 512>{}); break;
+            default: f(lt, st, std::integral_constant<int, 1024>{}); break;
+        }
+    };
+    auto by_storage = [&](auto lt) {
+        switch (b->storage) {
+            case LBM_F32: by_pitch(lt, BTag<float>{}); break;
+            case LBM_F16S: by_pitch(lt, BTag<__half>{}); break;
+            default: by_pitch(lt, BTag<__nv_bfloat16>{}); break;
+        }
+    };
+    if (fam == 0)
+        by_storage(BTag<D2Q9>{});
+    else
+        by_storage(BTag<D3Q27>{});
+}
+
+// Work tables of the row pipeline: per family, the row groups of its eligible members.
+static int batch_build_rows(lbm_batch* b) {
+    int sms = 0;
+    LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    for (int fam = 0; fam < 2; ++fam) {
+        long long maxnx = 0;
+        for (int k = 0; k < (int)b->descs.size(); ++k)
+            if ((b->descs[k].lattice == LBM_D2Q9) == (fam == 0) && batch_row_member(b, k))
+                maxnx = std::max<long long>(maxnx, b->descs[k].nx);
+        if (!maxnx) continue;
+        b->rows_pitch[fam] = pitch_for(maxnx);
+        std::vector<RowItem> items;
+        int rc = LBM_OK;
+        batch_rows_dispatch(b, fam, [&](auto lt, auto st, auto pi) {
+            using L = typename decltype(lt)::type;
+            using S = typename decltype(st)::type;
+            constexpr int PITCH = decltype(pi)::value;
+            using Sh = RowPipeShape<L, S, PITCH>;
+            for (int k = 0; k < (int)b->descs.size(); ++k) {
+                const lbm_desc& d = b->descs[k];
+                if ((d.lattice == LBM_D2Q9) != (fam == 0) || !batch_row_member(b, k)) continue;
+                const int rpg = Sh::rows_per_group((int)d.nx);
+                for (int z = 0; z < (int)d.nz; ++z)
+                    for (int y0 = 0; y0 < (int)d.ny; y0 += rpg)
+                        items.push_back(RowItem{k, y0, z, (int)std::min<long long>(rpg, d.ny - y0)});
+            }
+            auto kern = k_batch_rows<L, S, PITCH>;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()) !=
+                cudaSuccess) {
+                rc = set_error(LBM_ERR_CUDA, "row pipeline shared-memory attribute");
+                return;
+            }
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()) !=
+                    cudaSuccess || per_sm < 1) {
+                rc = set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
+                return;
+            }
+            b->rows_grid[fam] = (int)std::min<long long>((long long)items.size(), (long long)per_sm * sms);
+        });
+        if (rc) return rc;
+        if (b->items_d[fam]) cudaFree(b->items_d[fam]);
+        b->items_d[fam] = nullptr;
+        b->n_items[fam] = (long long)items.size();
+        if (cudaMalloc(&b->items_d[fam], sizeof(RowItem) * items.size()) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(LBM_ERR_NOMEM, "row work table allocation failed");
+        }
+        LBM_CK(cudaMemcpy(b->items_d[fam], items.data(), sizeof(RowItem) * items.size(), cudaMemcpyHostToDevice));
+    }
+    return LBM_OK;
+}
+
 static int batch_build_tiles(lbm_batch* b, int tile_x) {
     std::vector<Tile> t[2];
     for (int k = 0; k < (int)b->descs.size(); ++k) {
         const lbm_desc& d = b->descs[k];
         const int fam = d.lattice == LBM_D2Q9 ? 0 : 1;
+        if (b->use_rows && batch_row_member(b, k)) continue;  // stepped by the row pipeline
         for (int z = 0; z < (int)d.nz; ++z)
             for (int y = 0; y < (int)d.ny; ++y)
                 for (int x0 = 0; x0 < (int)d.nx; x0 += tile_x) t[fam].push_back(Tile{k, y, z, x0});
@@ -121,6 +327,18 @@ static void batch_launch(lbm_batch* b, int parity, cudaStream_t s) {
         if (b->n_tiles[1])
             k_batch_bgk<D3Q27, S><<<(unsigned)b->n_tiles[1], b->tile_x, 0, s>>>(lats, b->tiles_d[1], parity);
     });
+    if (!b->use_rows) return;
+    for (int fam = 0; fam < 2; ++fam) {
+        if (!b->n_items[fam]) continue;
+        batch_rows_dispatch(b, fam, [&](auto lt, auto st, auto pi) {
+            using L = typename decltype(lt)::type;
+            using S = typename decltype(st)::type;
+            using R = typename Codec<S>::Real;
+            using Sh = RowPipeShape<L, S, decltype(pi)::value>;
+            k_batch_rows<L, S, decltype(pi)::value><<<b->rows_grid[fam], Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(
+                static_cast<const BatchLattice<R>*>(b->lats_d), b->items_d[fam], b->n_items[fam], parity, b->err);
+        });
+    }
 }
 
 static int batch_build_graphs(lbm_batch* b) {
@@ -141,31 +359,56 @@ static int batch_build_graphs(lbm_batch* b) {
     return LBM_OK;
 }
 
-// Tile width: time one step for each candidate (reads the current buffers, writes the others).
+// Configuration: time one step of each candidate (reads the current buffers, writes the others):
+// the tile kernel alone at tile widths 64/128/256, then the row pipeline for the eligible members
+// with the best tile width for the rest.  LBM_BATCH_* modes in lbm_batch_set_mode pin a choice.
 static int batch_autotune(lbm_batch* b) {
     cudaEvent_t e0, e1;
     LBM_CK(cudaEventCreate(&e0));
     LBM_CK(cudaEventCreate(&e1));
-    float best = 1e30f;
-    int best_tx = 128;
-    for (int tx : {64, 128, 256}) {
-        int rc = batch_build_tiles(b, tx);
-        if (rc) return rc;
+    auto time_step = [&](float& ms) -> int {
         batch_launch(b, b->parity, b->stream);
         LBM_CK(cudaEventRecord(e0, b->stream));
         for (int r = 0; r < 2; ++r) batch_launch(b, b->parity, b->stream);
         LBM_CK(cudaEventRecord(e1, b->stream));
         LBM_CK(cudaEventSynchronize(e1));
-        float ms = 0;
         LBM_CK(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) {
+        return LBM_OK;
+    };
+    bool any_rows = false;
+    for (int k = 0; k < (int)b->descs.size(); ++k) any_rows = any_rows || batch_row_member(b, k);
+    float best = 1e30f;
+    int best_tx = 128;
+    bool best_rows = false;
+    if (b->mode != LBM_BATCH_ROWS || !any_rows) {
+        b->use_rows = false;
+        for (int tx : {64, 128, 256}) {
+            int rc = batch_build_tiles(b, tx);
+            float ms = 0;
+            if (!rc) rc = time_step(ms);
+            if (rc) return rc;
+            if (ms < best) {
+                best = ms;
+                best_tx = tx;
+            }
+        }
+    }
+    if (any_rows && b->mode != LBM_BATCH_TILES) {
+        b->use_rows = true;
+        int rc = batch_build_rows(b);
+        if (!rc) rc = batch_build_tiles(b, best_tx);
+        float ms = 0;
+        if (!rc) rc = time_step(ms);
+        if (rc) return rc;
+        if (ms < best || b->mode == LBM_BATCH_ROWS) {
             best = ms;
-            best_tx = tx;
+            best_rows = true;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     LBM_CK(cudaGetLastError());
+    b->use_rows = best_rows;
     return batch_build_tiles(b, best_tx);
 }
 
@@ -178,6 +421,9 @@ static void batch_free(lbm_batch* b) {
     cudaFree(b->lats_d);
     cudaFree(b->tiles_d[0]);
     cudaFree(b->tiles_d[1]);
+    cudaFree(b->items_d[0]);
+    cudaFree(b->items_d[1]);
+    cudaFree(b->err);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -218,6 +464,11 @@ int lbm_batch_create(const lbm_desc* descs, int n, lbm_batch** out) {
     if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) {
         batch_free(b);
         return set_error(LBM_ERR_CUDA, "stream creation failed");
+    }
+    if (cudaMalloc(&b->err, sizeof(int)) != cudaSuccess || cudaMemset(b->err, 0, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        batch_free(b);
+        return set_error(LBM_ERR_NOMEM, "error word allocation failed");
     }
     int rc = LBM_OK;
     batch_dispatch(b->storage, [&](auto tag) {
@@ -315,7 +566,28 @@ int lbm_batch_sync(lbm_batch* b) {
     if (!b) return set_error(LBM_ERR_INVALID, "batch is NULL");
     LBM_CK(cudaSetDevice(b->device));
     LBM_CK(cudaStreamSynchronize(b->stream));
+    int e = 0;
+    LBM_CK(cudaMemcpy(&e, b->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return set_error(LBM_ERR_TIMEOUT, "a row-pipeline barrier wait ran out (the step did not complete)");
     return LBM_OK;
+}
+
+int lbm_batch_set_mode(lbm_batch* b, int mode) {
+    if (!b) return set_error(LBM_ERR_INVALID, "batch is NULL");
+    if (mode != LBM_BATCH_AUTO && mode != LBM_BATCH_TILES && mode != LBM_BATCH_ROWS)
+        return set_error(LBM_ERR_INVALID, "unknown batch mode");
+    LBM_CK(cudaSetDevice(b->device));
+    LBM_CK(cudaStreamSynchronize(b->stream));
+    b->mode = mode;
+    b->tile_x = 0;  // re-tune on the next step
+    batch_drop_graphs(b);
+    return LBM_OK;
+}
+
+int lbm_batch_get_mode(const lbm_batch* b) {
+    if (!b) return set_error(LBM_ERR_INVALID, "batch is NULL");
+    if (!b->tile_x) return LBM_BATCH_AUTO;
+    return b->use_rows ? LBM_BATCH_ROWS : LBM_BATCH_TILES;
 }
 
 int lbm_batch_get_populations(lbm_batch* b, int k, void* dst, int dtype, int memory) {

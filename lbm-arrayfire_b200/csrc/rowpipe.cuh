@@ -90,6 +90,9 @@ constexpr unsigned long long pack_c(bool z) {
 #ifndef LBM_ROWPIPE_NS
 #define LBM_ROWPIPE_NS 0  // stages; 0 = as many as the shared-memory budget holds
 #endif
+#ifndef LBM_ROWPIPE_THREADS
+#define LBM_ROWPIPE_THREADS 256  // consumer threads per row set at most
+#endif
 #ifndef LBM_ROWPIPE_CR
 #define LBM_ROWPIPE_CR 0  // consumer row sets per CTA; 0 = per lattice and storage type
 #endif
@@ -100,7 +103,8 @@ constexpr unsigned long long pack_c(bool z) {
 // row-buffer locality (F16S: 512 B 33 GLUPS, 1 KB 34-42, 2 KB 44, 4 KB 44.5).  FP32 reaches 0.97 of
 // the measured copy bandwidth with 2 KB copies, two consumer row sets and three stages in one CTA per
 // SM; 16-bit storage keeps one row set and two stages in each of two CTAs per SM.
-//   THREADS   consumer threads per row set (one x each; XPT = 2 x positions each for PITCH 1024)
+//   THREADS   consumer threads per row set (XPT = PITCH / THREADS x positions each): at most 256, so
+//             wide rows keep two CTAs (two independent stage rings) per SM where the stages fit
 //   CR        row sets: set r takes rows b = r, r + CR, ... of a group
 //   B         rows per group at nx == PITCH; the host may put more rows of a narrower lattice into
 //             the same stage (runtime rows per group, at most B * PITCH / nx)
@@ -110,7 +114,7 @@ struct RowPipeShape {
     static constexpr int Q = L::Q;
     static constexpr bool k16 = sizeof(S) == 2;
     static constexpr bool k3 = L::DIM == 3;
-    static constexpr int THREADS = PITCH > 512 ? 512 : PITCH;
+    static constexpr int THREADS = PITCH > LBM_ROWPIPE_THREADS ? LBM_ROWPIPE_THREADS : PITCH;
     static constexpr int XPT = PITCH / THREADS;
     static constexpr int kRowBytes = PITCH * (int)sizeof(S);
     static constexpr int kGroupBytes = LBM_ROWPIPE_GROUP_BYTES > 0 ? LBM_ROWPIPE_GROUP_BYTES : (k16 ? 2048 : 1024);
@@ -118,9 +122,13 @@ struct RowPipeShape {
     static constexpr int CR0 = CRQ * THREADS > 512 ? 512 / THREADS : CRQ;
     static constexpr int CR = CR0 < 1 ? 1 : CR0;
     static constexpr int CONSUMERS = CR * THREADS;
-    // CTAs per SM: D3Q27 collisions need ~90-120 registers per thread, D2Q9 far fewer
-    static constexpr int CTAS = k3 ? (CONSUMERS <= 256 ? 2 : 1) : (CONSUMERS <= 256 ? 3 : 2);
-    static constexpr int kLimit = (CTAS == 1 ? 224 : CTAS == 2 ? 112 : 74) * 1024;  // smem per CTA
+    // CTAs per SM: D3Q27 collisions need ~90-120 registers per thread, D2Q9 far fewer; fewer CTAs
+    // where two stages of one row would not fit into a CTA's share of shared memory
+    static constexpr int limit_of(int ctas) { return (ctas <= 1 ? 224 : ctas == 2 ? 112 : 74) * 1024; }
+    static constexpr bool fits(int ctas) { return 2 * (Q * kRowBytes + PITCH) + 128 <= limit_of(ctas); }
+    static constexpr int CTAS_R = k3 ? (CONSUMERS <= 256 ? 2 : 1) : (CONSUMERS <= 256 ? 3 : 2);
+    static constexpr int CTAS = fits(CTAS_R) ? CTAS_R : (CTAS_R > 2 && fits(2) ? 2 : 1);
+    static constexpr int kLimit = limit_of(CTAS);  // smem per CTA
     static constexpr int kBudget = (CTAS == 1 ? (k16 ? 216 : 166) : CTAS == 2 ? (k16 ? 110 : 83) : 72) * 1024;
     static constexpr int B0 = kGroupBytes / kRowBytes;
     static constexpr int B1 = B0 < CR ? CR : B0;

@@ -34,6 +34,7 @@ F32, F16S, BF16S, F64 = 0, 1, 2, 3
 MRT_REF, MRT_GRAM_SCHMIDT = 0, 1
 ARITH_DEVIATION, ARITH_ABSOLUTE = 0, 1
 KERNEL_AUTO, KERNEL_PLAIN, KERNEL_ROWS = 0, 1, 2
+BATCH_AUTO, BATCH_TILES, BATCH_ROWS = 0, 1, 2
 DTYPE_F32, DTYPE_F64 = 0, 1
 HOST, DEVICE = 0, 1
 BOUNCE, SET_RHO, SET_UX, SET_UY, SET_UZ, EQUILIBRIUM, ZEROGRAD_XP = 1, 2, 4, 8, 16, 32, 64
@@ -121,6 +122,8 @@ _SIGS = {
     "lbm_batch_set_populations": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int]),
     "lbm_batch_get_macros": (C.c_int, [_P, C.c_int, _P, _P, C.c_int, C.c_int]),
     "lbm_batch_sums_fp64": (C.c_int, [_P, C.c_int, _P]),
+    "lbm_batch_set_mode": (C.c_int, [_P, C.c_int]),
+    "lbm_batch_get_mode": (C.c_int, [_P]),
     "lbm_batch_cells": (C.c_int64, [_P]),
     "lbm_batch_stream": (_P, [_P]),
     "lbm_batch_tile_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
@@ -451,6 +454,13 @@ class Batch:
 
     def stream(self) -> int:
         return lib().lbm_batch_stream(self._h) or 0
+
+    def set_mode(self, mode: int):
+        """BATCH_AUTO (time both), BATCH_TILES (tile kernel only) or BATCH_ROWS (row pipeline)."""
+        _check(lib().lbm_batch_set_mode(self._h, mode))
+
+    def mode(self) -> int:
+        return lib().lbm_batch_get_mode(self._h)
 
     def tile_info(self):
         tx = C.c_int()

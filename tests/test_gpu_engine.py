@@ -162,24 +162,32 @@ def test_external_stream():
         assert np.array_equal(lat2.get_populations(np.float32), a)
 
 
+@pytest.mark.parametrize("mode", [lb.BATCH_TILES, lb.BATCH_ROWS])
 @pytest.mark.parametrize("storage", [lb.F32, lb.F16S])
-def test_batch_equals_individual_lattices(storage):
+def test_batch_equals_individual_lattices(storage, mode):
+    """Every member of a batch (tile kernel, or row pipeline for the members whose rows the bulk copies
+    can move and tiles for the rest, in the same step) equals the lattice stepped alone."""
     members = []
     for n in (48, 80):
         d, m, F0 = cavity2d(n=n, u_lid=0.1, re=300, storage=storage)
         members.append((d, m, F0))
-    d, m, F0 = cavity3d(n=(20, 14, 12), u_lid=0.05, omega=1.2, storage=storage)
+    d, m, F0 = cavity3d(n=(20, 14, 12), u_lid=0.05, omega=1.2, storage=storage)  # nx = 20: tiles
     members.append((d, m, F0))
-    dd = lb.make_desc(lb.D3Q27, lb.BGK, storage, (40, 16, 16), omega=1.6)
-    mm = lb.setup_duct3d(dd, 0.04, 11, 8, 8, 4)
-    solid = mm == 1
-    F0 = O.init_equilibrium(oracle_problem(dd, mm), rho=np.where(solid, 0.0, 1.0),
-                            u=np.concatenate([np.where(solid, 0.0, 0.04), np.zeros(2 * mm.size)]))
-    members.append((dd, mm, F0))
+    d, m, F0 = cavity3d(n=(32, 14, 12), u_lid=0.05, omega=1.2, storage=storage)
+    members.append((d, m, F0))
+    for nx in (40, 64):
+        dd = lb.make_desc(lb.D3Q27, lb.BGK, storage, (nx, 16, 16), omega=1.6)
+        mm = lb.setup_duct3d(dd, 0.04, 11, 8, 8, 4)
+        solid = mm == 1
+        F0 = O.init_equilibrium(oracle_problem(dd, mm), rho=np.where(solid, 0.0, 1.0),
+                                u=np.concatenate([np.where(solid, 0.0, 0.04), np.zeros(2 * mm.size)]))
+        members.append((dd, mm, F0))
     b = lb.Batch([x[0] for x in members], [x[1] for x in members])
+    b.set_mode(mode)
     for k, (_, _, F0) in enumerate(members):
         b.set_populations(k, np.asarray(F0, dtype=np.float64))
     b.step(37)
+    assert b.mode() == mode
     tx, nt = b.tile_info()
     assert tx in (64, 128, 256) and nt > 0
     for k, (d, m, F0) in enumerate(members):
@@ -190,6 +198,29 @@ def test_batch_equals_individual_lattices(storage):
             r1, u1 = b.macros(k)
             r2, u2 = lat.macros()
             assert np.array_equal(u1, u2)
+    b.close()
+
+
+@pytest.mark.parametrize("storage", [lb.F32, lb.BF16S])
+def test_batch_rows_many_groups_equal_individual(storage):
+    """Row-pipeline batch with ~10x more row groups than resident CTAs (every CTA cycles its stage ring
+    over groups of different members and widths): each member equals the lattice stepped alone."""
+    members = []
+    for nx, ny, nz in ((256, 40, 30), (128, 33, 17), (96, 20, 9)):
+        d = lb.make_desc(lb.D3Q27, lb.BGK, storage, (nx, ny, nz), omega=1.5)
+        members.append((d, lb.setup_cavity3d(d, 0.06)))
+    for n in (512, 64, 208):
+        d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (n, n), omega=1.7)
+        members.append((d, lb.setup_cavity2d(d, 0.1)))
+    b = lb.Batch([x[0] for x in members], [x[1] for x in members])
+    b.set_mode(lb.BATCH_ROWS)
+    b.step(9)
+    b.sync()
+    assert b.mode() == lb.BATCH_ROWS
+    for k, (d, m) in enumerate(members):
+        with lb.Lattice(d, m) as lat:
+            lat.step(9)
+            assert np.array_equal(b.get_populations(k, np.float32), lat.get_populations(np.float32)), k
     b.close()
 
 
