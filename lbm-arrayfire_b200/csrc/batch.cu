@@ -30,7 +30,7 @@ struct BatchLattice {
     long long N;
     R omega, one_m_omega;
     R scale, inv_scale;
-    ClassTable<R> cls;
+    alignas(16) ClassTable<R> cls;  // 16-byte aligned: the row pipeline bulk-copies it into shared memory
 };
 
 struct Tile {
@@ -48,10 +48,27 @@ __global__ void __launch_bounds__(256) k_batch_bgk(const BatchLattice<typename C
     bgk_cell<L, S, false>(p, static_cast<const S*>(p.f[parity]), static_cast<S*>(p.f[parity ^ 1]), x, t.y, t.z);
 }
 
+// A member's per-cell parameters for one row group: the scalars in registers (the stores of the group
+// could alias the member table as far as the compiler knows, so reading them through `lats` would
+// reload them after every cell) and the class table in the stage's shared memory.
+template <class R>
+struct MemberCell {
+    long long N;
+    R omega, one_m_omega;
+    const ClassTable<R>& cls;
+};
+
 // One row group of one member: rows y0 .. y0 + nb - 1 at z.
 struct RowItem {
     int lat, y0, z, nb;
 };
+
+// Shared memory of k_batch_rows: the row pipeline's stages plus one class table per stage.
+template <class L, class S, int PITCH>
+constexpr size_t batch_rows_smem() {
+    using Sh = RowPipeShape<L, S, PITCH>;
+    return Sh::smem_bytes() + (size_t)Sh::NS * sizeof(ClassTable<typename Codec<S>::Real>);
+}
 
 // The row pipeline of rowpipe.cuh over a work table of row groups of several lattices (BGK).
 template <class L, class S, int PITCH>
@@ -72,6 +89,9 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     uint64_t* empty = full + NS;
     S* in = reinterpret_cast<S*>(smem + 128);                                 // [NS][Q][SB]
     uint8_t* mask_st = reinterpret_cast<uint8_t*>(in + (size_t)NS * Q * SB);  // [NS][SB]
+    using CT = ClassTable<R>;
+    static_assert(sizeof(CT) % 16 == 0 && (Sh::smem_bytes() % 16) == 0, "class-table copies need 16-byte multiples");
+    CT* cls_st = reinterpret_cast<CT*>(smem + Sh::smem_bytes());              // [NS]
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const long long first = blockIdx.x, stride = gridDim.x;
@@ -82,7 +102,8 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         const int nx = m.nx, ny = m.ny, nz = m.nz, nb = it.nb;
         const uint32_t row_bytes = (uint32_t)(nx * sizeof(S));
         if (lane == 0)
-            mbar_arrive_expect_tx(&full[s], (uint32_t)(Q * nb) * row_bytes + (m.mask ? (uint32_t)(nb * nx) : 0u));
+            mbar_arrive_expect_tx(&full[s], (uint32_t)(Q * nb) * row_bytes + (m.mask ? (uint32_t)(nb * nx) : 0u) +
+                                                (uint32_t)sizeof(CT));
         __syncwarp();
         if (lane < Q) {
             const int cy = (int)((kCy >> (2 * lane)) & 3) - 1, cz = (int)((kCz >> (2 * lane)) & 3) - 1;
@@ -97,6 +118,8 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
             if (run < nb) bulk_load(dst + run * nx, plane, (uint32_t)(nb - run) * row_bytes, &full[s]);
         } else if (lane == Q && m.mask) {
             bulk_load(mask_st + s * SB, m.mask + ((long long)it.z * ny + it.y0) * nx, (uint32_t)(nb * nx), &full[s]);
+        } else if (lane == Q + 1) {
+            bulk_load(cls_st + s, &m.cls, (uint32_t)sizeof(CT), &full[s]);
         }
     };
 
@@ -135,6 +158,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         const int nx = m.nx;
         R sc, isc;
         storage_scale<S>(m, sc, isc);
+        const MemberCell<R> mc{m.N, m.omega, m.one_m_omega, cls_st[s]};
         const S* st = in + (long long)s * Q * SB;
         const uint8_t* ms = m.mask ? mask_st + s * SB : nullptr;
         S* out0 = static_cast<S*>(m.f[parity ^ 1]) + ((long long)it.z * m.ny + it.y0) * nx;
@@ -142,7 +166,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         int b = tid / nx, x = tid - b * nx;
 #pragma unroll 1
         for (int c = tid; c < it.nb * nx; c += CONS) {
-            row_cell<L, S, SB, 0>(m, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc, out0 + (long long)b * nx);
+            row_cell<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc, out0 + (long long)b * nx);
             x += CONS;
             while (x >= nx) {
                 x -= nx;
@@ -265,14 +289,14 @@ static int batch_build_rows(lbm_batch* b) {
                         items.push_back(RowItem{k, y0, z, (int)std::min<long long>(rpg, d.ny - y0)});
             }
             auto kern = k_batch_rows<L, S, PITCH>;
-            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()) !=
-                cudaSuccess) {
+            constexpr size_t smem = batch_rows_smem<L, S, PITCH>();
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
                 rc = set_error(LBM_ERR_CUDA, "row pipeline shared-memory attribute");
                 return;
             }
             int per_sm = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()) !=
-                    cudaSuccess || per_sm < 1) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, smem) != cudaSuccess ||
+                per_sm < 1) {
                 rc = set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
                 return;
             }
@@ -335,7 +359,8 @@ static void batch_launch(lbm_batch* b, int parity, cudaStream_t s) {
             using S = typename decltype(st)::type;
             using R = typename Codec<S>::Real;
             using Sh = RowPipeShape<L, S, decltype(pi)::value>;
-            k_batch_rows<L, S, decltype(pi)::value><<<b->rows_grid[fam], Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(
+            k_batch_rows<L, S, decltype(pi)::value><<<b->rows_grid[fam], Sh::CONSUMERS + 32,
+                                                      batch_rows_smem<L, S, decltype(pi)::value>(), s>>>(
                 static_cast<const BatchLattice<R>*>(b->lats_d), b->items_d[fam], b->n_items[fam], parity, b->err);
         });
     }
