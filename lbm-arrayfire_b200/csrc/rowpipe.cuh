@@ -101,8 +101,10 @@ constexpr unsigned long long pack_c(bool z) {
 // lattice's nx is at most PITCH).  Measured on B200 (D3Q27 MRT, 256^3): the size of each
 // per-direction bulk copy matters most — every copy is a separate DRAM stream, so small copies lose
 // row-buffer locality (F16S: 512 B 33 GLUPS, 1 KB 34-42, 2 KB 44, 4 KB 44.5).  FP32 reaches 0.97 of
-// the measured copy bandwidth with 2 KB copies, two consumer row sets and three stages in one CTA per
-// SM; 16-bit storage keeps one row set and two stages in each of two CTAs per SM.
+// the measured copy bandwidth with 2 KB copies (2 rows at 256 wide, 1 KB target), two consumer row
+// sets and three stages in one CTA per SM.  16-bit storage: 4 KB copies, two row sets, two stages,
+// one CTA per SM (A/B on one B200: 43.8 vs 42.6 GLUPS for MRT 256^3 and 42.0 vs 40.3 for the config-5
+// ensemble against 2 KB copies, one row set, two CTAs per SM).
 //   THREADS   consumer threads per row set (XPT = PITCH / THREADS x positions each): at most 256, so
 //             wide rows keep two CTAs (two independent stage rings) per SM where the stages fit
 //   CR        row sets: set r takes rows b = r, r + CR, ... of a group
@@ -117,8 +119,8 @@ struct RowPipeShape {
     static constexpr int THREADS = PITCH > LBM_ROWPIPE_THREADS ? LBM_ROWPIPE_THREADS : PITCH;
     static constexpr int XPT = PITCH / THREADS;
     static constexpr int kRowBytes = PITCH * (int)sizeof(S);
-    static constexpr int kGroupBytes = LBM_ROWPIPE_GROUP_BYTES > 0 ? LBM_ROWPIPE_GROUP_BYTES : (k16 ? 2048 : 1024);
-    static constexpr int CRQ = LBM_ROWPIPE_CR > 0 ? LBM_ROWPIPE_CR : (k3 && !k16 ? 2 : 1);
+    static constexpr int kGroupBytes = LBM_ROWPIPE_GROUP_BYTES > 0 ? LBM_ROWPIPE_GROUP_BYTES : (k16 ? 4096 : 1024);
+    static constexpr int CRQ = LBM_ROWPIPE_CR > 0 ? LBM_ROWPIPE_CR : 2;
     static constexpr int CR0 = CRQ * THREADS > 512 ? 512 / THREADS : CRQ;
     static constexpr int CR = CR0 < 1 ? 1 : CR0;
     static constexpr int CONSUMERS = CR * THREADS;
