@@ -131,23 +131,35 @@ __device__ __forceinline__ R momentum_sum(const R (&v)[L::Q]) {
 }
 
 template <class L, bool ABS, class R>
-__device__ __forceinline__ void moments(const R (&v)[L::Q], R isc, R& rho, R& drho, R& ux, R& uy, R& uz) {
+__device__ __forceinline__ void moments(const R (&v)[L::Q], R sc, R isc, R& rho, R& drho, R& ux, R& uy, R& uz) {
     R r = v[0];
     static_for<L::Q - 1>([&](auto I) { r = r + v[I + 1]; });
     R jx = momentum_sum<L, 0>(v), jy = momentum_sum<L, 1>(v), jz = momentum_sum<L, 2>(v);
     if constexpr (ABS) {
+        // the reference's arithmetic: u = j / rho
         rho = r;
         drho = r - R(1);
+        ux = jx / rho;
+        uy = jy / rho;
+        uz = L::DIM == 3 ? jz / rho : R(0);
     } else {
+        // One division whose numerator is the (power-of-two) storage scale, then a product and one
+        // correction step per component (Markstein: q = j/rho, e = j - q rho exactly by fma, q + e/rho),
+        // which returns the correctly rounded quotient in all but rare cases.  A plain j / rho per
+        // component took the division's slow path for every zero or tiny momentum (cells at rest).
         drho = r * isc;
         rho = R(1) + drho;
-        jx = jx * isc;
-        jy = jy * isc;
-        jz = jz * isc;
+        const R inv = isc / rho;  // (1 / rho) / scale
+        const R rinv = inv * sc;  // 1 / rho: exact rescale by a power of two
+        auto quot = [&](R j) {
+            const R q = j * inv;
+            const R e = mad(-q, rho, j * isc);
+            return mad(e, rinv, q);
+        };
+        ux = quot(jx);
+        uy = quot(jy);
+        uz = L::DIM == 3 ? quot(jz) : R(0);
     }
-    ux = jx / rho;
-    uy = jy / rho;
-    uz = L::DIM == 3 ? jz / rho : R(0);
 }
 
 // The reference's boundary overwrites of DENSITY/UX/UY/UZ (cpp/d2q9_bgk_lid.cpp:141-146).
@@ -274,7 +286,7 @@ template <class L, bool ABS, class P, class R>
 __device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, const R (&v)[L::Q], R sc, R isc,
                                             R (&out)[L::Q]) {
     R rho, drho, ux, uy, uz;
-    moments<L, ABS>(v, isc, rho, drho, ux, uy, uz);
+    moments<L, ABS>(v, sc, isc, rho, drho, ux, uy, uz);
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
     R fe[L::Q];
     equilibrium_v<L, ABS>(rho, drho, ux, uy, uz, sc, fe);
@@ -488,7 +500,7 @@ __global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepPar
     R sc, isc;
     storage_scale<S>(p, sc, isc);
     R rho, drho, ux, uy, uz;
-    moments<L, ABS>(v, isc, rho, drho, ux, uy, uz);
+    moments<L, ABS>(v, sc, isc, rho, drho, ux, uy, uz);
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 2);
     R Fx, Fy;
     sc_force(p, rows, x, c, Fx, Fy);
@@ -544,7 +556,7 @@ __global__ void k_macros(const __grid_constant__ StepParams<typename Codec<S>::R
     R sc, isc;
     storage_scale<S>(p, sc, isc);
     R rho, drho, ux, uy, uz;
-    moments<L, false>(d, isc, rho, drho, ux, uy, uz);
+    moments<L, false>(d, sc, isc, rho, drho, ux, uy, uz);
     if (pulled && fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
     if constexpr (L::DIM == 2) {
         if (pulled && collision == 2) {
