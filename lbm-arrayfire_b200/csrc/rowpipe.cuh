@@ -1,4 +1,5 @@
-// rowpipe.cuh — D3Q27 step kernel with bulk-copy (TMA) staging of lattice rows.
+// rowpipe.cuh — the D3Q27 (BGK, MRT) and D2Q9 (BGK) step kernel with bulk-copy (TMA) staging of
+// lattice rows.
 //
 // A CTA owns a group of up to B consecutive lattice rows (y0..y0+nb-1, z) at a time — one thread per
 // x, each handling the nb cells of its column — and walks a strided list of row groups.  For each
@@ -12,10 +13,13 @@
 // the staged populations with immediate-offset shared loads, collide, store their cells straight to
 // global memory (coalesced along x) and release the stage on empty[s]; the producer refills a stage as
 // soon as empty[s] completes.  Measured on B200 (MRT, 256^3), against the alternatives:
-//   - staging the outputs for bulk stores too: 25 vs 29 GLUPS (FP32) — the copy engine's request
-//     rate, not the bytes, was the limit; for the same reason a group spans 1-2 KB per direction;
+//   - staging the outputs for bulk stores too: 25 vs 29 GLUPS (FP32) — twice the copies, each small;
+//     every copy is a separate DRAM stream, so a group spans 1-4 KB per direction (RowPipeShape);
 //   - no producer warp, the last consumer warp out of a stage refilling it: 40 vs 44 GLUPS (F16S),
-//     25 vs 28 GLUPS (FP32) — the refill then waits for the slowest warp of the CTA.
+//     25 vs 28 GLUPS (FP32) — the refill then waits for the slowest warp of the CTA;
+//   - outputs through a per-warp shared-memory transpose and 16-byte stores along the planes (fewer
+//     store and address instructions, smaller groups to make room): 43.0 vs 43.7 GLUPS (F16S MRT),
+//     46.6 vs 48.1 (F16S BGK).
 // Compared with the one-cell-per-thread kernel this removes the per-population 64-bit load-address
 // arithmetic and decouples memory latency from occupancy.
 //
