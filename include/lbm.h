@@ -168,8 +168,8 @@ int   lbm_get_desc(const lbm_ctx* c, lbm_desc* out);
 int   lbm_set_block(lbm_ctx* c, int threads_x);
 int   lbm_get_block(const lbm_ctx* c);
 /* Step-kernel family.  PLAIN: one thread per cell, populations read straight from HBM.  ROWS
- * (D3Q27 BGK/MRT or D2Q9 BGK, deviation arithmetic, F32/F16S/BF16S, 32 <= nx <= 1024, nx a multiple
- * of 16): groups of whole rows staged in shared memory by bulk
+ * (D3Q27 BGK/MRT or D2Q9 BGK, deviation arithmetic, F32/F16S/BF16S, nx >= 32 a multiple of 16):
+ * groups of whole rows (segments of rows wider than 1024 cells) staged in shared memory by bulk
  * copies (TMA) through an mbarrier ring.  AUTO (default): the autotuner times the eligible ones.
  * Both give bit-identical results.                                                                  */
 enum lbm_kernel { LBM_KERNEL_AUTO = 0, LBM_KERNEL_PLAIN = 1, LBM_KERNEL_ROWS = 2 };

@@ -166,7 +166,8 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         int b = tid / nx, x = tid - b * nx;
 #pragma unroll 1
         for (int c = tid; c < it.nb * nx; c += CONS) {
-            row_cell<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc, out0 + (long long)b * nx);
+            row_cell_wrap<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
+                                       out0 + (long long)b * nx);
             x += CONS;
             while (x >= nx) {
                 x -= nx;

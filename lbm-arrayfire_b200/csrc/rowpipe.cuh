@@ -115,11 +115,21 @@ constexpr unsigned long long pack_c(bool z) {
 //   B         rows per group at nx == PITCH; the host may put more rows of a narrower lattice into
 //             the same stage (runtime rows per group, at most B * PITCH / nx)
 //   NS        stages
-template <class L, class S, int PITCH>
+//   SEG       rows wider than PITCH: a work item is one row segment of up to SEGW = PITCH - 16 cells
+//             (SEGW_RUN by default) staged with HALO = 8 cells on either side, one segment per stage;
+//             CR only sets the consumer count, and every stage the CTA's shared memory holds is used
+template <class L, class S, int PITCH, bool SEG = false>
 struct RowPipeShape {
+    static constexpr int HALO = 8;
+    static constexpr int SEGW = PITCH - 2 * HALO;
     static constexpr int Q = L::Q;
     static constexpr bool k16 = sizeof(S) == 2;
     static constexpr bool k3 = L::DIM == 3;
+    // segment width the segmented kernel runs with: a stage costs about max(floor, its cells' compute),
+    // the floor (the stage's refill latency) near 900 D3Q27 cells; A/B, D3Q27 MRT F16S GLUPS at
+    // 2048/3072/4096 x 128 x ...: 896 37.7/42.0/44.7, 1008 36.3/40.9/43.5, 832 36.8/40.6/43.7;
+    // D2Q9 8192^2 F16S: 1008 134.6, 896 133.4
+    static constexpr int SEGW_RUN = k3 ? 896 : SEGW;
     static constexpr int THREADS = PITCH > LBM_ROWPIPE_THREADS ? LBM_ROWPIPE_THREADS : PITCH;
     static constexpr int XPT = PITCH / THREADS;
     static constexpr int kRowBytes = PITCH * (int)sizeof(S);
@@ -127,6 +137,7 @@ struct RowPipeShape {
     // (FP32 85.1 vs 78.3 GLUPS against the D3Q27 shape)
     static constexpr int kGroupBytes =
         LBM_ROWPIPE_GROUP_BYTES > 0 ? LBM_ROWPIPE_GROUP_BYTES : (!k3 ? 2048 : k16 ? 4096 : 1024);
+    // segments (SEG) stage one row segment per stage: CR only sets the consumer count (B stays 1)
     static constexpr int CRQ = LBM_ROWPIPE_CR > 0 ? LBM_ROWPIPE_CR : (k3 ? 2 : 1);
     static constexpr int CR0 = CRQ * THREADS > 512 ? 512 / THREADS : CRQ;
     static constexpr int CR = CR0 < 1 ? 1 : CR0;
@@ -139,14 +150,15 @@ struct RowPipeShape {
     static constexpr int CTAS = fits(CTAS_R) ? CTAS_R : (CTAS_R > 2 && fits(2) ? 2 : 1);
     static constexpr int kLimit = limit_of(CTAS);  // smem per CTA
     static constexpr int kBudget = (CTAS == 1 ? (k16 ? 216 : 166) : CTAS == 2 ? (k16 ? 110 : 83) : 72) * 1024;
-    static constexpr int B0 = kGroupBytes / kRowBytes;
+    static constexpr int B0 = SEG ? 1 : kGroupBytes / kRowBytes;
     static constexpr int B1 = B0 < CR ? CR : B0;
     static constexpr int BMAX0 = (kLimit - 128) / (2 * (Q * kRowBytes + PITCH));
-    static constexpr int BMAX = BMAX0 > 8 ? 8 : BMAX0;
+    static constexpr int BMAX = SEG ? 1 : BMAX0 > 8 ? 8 : BMAX0;
     static constexpr int B = B1 > BMAX ? BMAX : (B1 < 1 ? 1 : B1);
     static constexpr int SB = B * PITCH;  // elements per direction in a stage
     static constexpr int STAGE = Q * SB * (int)sizeof(S) + SB;  // populations + mask bytes
-    static constexpr int NSB = (kBudget < kLimit - 128 ? kBudget : kLimit - 128) / STAGE;
+    // segments (one short row per stage) take every stage the CTA's shared memory holds: depth in flight
+    static constexpr int NSB = (SEG || kBudget > kLimit - 128 ? kLimit - 128 : kBudget) / STAGE;
     static constexpr int NS0 = LBM_ROWPIPE_NS > 0 ? LBM_ROWPIPE_NS : NSB;
     static constexpr int NS = NS0 < 2 ? 2 : (NS0 > 8 ? 8 : NS0);
     static_assert(B >= 1, "a row group must fit twice into shared memory");
@@ -164,15 +176,20 @@ struct RowPipeShape {
     }
 };
 
+// Staged pitch of the segmented kernel: segments of up to 1008 cells plus two 8-cell halos.  (512-cell
+// segments in 528-cell stages, 7 of them in flight, were measured: 2048 x 128 x 64 D3Q27 MRT F16S
+// 28.7 vs 35.8 GLUPS with 1008-cell segments; short segments mean small bulk copies.)
+constexpr int kSegPitch = 1024;
+
 // One cell of the row pipeline: st points at the staged row of direction 0 (direction i at
-// st[i * SB]), mrow at the cell classes of the row, orow at the row's first cell in the output buffer.
+// st[i * SB]); x, xm, xp are the staged indices of the cell and of its left and right neighbours
+// (periodic wrap already applied), mrow[mi] its class, orow[ox] its place in the output row.
 template <class L, class S, int SB, int COLL, class P>
-__device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t* mrow, int x, int nx,
-                                         typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow) {
+__device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t* mrow, int x, int xm, int xp,
+                                         int mi, int ox, typename Codec<S>::Real sc, typename Codec<S>::Real isc,
+                                         S* orow) {
     using R = typename Codec<S>::Real;
     constexpr int Q = L::Q;
-    const int xm = x == 0 ? nx - 1 : x - 1;
-    const int xp = x == nx - 1 ? 0 : x + 1;
     R v[Q];
     static_for<Q>([&](auto I) {
         constexpr int i = I;
@@ -180,7 +197,7 @@ __device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t*
         const int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
         v[i] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
     });
-    const int cls = mrow ? (int)mrow[x] : 0;
+    const int cls = mrow ? (int)mrow[mi] : 0;
     const uint32_t fl = p.cls.flags[cls];
     if (fl & kZeroGradXp) {
         static_for<Q>([&](auto I) {
@@ -208,11 +225,20 @@ __device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t*
             });
         }
     }
-    S* __restrict__ fo = orow + x;
+    S* __restrict__ fo = orow + ox;
     static_for<Q>([&](auto I) {
         constexpr int i = I;
         fo[(long long)i * p.N] = Codec<S>::enc(out[i], R(L::w(i)));
     });
+}
+
+// A cell of a whole staged row of width nx (periodic in x).
+template <class L, class S, int SB, int COLL, class P>
+__device__ __forceinline__ void row_cell_wrap(const P& p, const S* st, const uint8_t* mrow, int x, int nx,
+                                              typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow) {
+    const int xm = x == 0 ? nx - 1 : x - 1;
+    const int xp = x == nx - 1 ? 0 : x + 1;
+    row_cell<L, S, SB, COLL>(p, st, mrow, x, xm, xp, x, x, sc, isc, orow);
 }
 
 // COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt).  Deviation arithmetic.
@@ -245,14 +271,16 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int B = rows;
     const int gy = (ny + B - 1) / B;  // row groups per z plane; the last one may be short
-    const long long groups = (long long)gy * nz;
+    // item indices in 32 bits (the host keeps the item count below 2^31): a 64-bit division by a
+    // runtime divisor is a long software sequence, paid once per stage by every consumer thread
+    const unsigned groups = (unsigned)gy * (unsigned)nz, ugy = (unsigned)gy;
     const uint32_t row_bytes = (uint32_t)(nx * sizeof(S));
-    const long long first = blockIdx.x, stride = gridDim.x;
+    const unsigned first = blockIdx.x, stride = gridDim.x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
 
     // Issue the bulk loads of group g into stage s (one warp; lanes 0..Q-1 one direction each).
-    auto issue = [&](long long g, int s) {
-        const int y0 = (int)(g % gy) * B, z = (int)(g / gy);
+    auto issue = [&](unsigned g, int s) {
+        const int y0 = (int)(g % ugy) * B, z = (int)(g / ugy);
         const int nb = ny - y0 < B ? ny - y0 : B;
         if (lane == 0)
             mbar_arrive_expect_tx(&full[s], (uint32_t)(Q * nb) * row_bytes + (has_mask ? (uint32_t)(nb * nx) : 0u));
@@ -284,7 +312,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     if (tid >= Sh::CONSUMERS) {  // producer warp
         for (int s = 0; s < NS; ++s)
             if (first + s * stride < groups) issue(first + s * stride, s);
-        for (long long k = 0; first + (k + NS) * stride < groups; ++k) {
+        for (unsigned k = 0; first + (k + NS) * stride < groups; ++k) {
             const int s = (int)(k % NS);
             if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1))) {
                 if (lane == 0) atomicExch(err, kRowPipeTimeout);
@@ -298,8 +326,8 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     const int tx = tid % Sh::THREADS, rset = tid / Sh::THREADS;
     R sc, isc;
     storage_scale<S>(p, sc, isc);
-    for (long long k = 0; first + k * stride < groups; ++k) {
-        const long long g = first + k * stride;
+    for (unsigned k = 0; first + k * stride < groups; ++k) {
+        const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
         if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1))) {
             if (lane == 0) atomicExch(err, kRowPipeTimeout);
@@ -308,7 +336,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
                 if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1), 1LL << 28)) break;
             return;
         }
-        const int y0 = (int)(g % gy) * B, z = (int)(g / gy);
+        const int y0 = (int)(g % ugy) * B, z = (int)(g / ugy);
         const int nb = ny - y0 < B ? ny - y0 : B;
 #pragma unroll 1
         for (int b = rset; b < nb; b += CR) {
@@ -318,11 +346,127 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
 #pragma unroll 1
             for (int xx = 0; xx < Sh::XPT; ++xx) {
                 const int x = tx + xx * Sh::THREADS;
-                if (x < nx) row_cell<L, S, SB, COLL>(p, st, mrow, x, nx, sc, isc, orow);
+                if (x < nx) row_cell_wrap<L, S, SB, COLL>(p, st, mrow, x, nx, sc, isc, orow);
             }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
+    }
+}
+
+// Rows wider than 1024 cells: a work item is one row segment [x0, x0 + w), x0 = seg * segw, w = segw
+// except for the row's last segment, staged with HALO = 8 cells on either side, so the pull's x
+// neighbours of every cell are in shared memory.  segw (host-chosen, seg_width in runtime.cu) is a
+// multiple of 16 and at most SEGW = kSegPitch - 16 = 1008.  The halos of the first and the last
+// segment of a row are the row's other end (periodic in x) and come by their own copies (16 bytes for
+// 16-bit storage, 32 for FP32).  With nx a multiple of 16 every copy starts on a 16-byte boundary and moves a multiple of
+// 16 bytes: population rows at x0 - 8, mask rows at x0 for w bytes.  Stage s, direction i, staged
+// index j holds x = x0 - HALO + j.
+template <class L, class S, int COLL>
+__global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS + 32, RowPipeShape<L, S, kSegPitch, true>::CTAS)
+    k_step_rows_seg(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int segw, int* __restrict__ err) {
+    using R = typename Codec<S>::Real;
+    using Sh = RowPipeShape<L, S, kSegPitch, true>;
+    constexpr int Q = L::Q;
+    constexpr int NS = Sh::NS;
+    constexpr int SB = Sh::SB;
+    constexpr int H = Sh::HALO;
+    constexpr int W = Sh::CONSUMERS / 32;
+    static_assert(NS <= 8, "barriers occupy the first 128 bytes");
+    static_assert(SB >= Sh::SEGW + 2 * H && Sh::SEGW % 16 == 0, "segment and halos must fit the staged row");
+    const int SW = segw;
+    constexpr unsigned long long kCy = pack_c<L>(false), kCz = pack_c<L>(true);
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* empty = full + NS;
+    S* in = reinterpret_cast<S*>(smem + 128);                                 // [NS][Q][SB]
+    uint8_t* mask_st = reinterpret_cast<uint8_t*>(in + (size_t)NS * Q * SB);  // [NS][SB]
+    const bool has_mask = p.mask != nullptr;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    const int nseg = (nx + SW - 1) / SW;
+    const unsigned groups = (unsigned)nseg * (unsigned)ny * (unsigned)nz;  // < 2^31 (host-checked)
+    const unsigned useg = (unsigned)nseg, uny = (unsigned)ny;
+    const unsigned first = blockIdx.x, stride = gridDim.x;
+    const S* __restrict__ fin = static_cast<const S*>(p.fin);
+
+    auto issue = [&](unsigned g, int s) {
+        const unsigned row = g / useg;
+        const int seg = (int)(g - row * useg);
+        const int z = (int)(row / uny), y = (int)(row - (unsigned)z * uny);
+        const int x0 = seg * SW;
+        const int w = nx - x0 < SW ? nx - x0 : SW;
+        if (lane == 0)
+            mbar_arrive_expect_tx(&full[s], (uint32_t)(Q * (w + 2 * H) * sizeof(S)) + (has_mask ? (uint32_t)w : 0u));
+        __syncwarp();
+        if (lane < Q) {
+            const int cy = (int)((kCy >> (2 * lane)) & 3) - 1, cz = (int)((kCz >> (2 * lane)) & 3) - 1;
+            int zs = z - cz, ys = y - cy;
+            zs = zs < 0 ? zs + nz : (zs >= nz ? zs - nz : zs);
+            ys = ys < 0 ? ys + ny : (ys >= ny ? ys - ny : ys);
+            const S* src = fin + (long long)lane * p.N + ((long long)zs * ny + ys) * nx;
+            S* dst = in + ((long long)s * Q + lane) * SB;
+            const bool left = x0 == 0, right = x0 + w == nx;
+            if (!left && !right) {
+                bulk_load(dst, src + x0 - H, (uint32_t)((w + 2 * H) * sizeof(S)), &full[s]);
+            } else if (left) {  // nx > SW: the first segment is never the last
+                bulk_load(dst + H, src, (uint32_t)((w + H) * sizeof(S)), &full[s]);
+                bulk_load(dst, src + nx - H, (uint32_t)(H * sizeof(S)), &full[s]);
+            } else {
+                bulk_load(dst, src + x0 - H, (uint32_t)((w + H) * sizeof(S)), &full[s]);
+                bulk_load(dst + H + w, src, (uint32_t)(H * sizeof(S)), &full[s]);
+            }
+        } else if (lane == Q && has_mask) {
+            bulk_load(mask_st + s * SB, p.mask + ((long long)z * ny + y) * nx + x0, (uint32_t)w, &full[s]);
+        }
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], W);
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid >= Sh::CONSUMERS) {  // producer warp
+        for (int s = 0; s < NS; ++s)
+            if (first + s * stride < groups) issue(first + s * stride, s);
+        for (unsigned k = 0; first + (k + NS) * stride < groups; ++k) {
+            const int s = (int)(k % NS);
+            if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1))) {
+                if (lane == 0) atomicExch(err, kRowPipeTimeout);
+                return;
+            }
+            issue(first + (k + NS) * stride, s);
+        }
+        return;
+    }
+    R sc, isc;
+    storage_scale<S>(p, sc, isc);
+    for (unsigned k = 0; first + k * stride < groups; ++k) {
+        const unsigned g = first + k * stride;
+        const int s = (int)(k % NS);
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1))) {
+            if (lane == 0) atomicExch(err, kRowPipeTimeout);
+            for (int j = 1; j < NS && first + (k + j) * stride < groups; ++j)
+                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1), 1LL << 28)) break;
+            return;
+        }
+        const unsigned row = g / useg;
+        const int seg = (int)(g - row * useg);
+        const int x0 = seg * SW;
+        const int w = nx - x0 < SW ? nx - x0 : SW;
+        const S* st = in + (long long)s * Q * SB + H;  // staged index of x0 is 0
+        const uint8_t* mrow = has_mask ? mask_st + s * SB : nullptr;
+        S* orow = static_cast<S*>(p.fout) + (long long)row * nx + x0;
+#pragma unroll 1
+        for (int xl = tid; xl < w; xl += Sh::CONSUMERS)
+            row_cell<L, S, SB, COLL>(p, st, mrow, xl, xl - 1, xl + 1, xl, xl, sc, isc, orow);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
     }
 }
 

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -125,7 +126,7 @@ struct lbm_ctx {
     int kernel = LBM_KERNEL_AUTO;  // requested family
     int kernel_used = 0;           // family chosen (PLAIN or ROWS); 0 before the first step
     int rows_grid = 0;             // persistent grid of the row pipeline
-    int rows_rpg = 1;              // its rows per group
+    int rows_rpg = 1;              // its rows per group (segmented rows: the segment width)
     int* err = nullptr;            // device error word of the row pipeline
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int gsteps = 0;
@@ -191,19 +192,33 @@ StepParams<double>& params_of<double>(lbm_ctx* c) {
 }
 
 // ---- row pipeline (rowpipe.cuh) ------------------------------------------------------------
-// D3Q27 BGK/MRT or D2Q9 BGK, deviation arithmetic, F32/F16S/BF16S, 32 <= nx <= 1024 and nx a
-// multiple of 16: every bulk copy (population rows of nx * s bytes, mask rows of nx bytes) must start
-// on a 16-byte boundary and move a multiple of 16 bytes.
+// D3Q27 BGK/MRT or D2Q9 BGK, deviation arithmetic, F32/F16S/BF16S, nx >= 32 and a multiple of 16:
+// every bulk copy (population rows or segments, mask rows) must start on a 16-byte boundary and move a
+// multiple of 16 bytes.  Rows wider than 1024 cells go by segments (k_step_rows_seg).
 static bool rows_eligible(const lbm_ctx* c) {
     const lbm_desc& d = c->d;
     const bool coll_ok = d.lattice == LBM_D3Q27 ? (d.collision == LBM_BGK || d.collision == LBM_MRT)
                                                : d.collision == LBM_BGK;
+    // work items (row groups or row segments) are counted in 32 bits
+    const bool items_ok = (long long)d.ny * d.nz * ((d.nx + 63) / 64) < (1LL << 31);
     return coll_ok && d.arithmetic == LBM_ARITH_DEVIATION && d.storage != LBM_F64 && d.nx >= 32 &&
-           d.nx <= 1024 && d.nx % 16 == 0;
+           d.nx % 16 == 0 && items_ok;
 }
+static bool rows_segmented(const lbm_ctx* c) { return c->d.nx > 1024; }
+
+// Segment width of the segmented row kernel (RowPipeShape::SEGW_RUN: 896 cells for D3Q27, 1008 for D2Q9).
+#ifndef LBM_ROWPIPE_SEGW
+#define LBM_ROWPIPE_SEGW 0  // > 0: a narrower segment width (a multiple of 16), for A/B builds
+#endif
+static int seg_width(int w) { return LBM_ROWPIPE_SEGW > 0 ? std::min(LBM_ROWPIPE_SEGW / 16 * 16, 1008) : w; }
 
 template <class L, class S, int PITCH, int COLL>
 static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s) {
+    if (rows_segmented(c)) {
+        using Sh = RowPipeShape<L, S, kSegPitch, true>;
+        k_step_rows_seg<L, S, COLL><<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err);
+        return;
+    }
     using Sh = RowPipeShape<L, S, PITCH>;
     auto kern = k_step_rows<L, S, PITCH, COLL>;
     kern<<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err);  // + producer warp
@@ -211,16 +226,41 @@ static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>&
 
 template <class L, class S, int PITCH, int COLL>
 static int prepare_rows_t(lbm_ctx* c) {
-    using Sh = RowPipeShape<L, S, PITCH>;
-    auto kern = k_step_rows<L, S, PITCH, COLL>;
-    LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
     int per_sm = 0, sms = 0;
-    LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
     LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->d.device));
+    long long groups = 0;
+    int gy = 1;
+    if (rows_segmented(c)) {
+        using Sh = RowPipeShape<L, S, kSegPitch, true>;
+        auto kern = k_step_rows_seg<L, S, COLL>;
+        LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
+        LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
+        c->rows_rpg = seg_width(Sh::SEGW_RUN);
+        const int nseg = (int)((c->d.nx + c->rows_rpg - 1) / c->rows_rpg);
+        groups = (long long)nseg * c->d.ny * c->d.nz;
+        if (per_sm < 1) return set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
+        // CTA b takes items b, b + grid, ...; with grid and nseg coprime it cycles through every
+        // segment of a row, so no CTA is left with only the short last segments (148 = 4 x 37 CTAs
+        // and 4 segments per row would be)
+        int grid = (int)std::min<long long>(groups, (long long)per_sm * sms);
+        while (grid > 1 && std::gcd(grid, nseg) != 1) --grid;
+        c->rows_grid = grid;
+        return LBM_OK;
+    } else {
+        using Sh = RowPipeShape<L, S, PITCH>;
+        auto kern = k_step_rows<L, S, PITCH, COLL>;
+        LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
+        LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
+        c->rows_rpg = Sh::rows_per_group((int)c->d.nx);
+        gy = (int)((c->d.ny + c->rows_rpg - 1) / c->rows_rpg);
+        groups = (long long)gy * c->d.nz;
+    }
     if (per_sm < 1) return set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
-    c->rows_rpg = Sh::rows_per_group((int)c->d.nx);
-    const long long groups = (c->d.ny + c->rows_rpg - 1) / c->rows_rpg * c->d.nz;
-    c->rows_grid = (int)std::min<long long>(groups, (long long)per_sm * sms);
+    int grid = (int)std::min<long long>(groups, (long long)per_sm * sms);
+    // a short last group in every plane: as for segments, keep it from landing on the same CTAs
+    if (c->d.ny % c->rows_rpg != 0)
+        while (grid > 1 && std::gcd(grid, gy) != 1) --grid;
+    c->rows_grid = grid;
     return LBM_OK;
 }
 
@@ -872,7 +912,7 @@ int lbm_set_kernel(lbm_ctx* c, int kind) {
     if (kind == LBM_KERNEL_ROWS && !rows_eligible(c))
         return set_error(LBM_ERR_UNSUPPORTED,
                          "the row pipeline needs D3Q27 BGK/MRT or D2Q9 BGK, deviation arithmetic, F32/F16S/BF16S "
-                         "and 32 <= nx <= 1024 with nx a multiple of 16");
+                         "and nx >= 32 a multiple of 16");
     LBM_CK(cudaSetDevice(c->d.device));
     LBM_CK(cudaStreamSynchronize(c->stream));
     drop_graphs(c);

@@ -334,11 +334,51 @@ def test_row_pipeline_other_widths_and_d2q9_equal_plain(storage, case):
     assert np.array_equal(a, b)
 
 
+def _periodic_noise(d, seed):
+    """Random near-equilibrium start on a mask-free (fully periodic) lattice: exercises the x wrap."""
+    _, _, _, w, _ = lb.velocities(d.lattice)
+    n = d.nx * d.ny * d.nz
+    rng = np.random.default_rng(seed)
+    return np.repeat(w, n) * (1.0 + 0.02 * rng.standard_normal(len(w) * n))
+
+
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.BF16S])
+@pytest.mark.parametrize("case", ["d2q9_channel_2048", "d2q9_periodic_1040", "d3q27_duct_2016",
+                                  "d3q27_mrt_periodic_1280", "d3q27_mrt_lid_3056"])
+def test_row_pipeline_segmented_wide_rows_equal_plain(storage, case):
+    """Rows wider than 1024 cells go through the segmented row kernel (1008-cell segments with 8-cell
+    halos; the first and last segment fetch their halo from the row's other end).  Widths with a
+    32-cell last segment (1040, 2048, 3056) and with whole segments (2016); inlets, zero-gradient
+    outlets, bounce-back walls and the periodic wrap all cross segment edges: bit-identical to the
+    one-cell-per-thread kernel."""
+    if case == "d2q9_channel_2048":
+        d, m, F0 = channel2d(2048, 40, 0.04, 100.0, 1000, 20, 8, storage=storage, config_mode=True, seed=2,
+                             noise=1e-4)
+    elif case == "d2q9_periodic_1040":
+        d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (1040, 24), omega=1.6)
+        m, F0 = None, _periodic_noise(d, 5)
+    elif case == "d3q27_duct_2016":
+        d = lb.make_desc(lb.D3Q27, lb.BGK, storage, (2016, 10, 6), omega=1.7)
+        m = lb.setup_duct3d(d, 0.04, 1008, 5, 3, 2)
+        F0 = None
+    elif case == "d3q27_mrt_periodic_1280":
+        d = lb.make_desc(lb.D3Q27, lb.MRT, storage, (1280, 6, 5), mrt_s=lb.mrt_rates(1.7, 1.1),
+                         mrt_basis=lb.MRT_GRAM_SCHMIDT)
+        m, F0 = None, _periodic_noise(d, 6)
+    else:
+        d = lb.make_desc(lb.D3Q27, lb.MRT, storage, (3056, 6, 5), mrt_s=lb.mrt_rates(1.8, 1.2),
+                         mrt_basis=lb.MRT_REF)
+        m = lb.setup_cavity3d(d, 0.05)
+        F0 = None
+    a, b = _rows_vs_plain(d, m, F0, 25)
+    assert np.array_equal(a, b)
+
+
 def test_row_pipeline_needs_eligible_shape():
     rejected = [
         lb.make_desc(lb.D2Q9, lb.SHANCHEN, lb.F32, (128, 128), omega=1.0, sc_G=-5.0),  # two-pass model
         lb.make_desc(lb.D3Q27, lb.BGK, lb.F32, (100, 8, 8), omega=1.3),  # 100-byte mask rows
-        lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (2048, 8), omega=1.3),  # wider than 1024
+        lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (2056, 8), omega=1.3),  # segmented, but 2056 % 16 != 0
         lb.make_desc(lb.D3Q27, lb.BGK, lb.F64, (128, 8, 8), omega=1.3),  # FP64 storage
         lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (128, 8), omega=1.3, arithmetic=lb.ARITH_ABSOLUTE),
     ]
