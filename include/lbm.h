@@ -164,6 +164,13 @@ int   lbm_set_stream(lbm_ctx* c, void* stream);          /* NULL restores the co
 /* Current population buffer on the device (storage type of the descriptor) and its byte size. */
 void* lbm_device_populations(lbm_ctx* c, size_t* bytes);
 int   lbm_get_desc(const lbm_ctx* c, lbm_desc* out);
+/* Faces of the slowest axis (z planes of D3Q27, y rows of D2Q9) for halo exchanges between slabs of
+ * one lattice (no counterpart in the reference, which runs on one device): the populations of
+ * directions dirs[0..ndirs) on plane `plane` of the current buffer, packed [ndirs][plane cells] as
+ * stored words (the descriptor's storage type, no conversion, so an exchange is bit-exact).
+ * memory = LBM_DEVICE: asynchronous on the context stream; LBM_HOST: returns when the copy is done. */
+int   lbm_face_get(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, void* dst, int memory);
+int   lbm_face_set(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, const void* src, int memory);
 /* Block width (threads along x) used by the step kernel; 0 = autotune on first step. */
 int   lbm_set_block(lbm_ctx* c, int threads_x);
 int   lbm_get_block(const lbm_ctx* c);

@@ -159,7 +159,8 @@ struct RowPipeShape {
     static constexpr int STAGE = Q * SB * (int)sizeof(S) + SB;  // populations + mask bytes
     // segments (one short row per stage) take every stage the CTA's shared memory holds: depth in flight
     static constexpr int NSB = (SEG || kBudget > kLimit - 128 ? kLimit - 128 : kBudget) / STAGE;
-    static constexpr int NS0 = LBM_ROWPIPE_NS > 0 ? LBM_ROWPIPE_NS : NSB;
+    static constexpr int NSF = (kLimit - 128) / STAGE;  // stages that fit at all
+    static constexpr int NS0 = LBM_ROWPIPE_NS > 0 ? (LBM_ROWPIPE_NS < NSF ? LBM_ROWPIPE_NS : NSF) : NSB;
     static constexpr int NS = NS0 < 2 ? 2 : (NS0 > 8 ? 8 : NS0);
     static_assert(B >= 1, "a row group must fit twice into shared memory");
     static_assert((size_t)NS * STAGE + 128 <= (size_t)kLimit, "row pipeline stages exceed the shared-memory budget");

@@ -885,6 +885,43 @@ void* lbm_device_populations(lbm_ctx* c, size_t* bytes) {
     return c->f[c->cur];
 }
 
+// One plane of the slowest axis is contiguous per direction in the [x, y(, z), i] layout, so a face is
+// one copy per direction.
+static int face_copy(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, void* host_or_dev,
+                     int memory, bool get) {
+    if (!c || !dirs || !host_or_dev) return set_error(LBM_ERR_INVALID, "NULL argument");
+    if (memory != LBM_HOST && memory != LBM_DEVICE) return set_error(LBM_ERR_INVALID, "memory must be HOST or DEVICE");
+    const long long planes = c->dim == 3 ? c->d.nz : c->d.ny;
+    if (plane < 0 || plane >= planes) return set_error(LBM_ERR_INVALID, "plane outside the lattice");
+    if (ndirs < 1 || ndirs > c->q) return set_error(LBM_ERR_INVALID, "ndirs must be in 1..Q");
+    for (int k = 0; k < ndirs; ++k)
+        if (dirs[k] < 0 || dirs[k] >= c->q) return set_error(LBM_ERR_INVALID, "direction outside 0..Q-1");
+    LBM_CK(cudaSetDevice(c->d.device));
+    const long long cells = c->N / planes;
+    const size_t bytes = (size_t)cells * c->sbytes;
+    char* f = static_cast<char*>(c->f[c->cur]);
+    char* io = static_cast<char*>(host_or_dev);
+    const cudaMemcpyKind kind = memory == LBM_HOST ? (get ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice)
+                                                   : cudaMemcpyDeviceToDevice;
+    for (int k = 0; k < ndirs; ++k) {
+        char* dev = f + ((size_t)dirs[k] * c->N + (size_t)plane * cells) * c->sbytes;
+        if (get)
+            LBM_CK(cudaMemcpyAsync(io + k * bytes, dev, bytes, kind, c->stream));
+        else
+            LBM_CK(cudaMemcpyAsync(dev, io + k * bytes, bytes, kind, c->stream));
+    }
+    if (memory == LBM_HOST) LBM_CK(cudaStreamSynchronize(c->stream));
+    return LBM_OK;
+}
+
+int lbm_face_get(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, void* dst, int memory) {
+    return face_copy(c, plane, dirs, ndirs, dst, memory, true);
+}
+
+int lbm_face_set(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, const void* src, int memory) {
+    return face_copy(c, plane, dirs, ndirs, const_cast<void*>(src), memory, false);
+}
+
 int lbm_get_desc(const lbm_ctx* c, lbm_desc* out) {
     if (!c || !out) return set_error(LBM_ERR_INVALID, "NULL argument");
     *out = c->d;

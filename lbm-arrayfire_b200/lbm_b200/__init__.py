@@ -31,6 +31,7 @@ LIB_PATH = Path(os.environ.get("LBM_B200_LIB", Path(__file__).resolve().parent /
 D2Q9, D3Q27 = 0, 1
 BGK, MRT, SHANCHEN = 0, 1, 2
 F32, F16S, BF16S, F64 = 0, 1, 2, 3
+STORAGE_BYTES = {F32: 4, F16S: 2, BF16S: 2, F64: 8}  # bytes of one stored population
 MRT_REF, MRT_GRAM_SCHMIDT = 0, 1
 ARITH_DEVIATION, ARITH_ABSOLUTE = 0, 1
 KERNEL_AUTO, KERNEL_PLAIN, KERNEL_ROWS = 0, 1, 2
@@ -107,6 +108,8 @@ _SIGS = {
     "lbm_stream": (_P, [_P]),
     "lbm_set_stream": (C.c_int, [_P, _P]),
     "lbm_device_populations": (_P, [_P, C.POINTER(C.c_size_t)]),
+    "lbm_face_get": (C.c_int, [_P, C.c_int64, C.POINTER(C.c_int32), C.c_int32, _P, C.c_int]),
+    "lbm_face_set": (C.c_int, [_P, C.c_int64, C.POINTER(C.c_int32), C.c_int32, _P, C.c_int]),
     "lbm_get_desc": (C.c_int, [_P, _DP]),
     "lbm_set_block": (C.c_int, [_P, C.c_int]),
     "lbm_get_block": (C.c_int, [_P]),
@@ -351,6 +354,34 @@ class Lattice:
         nbytes = C.c_size_t()
         p = lib().lbm_device_populations(self._h, C.byref(nbytes))
         return p, nbytes.value
+
+    def face_cells(self) -> int:
+        """Cells of one plane of the slowest axis (nx*ny for D3Q27, nx for D2Q9)."""
+        return self.n // (self.desc.nz if self.dim == 3 else self.desc.ny)
+
+    def _face(self, fn, plane: int, dirs, buf):
+        dirs = [int(i) for i in dirs]
+        want = len(dirs) * self.face_cells() * STORAGE_BYTES[self.desc.storage]
+        if hasattr(buf, "data_ptr"):
+            got, ptr, mem = buf.numel() * buf.element_size(), _torch_ptr(buf), DEVICE if buf.is_cuda else HOST
+            assert buf.is_contiguous()
+        else:
+            assert buf.flags["C_CONTIGUOUS"]
+            got, ptr, mem = buf.nbytes, _ptr(buf), HOST
+        if got != want:
+            raise ValueError(f"face buffer holds {got} bytes, {want} needed")
+        _check(fn(self._h, plane, (C.c_int32 * len(dirs))(*dirs), len(dirs), ptr, mem))
+        return buf
+
+    def face_get(self, plane: int, dirs, out):
+        """Populations of directions `dirs` on plane `plane` of the slowest axis (z for D3Q27, y for
+        D2Q9) as stored words into `out` (numpy array or torch tensor of len(dirs) * face_cells()
+        words of the storage type; CUDA copies are asynchronous on the lattice's stream)."""
+        return self._face(lib().lbm_face_get, plane, dirs, out)
+
+    def face_set(self, plane: int, dirs, src):
+        """Inverse of face_get: write stored words into plane `plane` of the current buffer."""
+        return self._face(lib().lbm_face_set, plane, dirs, src)
 
     def init_equilibrium(self, rho=None, u=None):
         r = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64).ravel(order="F")

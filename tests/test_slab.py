@@ -1,0 +1,180 @@
+"""Slab decomposition of one lattice (lbm_b200.slab): ghost planes, the per-step face exchange and the
+gather must reproduce the undivided lattice bit for bit.
+
+CPU: the oracle steps every slab (one process, and a gloo world of 2 and 3 processes exchanging
+faces with isend/irecv).  GPU: the engine steps every slab of a `SlabSet` on one device (plain copies
+between slabs, no collective) and matches one engine lattice of the full size.
+"""
+import json
+import os
+import socket
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from helpers import O, channel2d, lb, oracle_problem
+
+from lbm_b200.slab import Slab, SlabSet, axis_dirs, local_problem, scatter_populations, split_planes
+
+
+class OracleStepper:
+    """The oracle behind the stepper interface Slab uses (FP64 populations are the stored words)."""
+
+    def __init__(self, desc, mask):
+        self.p = oracle_problem(desc, mask)
+        self.q, self.n = desc.q, desc.cells
+        self.planes = desc.nz if desc.dim == 3 else desc.ny
+        self.F = None
+
+    def face_cells(self):
+        return self.n // self.planes
+
+    def set_populations(self, F):
+        self.F = np.array(F, dtype=np.float64)
+
+    def get_populations(self, dtype=np.float64):
+        return self.F.astype(dtype)
+
+    def step(self, n=1):
+        self.F = O.run(self.p, self.F, n, dtype=np.float64, threads=1)[0]
+
+    def _view(self):
+        return self.F.reshape(self.q, self.planes, -1)
+
+    def face_get(self, plane, dirs, out):
+        a = out.numpy() if hasattr(out, "numpy") else out
+        a.reshape(len(dirs), -1)[:] = self._view()[dirs, plane, :]
+        return out
+
+    def face_set(self, plane, dirs, src):
+        a = src.numpy() if hasattr(src, "numpy") else src
+        self._view()[dirs, plane, :] = np.asarray(a).reshape(len(dirs), -1)
+
+    def set_stream(self, stream):
+        pass
+
+
+def mrt_cavity3d(storage=lb.F64, n=(12, 8, 9)):
+    d = lb.make_desc(lb.D3Q27, lb.MRT, storage, n, mrt_s=lb.mrt_rates(1.7, 1.1), mrt_basis=lb.MRT_GRAM_SCHMIDT)
+    m = lb.setup_cavity3d(d, 0.05)
+    _, _, _, w, _ = lb.velocities(lb.D3Q27)
+    rng = np.random.default_rng(11)
+    F0 = np.repeat(w, d.cells) * (1.0 + 0.01 * rng.standard_normal(27 * d.cells))
+    return d, m, F0
+
+
+def channel(storage=lb.F64, nx=48, ny=20):
+    return channel2d(nx, ny, 0.04, 100.0, 14, 10, 4, storage=storage, config_mode=True, seed=1, noise=1e-3)
+
+
+def periodic3d(storage=lb.F64, n=(8, 6, 7)):
+    d = lb.make_desc(lb.D3Q27, lb.BGK, storage, n, omega=1.6)
+    _, _, _, w, _ = lb.velocities(lb.D3Q27)
+    rng = np.random.default_rng(12)
+    return d, None, np.repeat(w, d.cells) * (1.0 + 0.02 * rng.standard_normal(27 * d.cells))
+
+
+CASES = {"mrt_cavity3d": mrt_cavity3d, "channel2d": channel, "periodic3d": periodic3d}
+
+
+def test_split_planes_and_axis_dirs():
+    for n, world in [(10, 3), (7, 7), (256, 8), (5, 1)]:
+        parts = split_planes(n, world)
+        sizes = [b - a for a, b in parts]
+        assert parts[0][0] == 0 and parts[-1][1] == n and max(sizes) - min(sizes) <= 1 and min(sizes) >= 1
+        assert all(parts[k][1] == parts[k + 1][0] for k in range(world - 1))
+    with pytest.raises(ValueError):
+        split_planes(3, 4)
+    for lat, k in [(lb.D3Q27, 9), (lb.D2Q9, 3)]:
+        up, down = axis_dirs(lat)
+        assert len(up) == len(down) == k
+        opp = lb.velocities(lat)[4]
+        assert sorted(int(opp[i]) for i in up) == down
+
+
+def test_local_problem_ghost_planes_and_rejects_shanchen():
+    d, m, F0 = mrt_cavity3d()
+    ld, lm = local_problem(d, m, 3, 7)
+    assert (ld.nx, ld.ny, ld.nz) == (12, 8, 6) and ld.n_classes == d.n_classes + 1
+    g = lm.reshape(6, -1)
+    assert (g[0] == d.n_classes).all() and (g[-1] == d.n_classes).all()
+    assert np.array_equal(g[1:5].ravel(), np.asarray(m).ravel(order="F")[3 * 96:7 * 96])
+    Fl = scatter_populations(d, F0, 0, 2).reshape(27, 4, -1)
+    Fg = F0.reshape(27, 9, -1)
+    assert np.array_equal(Fl[:, 0], Fg[:, 8]) and np.array_equal(Fl[:, 1:3], Fg[:, 0:2])
+    sc = lb.make_desc(lb.D2Q9, lb.SHANCHEN, lb.F32, (16, 16), omega=1.0, sc_G=-5.0)
+    with pytest.raises(ValueError):
+        local_problem(sc, None, 0, 8)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("parts", [1, 2, 3])
+def test_slabset_of_oracles_equals_undivided_oracle(case, parts):
+    d, m, F0 = CASES[case]()
+    ref = O.run(oracle_problem(d, m), np.array(F0, dtype=np.float64), 12, dtype=np.float64, threads=1)[0]
+    s = SlabSet(d, m, F0, parts, lattice_factory=OracleStepper)
+    s.step(12)
+    assert np.array_equal(s.gather_populations(), ref)
+    assert np.allclose(s.sums(), O.sums(oracle_problem(d, m), ref), rtol=1e-12, atol=1e-12)
+
+
+def _free_port():
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def _gloo_body(rank, world, port, case, out_dir):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        d, m, F0 = CASES[case]()
+        slab = Slab(d, m, F0, rank, world, lattice_factory=OracleStepper)
+        slab.step(9)
+        F = slab.gather_populations()
+        sums = slab.sums()
+        if rank == 0:
+            np.save(Path(out_dir) / "F.npy", F)
+            (Path(out_dir) / "sums.json").write_text(json.dumps(list(map(float, sums))))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case,world", [("mrt_cavity3d", 2), ("channel2d", 3)])
+def test_slab_gloo_ranks_equal_undivided_oracle(tmp_path, case, world):
+    mp.start_processes(_gloo_body, args=(world, _free_port(), case, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    d, m, F0 = CASES[case]()
+    ref = O.run(oracle_problem(d, m), np.array(F0, dtype=np.float64), 9, dtype=np.float64, threads=1)[0]
+    assert np.array_equal(np.load(tmp_path / "F.npy"), ref)
+    sums = json.loads((tmp_path / "sums.json").read_text())
+    assert np.allclose(sums, O.sums(oracle_problem(d, m), ref), rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S])
+@pytest.mark.parametrize("case", ["mrt_cavity3d", "channel2d", "periodic3d", "mrt_rows"])
+@pytest.mark.parametrize("parts", [2, 3])
+def test_slabset_of_engine_lattices_equals_one_lattice(storage, case, parts):
+    """Slabs stepped by the engine (its kernel choice per slab: plain or row pipeline) and exchanged
+    by face_get/face_set: bit-identical to one lattice of the full size."""
+    if case == "mrt_rows":
+        d, m, F0 = mrt_cavity3d(storage, n=(128, 16, 24))  # row-pipeline eligible slabs
+    else:
+        d, m, F0 = CASES[case](storage)
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(np.asarray(F0, dtype=np.float64))
+        lat.step(15)
+        ref = lat.get_populations(np.float32)
+    s = SlabSet(d, m, F0, parts)
+    try:
+        s.step(15)
+        got = s.gather_populations(np.float32)
+    finally:
+        s.close()
+    assert np.isfinite(got).all() and np.array_equal(got, ref)
