@@ -97,6 +97,9 @@ constexpr unsigned long long pack_c(bool z) {
 #ifndef LBM_ROWPIPE_THREADS
 #define LBM_ROWPIPE_THREADS 256  // consumer threads per row set at most
 #endif
+#ifndef LBM_ROWPIPE_CWARPS3
+#define LBM_ROWPIPE_CWARPS3 0
+#endif
 #ifndef LBM_ROWPIPE_CR
 #define LBM_ROWPIPE_CR 0  // consumer row sets per CTA; 0 = per lattice and storage type
 #endif
@@ -141,7 +144,9 @@ struct RowPipeShape {
     static constexpr int CRQ = LBM_ROWPIPE_CR > 0 ? LBM_ROWPIPE_CR : (k3 ? 2 : 1);
     static constexpr int CR0 = CRQ * THREADS > 512 ? 512 / THREADS : CRQ;
     static constexpr int CR = CR0 < 1 ? 1 : CR0;
-    static constexpr int CONSUMERS = CR * THREADS;
+    // D3Q27 consumer warps (0: CR row sets of THREADS): the register file holds 5 warps of 96
+    // registers per SM sub-partition, i.e. up to 19 consumer warps beside the producer
+    static constexpr int CONSUMERS = k3 && LBM_ROWPIPE_CWARPS3 > 0 ? LBM_ROWPIPE_CWARPS3 * 32 : CR * THREADS;
     // CTAs per SM: D3Q27 collisions need ~90-120 registers per thread, D2Q9 far fewer; fewer CTAs
     // where two stages of one row would not fit into a CTA's share of shared memory
     static constexpr int limit_of(int ctas) { return (ctas <= 1 ? 224 : ctas == 2 ? 112 : 74) * 1024; }
@@ -256,7 +261,6 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     constexpr int Q = L::Q;
     constexpr int NS = Sh::NS;
     constexpr int SB = Sh::SB;
-    constexpr int CR = Sh::CR;
     constexpr int W = Sh::CONSUMERS / 32;  // consumer warps
     static_assert(NS <= 8, "barriers occupy the first 128 bytes");
     constexpr unsigned long long kCy = pack_c<L>(false), kCz = pack_c<L>(true);
@@ -324,9 +328,12 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         return;
     }
 
-    const int tx = tid % Sh::THREADS, rset = tid / Sh::THREADS;
     R sc, isc;
     storage_scale<S>(p, sc, isc);
+    // cells of a group flattened (row b, column x; staged index b * nx + x), CONSUMERS apart and
+    // continued across stages: the cells one stage leaves over go to other threads in the next
+    const int cq = Sh::CONSUMERS / nx, cr = Sh::CONSUMERS - cq * nx;
+    int b = tid / nx, x = tid - b * nx;
     for (unsigned k = 0; first + k * stride < groups; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
@@ -339,17 +346,21 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         }
         const int y0 = (int)(g % ugy) * B, z = (int)(g / ugy);
         const int nb = ny - y0 < B ? ny - y0 : B;
+        const S* st0 = in + (long long)s * Q * SB;
+        const uint8_t* ms0 = has_mask ? mask_st + s * SB : nullptr;
+        S* out0 = static_cast<S*>(p.fout) + ((long long)z * ny + y0) * nx;
 #pragma unroll 1
-        for (int b = rset; b < nb; b += CR) {
-            const S* st = in + (long long)s * Q * SB + b * nx;
-            const uint8_t* mrow = has_mask ? mask_st + s * SB + b * nx : nullptr;
-            S* orow = static_cast<S*>(p.fout) + ((long long)z * ny + y0 + b) * nx;
-#pragma unroll 1
-            for (int xx = 0; xx < Sh::XPT; ++xx) {
-                const int x = tx + xx * Sh::THREADS;
-                if (x < nx) row_cell_wrap<L, S, SB, COLL>(p, st, mrow, x, nx, sc, isc, orow);
+        while (b < nb) {
+            row_cell_wrap<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, x, nx, sc, isc,
+                                          out0 + (long long)b * nx);
+            x += cr;
+            b += cq;
+            if (x >= nx) {
+                x -= nx;
+                ++b;
             }
         }
+        b -= nb;
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
     }

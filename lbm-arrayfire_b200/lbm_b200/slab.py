@@ -29,9 +29,6 @@ from . import (BGK, BOUNCE, D3Q27, MAX_CLASSES, MRT, SET_RHO, SET_UX, SET_UY, SE
 
 __all__ = ["split_planes", "axis_dirs", "local_problem", "scatter_populations", "Slab", "SlabSet"]
 
-_TORCH_WORD = {4: "float32", 8: "float64", 2: "int16"}
-
-
 def split_planes(n: int, world: int):
     """[(p0, p1)] per rank: n planes in `world` contiguous runs whose sizes differ by at most one."""
     if world < 1 or n < world:
@@ -120,9 +117,10 @@ class Slab:
         if self.device.type == "cuda":
             # one stream for the steps, the face copies and the NCCL transfers: ordered without events
             self.lat.set_stream(torch.cuda.current_stream(self.device).cuda_stream)
-        word = getattr(torch, _TORCH_WORD[STORAGE_BYTES[self.desc.storage]]) \
-            if lattice_factory is None else torch.float64
+        # faces travel as raw bytes of the stored words (NCCL has no 16-bit integer type; a
+        # point-to-point transfer never touches the values); an injected stepper uses FP64 words
         k = len(self.up_dirs) * self.lat.face_cells()
+        word, k = (torch.uint8, k * STORAGE_BYTES[self.desc.storage]) if lattice_factory is None else (torch.float64, k)
         self._buf = {name: torch.empty(k, dtype=word, device=self.device)
                      for name in ("send_up", "send_down", "recv_down", "recv_up")}
         if F0 is None:
@@ -165,6 +163,8 @@ class Slab:
 
     def gather_populations(self, dtype=np.float64):
         """Global populations (flat [x, y(, z), i]) on every rank (all_gather_object: for checks)."""
+        if self.world == 1:
+            return self.interior_populations(dtype).ravel()
         parts = [None] * self.world
         self.dist.all_gather_object(parts, self.interior_populations(dtype), group=self.group)
         return np.concatenate(parts, axis=1).ravel()

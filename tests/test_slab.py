@@ -178,3 +178,25 @@ def test_slabset_of_engine_lattices_equals_one_lattice(storage, case, parts):
     finally:
         s.close()
     assert np.isfinite(got).all() and np.array_equal(got, ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [lb.F32, lb.BF16S])
+def test_one_rank_slab_on_the_gpu_equals_one_lattice(storage):
+    """The rank-side Slab with CUDA byte buffers on torch's stream: with one rank its ghost planes are
+    filled from its own far planes (the periodic wrap), so it equals the undivided lattice."""
+    import torch
+
+    d, m, F0 = mrt_cavity3d(storage, n=(128, 16, 12))
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(np.asarray(F0, dtype=np.float64))
+        lat.step(10)
+        ref = lat.get_populations(np.float32)
+        ref_sums = lat.sums()
+    slab = Slab(d, m, F0, 0, 1, device="cuda:0")
+    assert slab._buf["send_up"].dtype == torch.uint8 and slab._buf["send_up"].is_cuda
+    slab.step(10)
+    torch.cuda.synchronize()
+    assert np.array_equal(slab.gather_populations(np.float32), ref)
+    # lbm_sums_fp64 decodes each population in FP32 before its FP64 sum; Slab.sums decodes in FP64
+    assert np.allclose(slab.sums(), ref_sums, rtol=1e-6, atol=1e-6)
