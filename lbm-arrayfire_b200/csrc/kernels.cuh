@@ -432,6 +432,24 @@ __global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepPa
 
 // ---- Shan-Chen (D2Q9) --------------------------------------------------------------------
 // Pass 1: psi = 1 - exp(-rho) of the streamed density of every cell.
+// psi = 1 - exp(-rho) of the streamed density of one cell (the pseudopotential of the Shan-Chen
+// force); also returns the cell's pulled populations and class, which the collision reuses.
+template <class S, bool ABS, class R>
+__device__ __forceinline__ R sc_psi_of(const StepParams<R>& p, const S* __restrict__ fin, const Rows<D2Q9>& rows,
+                                       int x, long long c, R (&v)[9], int& cls, uint32_t& fl) {
+    using L = D2Q9;
+    pull<L, S, ABS>(fin, p, rows, x, v);
+    cell_class(p.mask, p.cls, c, cls, fl);
+    if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+    R sc, isc;
+    storage_scale<S>(p, sc, isc);
+    R sum = R(0);
+    static_for<9>([&](auto I) { sum += v[I]; });
+    R rho = ABS ? sum : R(1) + sum * isc;
+    if (fl & kSetRho) rho = R(p.cls.rho[cls]);
+    return R(1) - exp(-rho);
+}
+
 template <class S, bool ABS>
 __global__ void __launch_bounds__(512) k_sc_psi(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D2Q9;
@@ -441,70 +459,58 @@ __global__ void __launch_bounds__(512) k_sc_psi(const __grid_constant__ StepPara
     const int y = blockIdx.y, z = blockIdx.z;
     const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
     const long long c = rows.base[1][1] + x;
-    const S* __restrict__ fin = static_cast<const S*>(p.fin);
     R v[9];
-    pull<L, S, ABS>(fin, p, rows, x, v);
     int cls;
     uint32_t fl;
-    cell_class(p.mask, p.cls, c, cls, fl);
-    if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
-    R sc, isc;
-    storage_scale<S>(p, sc, isc);
-    R sum = R(0);
-    static_for<9>([&](auto I) { sum += v[I]; });
-    R rho = ABS ? sum : R(1) + sum * isc;
-    if (fl & kSetRho) rho = R(p.cls.rho[cls]);
-    p.psi[c] = R(1) - exp(-rho);
+    p.psi[c] = sc_psi_of<S, ABS>(p, static_cast<const S*>(p.fin), rows, x, c, v, cls, fl);
 }
 
-// Shan-Chen force F = -G psi(x) sum_i w_i psi(x + c_i) c_i at cell (x, y) (periodic).
-template <class R>
-__device__ __forceinline__ void sc_force(const StepParams<R>& p, const Rows<D2Q9>& rows, int x,
-                                         long long c, R& Fx, R& Fy) {
+// Shan-Chen force F = -G psi(x) sum_i w_i psi(x + c_i) c_i at one cell; psi_at(dx, dy) is psi of the
+// neighbour (x + dx, y + dy).  One summation order for every caller.
+template <class R, class PsiAt>
+__device__ __forceinline__ void sc_force_from(const StepParams<R>& p, PsiAt&& psi_at, R& Fx, R& Fy) {
     using L = D2Q9;
-    const int xm = x == 0 ? p.nx - 1 : x - 1;
-    const int xp = x == p.nx - 1 ? 0 : x + 1;
     R sx = R(0), sy = R(0);
     static_for<8>([&](auto I) {
         constexpr int i = I + 1;
         constexpr int cx = L::cx(i), cy = L::cy(i);
-        // neighbour x + c_i: the source row of the opposite direction
-        const int xn = cx == 1 ? xp : (cx == -1 ? xm : x);
-        const R v = R(L::w(i)) * __ldg(p.psi + rows.src(-cy, 0) + xn);
+        const R v = R(L::w(i)) * psi_at(cx, cy);
         if constexpr (cx == 1) sx += v;
         if constexpr (cx == -1) sx -= v;
         if constexpr (cy == 1) sy += v;
         if constexpr (cy == -1) sy -= v;
     });
-    const R g = -p.G * __ldg(p.psi + c);
+    const R g = -p.G * psi_at(0, 0);
     Fx = g * sx;
     Fy = g * sy;
 }
 
-template <class S, bool ABS>
-__global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
+// The force at cell (x, y) from the psi field in global memory (periodic).
+template <class R>
+__device__ __forceinline__ void sc_force(const StepParams<R>& p, const Rows<D2Q9>& rows, int x,
+                                         long long c, R& Fx, R& Fy) {
+    const int xm = x == 0 ? p.nx - 1 : x - 1;
+    const int xp = x == p.nx - 1 ? 0 : x + 1;
+    sc_force_from(p, [&](int dx, int dy) {
+        if (dx == 0 && dy == 0) return __ldg(p.psi + c);
+        // neighbour x + c_i: the source row of the opposite direction
+        const int xn = dx == 1 ? xp : (dx == -1 ? xm : x);
+        return __ldg(p.psi + rows.src(-dy, 0) + xn);
+    }, Fx, Fy);
+}
+
+// The Shan-Chen collision of one cell from its pulled populations v (class cls, flags fl) and the
+// force: moments, class overrides, velocity shift u_eq = u + tau F / rho (Shan & Chen 1993), BGK,
+// bounce-back, store.
+template <class S, bool ABS, class R>
+__device__ __forceinline__ void sc_collide_store(const StepParams<R>& p, long long c, const R (&v)[9], int cls,
+                                                 uint32_t fl, R Fx, R Fy) {
     using L = D2Q9;
-    using R = typename Codec<S>::Real;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= p.nx) return;
-    const int y = blockIdx.y, z = blockIdx.z;
-    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
-    const long long c = rows.base[1][1] + x;
-    const S* __restrict__ fin = static_cast<const S*>(p.fin);
-    R v[9];
-    pull<L, S, ABS>(fin, p, rows, x, v);
-    int cls;
-    uint32_t fl;
-    cell_class(p.mask, p.cls, c, cls, fl);
-    if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
     R sc, isc;
     storage_scale<S>(p, sc, isc);
     R rho, drho, ux, uy, uz;
     moments<L, ABS>(v, sc, isc, rho, drho, ux, uy, uz);
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 2);
-    R Fx, Fy;
-    sc_force(p, rows, x, c, Fx, Fy);
-    // velocity shift u_eq = u + tau F / rho (Shan & Chen 1993)
     R vx = ux, vy = uy;
     if (rho > R(0)) {
         const R k = R(1) / (p.omega * rho);
@@ -525,6 +531,101 @@ __global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepPar
         });
     }
     store_cell<L, S, ABS>(static_cast<S*>(p.fout), p, c, out);
+}
+
+// Second pass of the two-pass Shan-Chen step (psi from k_sc_psi in global memory).
+template <class S, bool ABS>
+__global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
+    using L = D2Q9;
+    using R = typename Codec<S>::Real;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= p.nx) return;
+    const int y = blockIdx.y, z = blockIdx.z;
+    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
+    const long long c = rows.base[1][1] + x;
+    const S* __restrict__ fin = static_cast<const S*>(p.fin);
+    R v[9];
+    pull<L, S, ABS>(fin, p, rows, x, v);
+    int cls;
+    uint32_t fl;
+    cell_class(p.mask, p.cls, c, cls, fl);
+    if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+    R Fx, Fy;
+    sc_force(p, rows, x, c, Fx, Fy);
+    sc_collide_store<S, ABS>(p, c, v, cls, fl, Fx, Fy);
+}
+
+// The whole Shan-Chen step in one pass.  A CTA owns a tile of kScTX x kScTY cells; every thread pulls
+// its own cell once (the populations stay in registers for the collision) and writes that cell's psi
+// into a shared (kScTX + 2) x (kScTY + 2) tile; the threads then compute psi of the tile's one-cell
+// ring (periodic wrap) from those cells' own pulls; after a block barrier the force comes from the
+// shared tile.  psi, force and collision are the two-pass kernels' device functions, so the result is
+// bit-identical; psi of the own cells is also written to global memory (the macros read it).
+#ifndef LBM_SC_TX
+#define LBM_SC_TX 32
+#endif
+#ifndef LBM_SC_TY
+#define LBM_SC_TY 16
+#endif
+constexpr int kScTX = LBM_SC_TX, kScTY = LBM_SC_TY;
+
+template <class S, bool ABS>
+__global__ void __launch_bounds__(kScTX * kScTY) k_step_sc_fused(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
+    using L = D2Q9;
+    using R = typename Codec<S>::Real;
+    constexpr int TX = kScTX, TY = kScTY, PX = TX + 2;
+    constexpr int RING = 2 * PX + 2 * TY;  // the rows above and below (PX each), the columns left and right
+    __shared__ R psi_s[(TY + 2) * PX];
+    const S* __restrict__ fin = static_cast<const S*>(p.fin);
+    const int nx = p.nx, ny = p.ny, z = blockIdx.z;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool own = x < nx && y < ny;
+    auto wrap = [](int a, int n) {
+        a %= n;
+        return a < 0 ? a + n : a;
+    };
+    R v[9];
+    int cls = 0;
+    uint32_t fl = 0;
+    {
+        // a thread past the lattice edge fills its slot with the periodic image the ring may need
+        const int xs = own ? x : wrap(x, nx), ys = own ? y : wrap(y, ny);
+        const Rows<L> rows(ys, z, nx, ny, p.nz);
+        const long long c = rows.base[1][1] + xs;
+        const R ps = sc_psi_of<S, ABS>(p, fin, rows, xs, c, v, cls, fl);
+        psi_s[(ty + 1) * PX + tx + 1] = ps;
+        if (own) p.psi[c] = ps;
+    }
+    for (int k = ty * TX + tx; k < RING; k += TX * TY) {
+        int lx, ly;
+        if (k < PX) {
+            lx = k;
+            ly = 0;
+        } else if (k < 2 * PX) {
+            lx = k - PX;
+            ly = TY + 1;
+        } else if (k < 2 * PX + TY) {
+            lx = 0;
+            ly = k - 2 * PX + 1;
+        } else {
+            lx = PX - 1;
+            ly = k - 2 * PX - TY + 1;
+        }
+        const int xr = wrap(x0 + lx - 1, nx), yr = wrap(y0 + ly - 1, ny);
+        const Rows<L> rows(yr, z, nx, ny, p.nz);
+        R w[9];
+        int c2;
+        uint32_t f2;
+        psi_s[ly * PX + lx] = sc_psi_of<S, ABS>(p, fin, rows, xr, rows.base[1][1] + xr, w, c2, f2);
+    }
+    __syncthreads();
+    if (!own) return;
+    const long long c = ((long long)z * ny + y) * nx + x;
+    R Fx, Fy;
+    sc_force_from(p, [&](int dx, int dy) { return psi_s[(ty + 1 + dy) * PX + tx + 1 + dx]; }, Fx, Fy);
+    sc_collide_store<S, ABS>(p, c, v, cls, fl, Fx, Fy);
 }
 
 // ---- macroscopic fields ------------------------------------------------------------------

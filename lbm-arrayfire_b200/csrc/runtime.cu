@@ -197,6 +197,7 @@ StepParams<double>& params_of<double>(lbm_ctx* c) {
 // multiple of 16 bytes.  Rows wider than 1024 cells go by segments (k_step_rows_seg).
 static bool rows_eligible(const lbm_ctx* c) {
     const lbm_desc& d = c->d;
+    if (d.collision == LBM_SHANCHEN) return d.lattice == LBM_D2Q9;  // the fused one-pass kernel: any shape
     const bool coll_ok = d.lattice == LBM_D3Q27 ? (d.collision == LBM_BGK || d.collision == LBM_MRT)
                                                : d.collision == LBM_BGK;
     // work items (row groups or row segments) are counted in 32 bits
@@ -304,6 +305,7 @@ static void dispatch_rows(const lbm_ctx* c, F&& f) {
 }
 
 static int prepare_rows(lbm_ctx* c) {
+    if (c->d.collision == LBM_SHANCHEN) return LBM_OK;  // k_step_sc_fused: static shared memory, grid from the shape
     int rc = LBM_OK;
     dispatch_rows(c, [&](auto lt, auto st, auto co, auto pi) {
         using L = typename decltype(lt)::type;
@@ -315,6 +317,23 @@ static int prepare_rows(lbm_ctx* c) {
 
 // Launch one time step reading buffer `from` and writing the other one.
 static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
+    if (c->kernel_used == LBM_KERNEL_ROWS && c->d.collision == LBM_SHANCHEN) {
+        const dim3 fb(kScTX, kScTY), fg((unsigned)((c->d.nx + kScTX - 1) / kScTX),
+                                        (unsigned)((c->d.ny + kScTY - 1) / kScTY), (unsigned)c->d.nz);
+        const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
+        dispatch_storage(c->d.storage, [&](auto tag) {
+            using S = typename decltype(tag)::type;
+            using R = typename Codec<S>::Real;
+            StepParams<R> p = params_of<R>(c);
+            p.fin = c->f[from];
+            p.fout = c->f[from ^ 1];
+            if (abs_arith)
+                k_step_sc_fused<S, true><<<fg, fb, 0, s>>>(p);
+            else
+                k_step_sc_fused<S, false><<<fg, fb, 0, s>>>(p);
+        });
+        return;
+    }
     if (c->kernel_used == LBM_KERNEL_ROWS) {
         dispatch_rows(c, [&](auto lt, auto st, auto co, auto pi) {
             using L = typename decltype(lt)::type;
@@ -399,7 +418,10 @@ static int autotune(lbm_ctx* c) {
         c->kernel_used = LBM_KERNEL_PLAIN;
         return LBM_OK;
     }
-    const bool try_rows = c->kernel == LBM_KERNEL_AUTO && rows_eligible(c);
+    // Shan-Chen: the one-pass kernel only when pinned (LBM_KERNEL_ROWS).  On the L2-resident 1024^2
+    // lattice it measured 41.1-41.6k vs 43.0-43.4k MLUPS for the two passes in FP32 (47.3k vs 46.1k in
+    // BF16S), while single-buffer trials here ranked it first.
+    const bool try_rows = c->kernel == LBM_KERNEL_AUTO && rows_eligible(c) && c->d.collision != LBM_SHANCHEN;
     const std::string key = tune_key(c) + (try_rows ? "/rows" : "/plain");
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
@@ -431,7 +453,9 @@ static int autotune(lbm_ctx* c) {
         LBM_CK(cudaEventCreate(&b));
         float best = 1e30f;
         const long long bytes = c->N * c->q * (long long)c->sbytes * 2;
-        const int reps = bytes > (256LL << 20) ? 2 : 6;
+        // about 2 ms of timed launches per candidate at ~5 TB/s (small, L2-resident lattices take many
+        // short launches to rank candidates a few percent apart), at least 2 and at most 50
+        const int reps = (int)std::max(2LL, std::min(50LL, 10000000000LL / std::max(1LL, bytes)));
         for (int blk : cands) {
             c->kernel_used = blk < 0 ? LBM_KERNEL_ROWS : LBM_KERNEL_PLAIN;
             launch_step(c, c->cur, c->stream, blk);

@@ -374,9 +374,45 @@ def test_row_pipeline_segmented_wide_rows_equal_plain(storage, case):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.F64])
+@pytest.mark.parametrize("arith", [lb.ARITH_ABSOLUTE, lb.ARITH_DEVIATION])
+@pytest.mark.parametrize("shape,solid", [((128, 128), False), ((100, 50), True), ((20, 10), False),
+                                         ((48, 36), True)])
+def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
+    """The one-pass Shan-Chen kernel (KERNEL_ROWS: psi of each tile and its ring recomputed in shared
+    memory) against the two-pass kernels (KERNEL_PLAIN: psi through global memory): bit-identical
+    populations and fields, on full and partial tiles, a lattice narrower than a tile, and with solid
+    (bounce-back, set-density) cells."""
+    if arith == lb.ARITH_ABSOLUTE and storage == lb.F16S:
+        pytest.skip("absolute arithmetic is F32/F64 only")
+    d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, storage, shape, omega=1.0, sc_G=-4.5, arithmetic=arith)
+    m = None
+    n = d.cells
+    if solid:
+        lb.set_classes(d, [(0, 1.0, 0.0, 0.0, 0.0), (lb.BOUNCE | lb.SET_RHO | lb.SET_UX | lb.SET_UY, 0.5, 0.0, 0.0, 0.0)])
+        xx, yy = np.meshgrid(np.arange(shape[0]), np.arange(shape[1]), indexing="ij")
+        m = ((xx - shape[0] // 3) ** 2 + (yy - shape[1] // 2) ** 2 <= (min(shape) // 5) ** 2).astype(np.uint8)
+        m = m.ravel(order="F")
+    rng = np.random.default_rng(4)
+    rho = 0.693 + 0.01 * rng.uniform(-1.0, 1.0, size=n)
+    out = {}
+    for kind in (lb.KERNEL_PLAIN, lb.KERNEL_ROWS):
+        with lb.Lattice(d, m) as lat:
+            lat.set_kernel(kind)
+            lat.init_equilibrium(rho=rho)
+            lat.step(40)
+            lat.sync()
+            assert lat.kernel() == kind
+            r, u = lat.macros()
+            out[kind] = (lat.get_populations(np.float64), r, u)
+    a, b = out[lb.KERNEL_PLAIN], out[lb.KERNEL_ROWS]
+    assert np.isfinite(b[0]).all()
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
 def test_row_pipeline_needs_eligible_shape():
     rejected = [
-        lb.make_desc(lb.D2Q9, lb.SHANCHEN, lb.F32, (128, 128), omega=1.0, sc_G=-5.0),  # two-pass model
         lb.make_desc(lb.D3Q27, lb.BGK, lb.F32, (100, 8, 8), omega=1.3),  # 100-byte mask rows
         lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (2056, 8), omega=1.3),  # segmented, but 2056 % 16 != 0
         lb.make_desc(lb.D3Q27, lb.BGK, lb.F64, (128, 8, 8), omega=1.3),  # FP64 storage
