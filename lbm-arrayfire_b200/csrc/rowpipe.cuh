@@ -112,9 +112,10 @@ constexpr unsigned long long pack_c(bool z) {
 // sets and three stages in one CTA per SM.  16-bit storage: 4 KB copies, two row sets, two stages,
 // one CTA per SM (A/B on one B200: 43.8 vs 42.6 GLUPS for MRT 256^3 and 42.0 vs 40.3 for the config-5
 // ensemble against 2 KB copies, one row set, two CTAs per SM).
-//   THREADS   consumer threads per row set (XPT = PITCH / THREADS x positions each): at most 256, so
-//             wide rows keep two CTAs (two independent stage rings) per SM where the stages fit
-//   CR        row sets: set r takes rows b = r, r + CR, ... of a group
+//   THREADS   consumer threads per row set: at most 256 (768-wide F16S BGK: 43.9 vs 39.1 GLUPS
+//             against 512)
+//   CR        row sets; CONSUMERS = CR * THREADS consumer threads walk a group's cells flattened
+//             (staged index b * nx + x), CONSUMERS apart and continued across stages
 //   B         rows per group at nx == PITCH; the host may put more rows of a narrower lattice into
 //             the same stage (runtime rows per group, at most B * PITCH / nx)
 //   NS        stages
