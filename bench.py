@@ -328,7 +328,7 @@ def build_workload(lb, args, storage):
     fn = WORKLOADS[args.workload][0]
     if args.dims and (args.workload.startswith("d3q27") or args.workload == "d2q9_shanchen_1024"):
         return fn(lb, storage, tuple(int(v) for v in args.dims.lower().split("x")))
-    if args.size and args.workload.startswith("d3q27"):
+    if args.size and (args.workload.startswith("d3q27") or args.workload == "d2q9_lid_8192"):
         return fn(lb, storage, args.size)
     return fn(lb, storage)
 
@@ -664,7 +664,8 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=150.0, help="time budget of the reference arm")
-    ap.add_argument("--size", type=int, default=0, help="cube side for D3Q27 workloads (default: the config's)")
+    ap.add_argument("--size", type=int, default=0,
+                    help="cube side for D3Q27 workloads, square side for d2q9_lid_8192 (default: the config's)")
     ap.add_argument("--dims", default="", help="NXxNYxNZ for D3Q27 workloads, NXxNY for the Shan-Chen one")
     ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "rows"], help="step-kernel family")
     ap.add_argument("--block", type=int, default=0, help="fixed block width (default: autotune)")

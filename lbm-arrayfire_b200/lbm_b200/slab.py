@@ -169,6 +169,11 @@ class Slab:
         self.dist.all_gather_object(parts, self.interior_populations(dtype), group=self.group)
         return np.concatenate(parts, axis=1).ravel()
 
+    def close(self):
+        """Release the slab's lattice (its device buffers)."""
+        if hasattr(self.lat, "close"):
+            self.lat.close()
+
     def sums(self) -> np.ndarray:
         """FP64 mass and momentum of the whole lattice (a sum over ranks)."""
         import torch

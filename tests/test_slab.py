@@ -200,3 +200,4 @@ def test_one_rank_slab_on_the_gpu_equals_one_lattice(storage):
     assert np.array_equal(slab.gather_populations(np.float32), ref)
     # lbm_sums_fp64 decodes each population in FP32 before its FP64 sum; Slab.sums decodes in FP64
     assert np.allclose(slab.sums(), ref_sums, rtol=1e-6, atol=1e-6)
+    slab.close()
