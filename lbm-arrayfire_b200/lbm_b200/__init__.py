@@ -363,10 +363,12 @@ class Lattice:
         dirs = [int(i) for i in dirs]
         want = len(dirs) * self.face_cells() * STORAGE_BYTES[self.desc.storage]
         if hasattr(buf, "data_ptr"):
+            if not buf.is_contiguous():
+                raise ValueError("face buffer must be contiguous")
             got, ptr, mem = buf.numel() * buf.element_size(), _torch_ptr(buf), DEVICE if buf.is_cuda else HOST
-            assert buf.is_contiguous()
         else:
-            assert buf.flags["C_CONTIGUOUS"]
+            if not buf.flags["C_CONTIGUOUS"]:
+                raise ValueError("face buffer must be contiguous")
             got, ptr, mem = buf.nbytes, _ptr(buf), HOST
         if got != want:
             raise ValueError(f"face buffer holds {got} bytes, {want} needed")

@@ -106,6 +106,8 @@ class Slab:
         import torch
         import torch.distributed as dist
 
+        if F0 is None:
+            raise ValueError("F0 (global start populations) is required")
         self.dist, self.group, self.rank, self.world = dist, group, rank, world
         self.global_desc = desc
         self.p0, self.p1 = split_planes(_planes(desc), world)[rank]
@@ -123,8 +125,6 @@ class Slab:
         word, k = (torch.uint8, k * STORAGE_BYTES[self.desc.storage]) if lattice_factory is None else (torch.float64, k)
         self._buf = {name: torch.empty(k, dtype=word, device=self.device)
                      for name in ("send_up", "send_down", "recv_down", "recv_up")}
-        if F0 is None:
-            raise ValueError("F0 (global start populations) is required")
         self.lat.set_populations(scatter_populations(desc, F0, self.p0, self.p1))
 
     def _pack(self):

@@ -109,6 +109,26 @@ def test_local_problem_ghost_planes_and_rejects_shanchen():
         local_problem(sc, None, 0, 8)
 
 
+def test_face_calls_validate_buffers_and_context():
+    """Face buffers are checked on the host (size, contiguity) and the C ABI rejects a NULL context;
+    nothing here reaches a GPU."""
+    import ctypes as C
+
+    class Unopened(lb.Lattice):
+        def __init__(self, d):  # no lbm_create: a NULL context
+            self.desc, self._h, self._mask = d, C.c_void_p(), None
+
+    d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F16S, (32, 8))
+    lat = Unopened(d)
+    with pytest.raises(ValueError):
+        lat.face_get(0, [2, 5, 6], np.empty(10, np.uint16))
+    with pytest.raises(ValueError):
+        lat.face_get(0, [2, 5, 6], np.empty((192, 2), np.uint16)[:, 0])
+    with pytest.raises(lb.LbmError):
+        lat.face_get(0, [2, 5, 6], np.empty(96, np.uint16))
+    lat._h = None
+
+
 @pytest.mark.parametrize("case", sorted(CASES))
 @pytest.mark.parametrize("parts", [1, 2, 3])
 def test_slabset_of_oracles_equals_undivided_oracle(case, parts):
