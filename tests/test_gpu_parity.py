@@ -3,7 +3,7 @@ fixtures.
 
 Two arithmetic modes are checked:
 * ABSOLUTE (the reference's arithmetic on the populations): FP32 engine vs FP32 oracle <= 1e-5
-  relative L2 — the north-star bound against the reference's FP32 results;
+  relative L2 — the stated tolerance against the reference's FP32 results;
 * DEVIATION (default, arithmetic on f - w): FP32 engine vs FP64 oracle <= 1e-5, and at least as
   close to the FP64 result as the FP32 restatement of the reference.
 F64 storage (either mode) vs FP64 oracle <= 1e-12; 16-bit shifted storage vs the FP64 engine run
