@@ -70,6 +70,28 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (clock64() - t0 > limit) return false;
     return true;
 }
+// The producer's wait for a consumed stage: SLEEP_NS = 0 the hinted wait; > 0 unhinted polls with a
+// fixed sleep between them (bounded by the same clock limit).
+template <int SLEEP_NS>
+__device__ __forceinline__ bool mbar_wait_producer(uint64_t* bar, uint32_t parity, long long limit = 1LL << 32) {
+    if constexpr (SLEEP_NS > 0) {
+        const long long t0 = clock64();
+        while (true) {
+            uint32_t done;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(smem_addr(bar)), "r"(parity)
+                : "memory");
+            if (done) return true;
+            if (clock64() - t0 > limit) return false;
+            __nanosleep(SLEEP_NS);
+        }
+    }
+    return mbar_wait_bounded(bar, parity, limit);
+}
 __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src_gmem, uint32_t bytes, uint64_t* bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_addr(dst_smem)),
@@ -137,6 +159,10 @@ struct RowPipeShape {
     static constexpr int THREADS = PITCH > LBM_ROWPIPE_THREADS ? LBM_ROWPIPE_THREADS : PITCH;
     static constexpr int XPT = PITCH / THREADS;
     static constexpr int kRowBytes = PITCH * (int)sizeof(S);
+    // the producer's wait for consumed stages: D3Q27 FP32 (memory-bound) polls unhinted every 512 ns
+    // (A/B, MRT 256^3: 29.35 vs 28.6 GLUPS, twice on one box; 16-bit storage and D2Q9 unchanged or
+    // 1 % slower, so they keep the hinted wait)
+    static constexpr int PRODUCER_SLEEP = k3 && !k16 ? 512 : 0;
     // D2Q9 (A/B, 1024 x 16384): one row set and 2 KB groups, i.e. more and smaller stages per SM
     // (FP32 85.1 vs 78.3 GLUPS against the D3Q27 shape)
     static constexpr int kGroupBytes =
@@ -320,7 +346,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
             if (first + s * stride < groups) issue(first + s * stride, s);
         for (unsigned k = 0; first + (k + NS) * stride < groups; ++k) {
             const int s = (int)(k % NS);
-            if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1))) {
+            if (!mbar_wait_producer<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1))) {
                 if (lane == 0) atomicExch(err, kRowPipeTimeout);
                 return;
             }
@@ -449,7 +475,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
             if (first + s * stride < groups) issue(first + s * stride, s);
         for (unsigned k = 0; first + (k + NS) * stride < groups; ++k) {
             const int s = (int)(k % NS);
-            if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1))) {
+            if (!mbar_wait_producer<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1))) {
                 if (lane == 0) atomicExch(err, kRowPipeTimeout);
                 return;
             }
