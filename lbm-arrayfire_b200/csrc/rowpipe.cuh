@@ -70,10 +70,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (clock64() - t0 > limit) return false;
     return true;
 }
-// The producer's wait for a consumed stage: SLEEP_NS = 0 the hinted wait; > 0 unhinted polls with a
-// fixed sleep between them (bounded by the same clock limit).
+// A bounded wait with a chosen polling: SLEEP_NS = 0 the hinted wait; > 0 unhinted polls with a fixed
+// sleep between them (bounded by the same clock limit).
 template <int SLEEP_NS>
-__device__ __forceinline__ bool mbar_wait_producer(uint64_t* bar, uint32_t parity, long long limit = 1LL << 32) {
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, long long limit = 1LL << 32) {
     if constexpr (SLEEP_NS > 0) {
         const long long t0 = clock64();
         while (true) {
@@ -119,6 +119,9 @@ constexpr unsigned long long pack_c(bool z) {
 #ifndef LBM_ROWPIPE_THREADS
 #define LBM_ROWPIPE_THREADS 256  // consumer threads per row set at most
 #endif
+#ifndef LBM_ROWPIPE_CONSUMER_SLEEP
+#define LBM_ROWPIPE_CONSUMER_SLEEP 0
+#endif
 #ifndef LBM_ROWPIPE_CWARPS3
 #define LBM_ROWPIPE_CWARPS3 0
 #endif
@@ -159,10 +162,12 @@ struct RowPipeShape {
     static constexpr int THREADS = PITCH > LBM_ROWPIPE_THREADS ? LBM_ROWPIPE_THREADS : PITCH;
     static constexpr int XPT = PITCH / THREADS;
     static constexpr int kRowBytes = PITCH * (int)sizeof(S);
-    // the producer's wait for consumed stages: D3Q27 FP32 (memory-bound) polls unhinted every 512 ns
-    // (A/B, MRT 256^3: 29.35 vs 28.6 GLUPS, twice on one box; 16-bit storage and D2Q9 unchanged or
-    // 1 % slower, so they keep the hinted wait)
+    // the waits for stages: D3Q27 FP32 (memory-bound, often under the power cap) polls unhinted, the
+    // producer every 512 ns and the consumers every 256 ns (A/B, MRT 256^3 GLUPS: 28.6 hinted, 29.35
+    // with the producer's sleep, 29.6 with both); 16-bit storage and D2Q9 were unchanged or 1 % slower
+    // and keep the hinted wait
     static constexpr int PRODUCER_SLEEP = k3 && !k16 ? 512 : 0;
+    static constexpr int CONSUMER_SLEEP = LBM_ROWPIPE_CONSUMER_SLEEP > 0 ? LBM_ROWPIPE_CONSUMER_SLEEP : (k3 && !k16 ? 256 : 0);
     // D2Q9 (A/B, 1024 x 16384): one row set and 2 KB groups, i.e. more and smaller stages per SM
     // (FP32 85.1 vs 78.3 GLUPS against the D3Q27 shape)
     static constexpr int kGroupBytes =
@@ -346,7 +351,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
             if (first + s * stride < groups) issue(first + s * stride, s);
         for (unsigned k = 0; first + (k + NS) * stride < groups; ++k) {
             const int s = (int)(k % NS);
-            if (!mbar_wait_producer<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1))) {
+            if (!mbar_wait_sleep<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1))) {
                 if (lane == 0) atomicExch(err, kRowPipeTimeout);
                 return;
             }
@@ -364,7 +369,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     for (unsigned k = 0; first + k * stride < groups; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
-        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1))) {
+        if (!mbar_wait_sleep<Sh::CONSUMER_SLEEP>(&full[s], (uint32_t)((k / NS) & 1))) {
             if (lane == 0) atomicExch(err, kRowPipeTimeout);
             // wait, briefly and bounded, for copies that may still land in this CTA's stages
             for (int j = 1; j < NS && first + (k + j) * stride < groups; ++j)
@@ -475,7 +480,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
             if (first + s * stride < groups) issue(first + s * stride, s);
         for (unsigned k = 0; first + (k + NS) * stride < groups; ++k) {
             const int s = (int)(k % NS);
-            if (!mbar_wait_producer<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1))) {
+            if (!mbar_wait_sleep<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1))) {
                 if (lane == 0) atomicExch(err, kRowPipeTimeout);
                 return;
             }
@@ -488,7 +493,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
     for (unsigned k = 0; first + k * stride < groups; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
-        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1))) {
+        if (!mbar_wait_sleep<Sh::CONSUMER_SLEEP>(&full[s], (uint32_t)((k / NS) & 1))) {
             if (lane == 0) atomicExch(err, kRowPipeTimeout);
             for (int j = 1; j < NS && first + (k + j) * stride < groups; ++j)
                 if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1), 1LL << 28)) break;
