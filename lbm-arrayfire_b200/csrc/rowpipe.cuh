@@ -120,7 +120,10 @@ constexpr unsigned long long pack_c(bool z) {
 #define LBM_ROWPIPE_THREADS 256  // consumer threads per row set at most
 #endif
 #ifndef LBM_ROWPIPE_CONSUMER_SLEEP
-#define LBM_ROWPIPE_CONSUMER_SLEEP 0
+#define LBM_ROWPIPE_CONSUMER_SLEEP 0  // > 0: overrides the consumers' polling sleep (ns) of every shape
+#endif
+#ifndef LBM_ROWPIPE_PRODUCER_SLEEP
+#define LBM_ROWPIPE_PRODUCER_SLEEP 0  // > 0: overrides the producer's polling sleep (ns) of every shape
 #endif
 #ifndef LBM_ROWPIPE_CWARPS3
 #define LBM_ROWPIPE_CWARPS3 0
@@ -166,7 +169,7 @@ struct RowPipeShape {
     // producer every 512 ns and the consumers every 256 ns (A/B, MRT 256^3 GLUPS: 28.6 hinted, 29.35
     // with the producer's sleep, 29.6 with both); 16-bit storage and D2Q9 were unchanged or 1 % slower
     // and keep the hinted wait
-    static constexpr int PRODUCER_SLEEP = k3 && !k16 ? 512 : 0;
+    static constexpr int PRODUCER_SLEEP = LBM_ROWPIPE_PRODUCER_SLEEP > 0 ? LBM_ROWPIPE_PRODUCER_SLEEP : (k3 && !k16 ? 512 : 0);
     static constexpr int CONSUMER_SLEEP = LBM_ROWPIPE_CONSUMER_SLEEP > 0 ? LBM_ROWPIPE_CONSUMER_SLEEP : (k3 && !k16 ? 256 : 0);
     // D2Q9 (A/B, 1024 x 16384): one row set and 2 KB groups, i.e. more and smaller stages per SM
     // (FP32 85.1 vs 78.3 GLUPS against the D3Q27 shape)
