@@ -163,7 +163,6 @@ struct RowPipeShape {
     // D2Q9 8192^2 F16S: 1008 134.6, 896 133.4
     static constexpr int SEGW_RUN = k3 ? 896 : SEGW;
     static constexpr int THREADS = PITCH > LBM_ROWPIPE_THREADS ? LBM_ROWPIPE_THREADS : PITCH;
-    static constexpr int XPT = PITCH / THREADS;
     static constexpr int kRowBytes = PITCH * (int)sizeof(S);
     // the waits for stages: D3Q27 FP32 (memory-bound, often under the power cap) polls unhinted, the
     // producer every 512 ns and the consumers every 256 ns (A/B, MRT 256^3 GLUPS: 28.6 hinted, 29.35
