@@ -125,6 +125,9 @@ constexpr unsigned long long pack_c(bool z) {
 #ifndef LBM_ROWPIPE_PRODUCER_SLEEP
 #define LBM_ROWPIPE_PRODUCER_SLEEP 0  // > 0: overrides the producer's polling sleep (ns) of every shape
 #endif
+#ifndef LBM_ROWPIPE_CWARPS2
+#define LBM_ROWPIPE_CWARPS2 0  // D2Q9 consumer warps (0: CR row sets of THREADS), for A/B
+#endif
 #ifndef LBM_ROWPIPE_CWARPS3
 #define LBM_ROWPIPE_CWARPS3 0
 #endif
@@ -180,7 +183,9 @@ struct RowPipeShape {
     static constexpr int CR = CR0 < 1 ? 1 : CR0;
     // D3Q27 consumer warps (0: CR row sets of THREADS): the register file holds 5 warps of 96
     // registers per SM sub-partition, i.e. up to 19 consumer warps beside the producer
-    static constexpr int CONSUMERS = k3 && LBM_ROWPIPE_CWARPS3 > 0 ? LBM_ROWPIPE_CWARPS3 * 32 : CR * THREADS;
+    static constexpr int CONSUMERS = k3 && LBM_ROWPIPE_CWARPS3 > 0    ? LBM_ROWPIPE_CWARPS3 * 32
+                                     : !k3 && LBM_ROWPIPE_CWARPS2 > 0 ? LBM_ROWPIPE_CWARPS2 * 32
+                                                                       : CR * THREADS;
     // CTAs per SM: D3Q27 collisions need ~90-120 registers per thread, D2Q9 far fewer; fewer CTAs
     // where two stages of one row would not fit into a CTA's share of shared memory
     static constexpr int limit_of(int ctas) { return (ctas <= 1 ? 224 : ctas == 2 ? 112 : 74) * 1024; }
