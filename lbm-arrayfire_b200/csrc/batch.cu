@@ -94,9 +94,10 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     CT* cls_st = reinterpret_cast<CT*>(smem + Sh::smem_bytes());              // [NS]
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const long long first = blockIdx.x, stride = gridDim.x;
+    // item indices in 32 bits (the host keeps the item count below 2^31)
+    const unsigned first = blockIdx.x, stride = gridDim.x, nit = (unsigned)n_items;
 
-    auto issue = [&](long long g, int s) {
+    auto issue = [&](unsigned g, int s) {
         const RowItem it = items[g];
         const BatchLattice<R>& m = lats[it.lat];
         const int nx = m.nx, ny = m.ny, nz = m.nz, nb = it.nb;
@@ -133,8 +134,8 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     __syncthreads();
     if (tid >= CONS) {  // producer warp
         for (int s = 0; s < NS; ++s)
-            if (first + s * stride < n_items) issue(first + s * stride, s);
-        for (long long k = 0; first + (k + NS) * stride < n_items; ++k) {
+            if (first + s * stride < nit) issue(first + s * stride, s);
+        for (unsigned k = 0; first + (k + NS) * stride < nit; ++k) {
             const int s = (int)(k % NS);
             if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1))) {
                 if (lane == 0) atomicExch(err, kRowPipeTimeout);
@@ -144,12 +145,12 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         }
         return;
     }
-    for (long long k = 0; first + k * stride < n_items; ++k) {
-        const long long g = first + k * stride;
+    for (unsigned k = 0; first + k * stride < nit; ++k) {
+        const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
         if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1))) {
             if (lane == 0) atomicExch(err, kRowPipeTimeout);
-            for (int j = 1; j < NS && first + (k + j) * stride < n_items; ++j)
+            for (unsigned j = 1; j < NS && first + (k + j) * stride < nit; ++j)
                 if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1), 1LL << 28)) break;
             return;
         }
@@ -162,14 +163,20 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         const S* st = in + (long long)s * Q * SB;
         const uint8_t* ms = m.mask ? mask_st + s * SB : nullptr;
         S* out0 = static_cast<S*>(m.f[parity ^ 1]) + ((long long)it.z * m.ny + it.y0) * nx;
-        // cells of the group, flattened (row b, column x), CONS apart
-        int b = tid / nx, x = tid - b * nx;
+        // cells of the group, flattened (row b, column x), CONS apart.  tid / nx and CONS / nx by a
+        // float reciprocal: exact here (numerators below 2^11, nx <= 1024: the quotient's distance to
+        // the next integer, at least 1/(2 nx), is far above the rounding error)
+        const float inv_nx = __frcp_rn((float)nx);
+        int b = (int)(((float)tid + 0.5f) * inv_nx), x = tid - b * nx;
+        const int cq = (int)(((float)CONS + 0.5f) * inv_nx), cr = CONS - cq * nx;
+        const int nb = it.nb;
 #pragma unroll 1
-        for (int c = tid; c < it.nb * nx; c += CONS) {
+        while (b < nb) {
             row_cell_wrap<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
                                        out0 + (long long)b * nx);
-            x += CONS;
-            while (x >= nx) {
+            x += cr;
+            b += cq;
+            if (x >= nx) {
                 x -= nx;
                 ++b;
             }
@@ -304,6 +311,7 @@ static int batch_build_rows(lbm_batch* b) {
             b->rows_grid[fam] = (int)std::min<long long>((long long)items.size(), (long long)per_sm * sms);
         });
         if (rc) return rc;
+        if (items.size() >= (1ull << 31)) return set_error(LBM_ERR_UNSUPPORTED, "row work table over 2^31 items");
         if (b->items_d[fam]) cudaFree(b->items_d[fam]);
         b->items_d[fam] = nullptr;
         b->n_items[fam] = (long long)items.size();
