@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     constexpr int CONS = Sh::CONSUMERS;
     constexpr int W = CONS / 32;
     static_assert(NS <= 8, "barriers occupy the first 128 bytes");
+    static_assert(CONS + 32 <= 2048 && PITCH <= 1024, "the reciprocal quotients below need numerators < 2^11, nx <= 1024");
     constexpr unsigned long long kCy = pack_c<L>(false), kCz = pack_c<L>(true);
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
