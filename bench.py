@@ -611,7 +611,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_kind == "measured" else "fallback 6.65 TB/s",
-                     "kernel": ("k_step_sc_fused" if d.collision == 2 else "k_step_rows") if kernel_family == "rows"
+                     "kernel": ("k_step_sc_window" if d.collision == 2 else "k_step_rows") if kernel_family == "rows"
                      else {0: "k_step_bgk", 1: "k_step_mrt", 2: "k_step_sc + k_sc_psi"}[d.collision],
                      "bytes_per_launch": bytes_cell * N / launches_per_step},
         "gpu_launches": args.steps * launches_per_step,

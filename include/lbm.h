@@ -178,9 +178,9 @@ int   lbm_get_block(const lbm_ctx* c);
  * (D3Q27 BGK/MRT or D2Q9 BGK, deviation arithmetic, F32/F16S/BF16S, nx >= 32 a multiple of 16):
  * groups of whole rows (segments of rows wider than 1024 cells) staged in shared memory by bulk
  * copies (TMA) through an mbarrier ring; for D2Q9 Shan-Chen (any shape and storage) the one-pass
- * tile kernel (psi of each tile and its one-cell ring recomputed in shared memory) instead of the two
- * passes of PLAIN.  AUTO (default): the autotuner times the eligible ones (Shan-Chen: the two passes
- * only; its one-pass kernel runs when pinned).  Both give bit-identical results.                   */
+ * kernel (a window sliding down y: psi of the next row into a shared ring, the force from it) instead
+ * of the two passes of PLAIN.  AUTO (default): the autotuner times the eligible ones.  Both give
+ * bit-identical results.                                                                            */
 enum lbm_kernel { LBM_KERNEL_AUTO = 0, LBM_KERNEL_PLAIN = 1, LBM_KERNEL_ROWS = 2 };
 int   lbm_set_kernel(lbm_ctx* c, int kind);
 int   lbm_get_kernel(const lbm_ctx* c);              /* the family in use (PLAIN or ROWS), or AUTO before the first step */

@@ -435,12 +435,15 @@ __global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepPa
 // psi = 1 - exp(-rho) of the streamed density of one cell (the pseudopotential of the Shan-Chen
 // force); also returns the cell's pulled populations and class, which the collision reuses.
 template <class S, bool ABS, class R>
-__device__ __forceinline__ R sc_psi_of(const StepParams<R>& p, const S* __restrict__ fin, const Rows<D2Q9>& rows,
-                                       int x, long long c, R (&v)[9], int& cls, uint32_t& fl) {
+__device__ __forceinline__ void sc_pull_cell(const StepParams<R>& p, const S* __restrict__ fin, const Rows<D2Q9>& rows,
+                                             int x, long long c, R (&v)[9], int& cls, uint32_t& fl) {
     using L = D2Q9;
     pull<L, S, ABS>(fin, p, rows, x, v);
     cell_class(p.mask, p.cls, c, cls, fl);
     if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
+}
+template <class S, bool ABS, class R>
+__device__ __forceinline__ R sc_psi_from(const StepParams<R>& p, const R (&v)[9], int cls, uint32_t fl) {
     R sc, isc;
     storage_scale<S>(p, sc, isc);
     R sum = R(0);
@@ -448,6 +451,12 @@ __device__ __forceinline__ R sc_psi_of(const StepParams<R>& p, const S* __restri
     R rho = ABS ? sum : R(1) + sum * isc;
     if (fl & kSetRho) rho = R(p.cls.rho[cls]);
     return R(1) - exp(-rho);
+}
+template <class S, bool ABS, class R>
+__device__ __forceinline__ R sc_psi_of(const StepParams<R>& p, const S* __restrict__ fin, const Rows<D2Q9>& rows,
+                                       int x, long long c, R (&v)[9], int& cls, uint32_t& fl) {
+    sc_pull_cell<S, ABS>(p, fin, rows, x, c, v, cls, fl);
+    return sc_psi_from<S, ABS>(p, v, cls, fl);
 }
 
 template <class S, bool ABS>
@@ -555,77 +564,72 @@ __global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepPar
     sc_collide_store<S, ABS>(p, c, v, cls, fl, Fx, Fy);
 }
 
-// The whole Shan-Chen step in one pass.  A CTA owns a tile of kScTX x kScTY cells; every thread pulls
-// its own cell once (the populations stay in registers for the collision) and writes that cell's psi
-// into a shared (kScTX + 2) x (kScTY + 2) tile; the threads then compute psi of the tile's one-cell
-// ring (periodic wrap) from those cells' own pulls; after a block barrier the force comes from the
-// shared tile.  psi, force and collision are the two-pass kernels' device functions, so the result is
-// bit-identical; psi of the own cells is also written to global memory (the macros read it).
-#ifndef LBM_SC_TX
-#define LBM_SC_TX 32
+// The whole Shan-Chen step in one pass, as a window sliding down y.  A CTA owns a strip of kScwTX
+// columns and rows [y0, y0 + rows); thread tx owns column x0 + tx.  Per row y it pulls row y + 1 once
+// (the populations stay in registers for the next row's collision), writes psi of row y + 1 into a
+// ring of 4 shared rows (two threads add the strip's edge columns, periodic wrap), and after one
+// block barrier takes the force at row y from ring rows y - 1 .. y + 1.  With 4 ring rows one barrier
+// per row suffices: a row's slot is rewritten two barriers after its last read.  psi, force and
+// collision are the two-pass kernels' device functions: bit-identical results.
+#ifndef LBM_SCW_TX
+#define LBM_SCW_TX 128
 #endif
-#ifndef LBM_SC_TY
-#define LBM_SC_TY 16
-#endif
-constexpr int kScTX = LBM_SC_TX, kScTY = LBM_SC_TY;
+constexpr int kScwTX = LBM_SCW_TX;
 
 template <class S, bool ABS>
-__global__ void __launch_bounds__(kScTX * kScTY) k_step_sc_fused(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
+__global__ void __launch_bounds__(kScwTX) k_step_sc_window(const __grid_constant__ StepParams<typename Codec<S>::Real> p,
+                                                           int rows_per_strip) {
     using L = D2Q9;
     using R = typename Codec<S>::Real;
-    constexpr int TX = kScTX, TY = kScTY, PX = TX + 2;
-    constexpr int RING = 2 * PX + 2 * TY;  // the rows above and below (PX each), the columns left and right
-    __shared__ R psi_s[(TY + 2) * PX];
+    constexpr int TX = kScwTX, PX = TX + 2;
+    static_assert(TX >= 2, "two edge threads");
+    __shared__ R ring[4][PX];
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
-    const int nx = p.nx, ny = p.ny, z = blockIdx.z;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int x = x0 + tx, y = y0 + ty;
-    const bool own = x < nx && y < ny;
-    auto wrap = [](int a, int n) {
-        a %= n;
-        return a < 0 ? a + n : a;
-    };
-    R v[9];
-    int cls = 0;
-    uint32_t fl = 0;
-    {
-        // a thread past the lattice edge fills its slot with the periodic image the ring may need
-        const int xs = own ? x : wrap(x, nx), ys = own ? y : wrap(y, ny);
-        const Rows<L> rows(ys, z, nx, ny, p.nz);
+    const int nx = p.nx, ny = p.ny;
+    const int tx = threadIdx.x;
+    const int x0 = blockIdx.x * TX;
+    const int ys = blockIdx.y * rows_per_strip;
+    if (ys >= ny) return;  // uniform over the block
+    const int ye = ys + rows_per_strip < ny ? ys + rows_per_strip : ny;
+    const int x = x0 + tx;
+    const bool own_x = x < nx;
+    const int xs = own_x ? x : x % nx;  // past the edge: the periodic image (only its psi is used)
+    int xe = tx == 0 ? x0 - 1 : x0 + TX;  // the strip's edge columns (threads 0 and 1)
+    xe = xe < 0 ? xe + nx : xe % nx;
+    const int le = tx == 0 ? 0 : PX - 1;
+    auto psi_row = [&](int y, R (&v)[9], int& cls, uint32_t& fl) {
+        const int yw = y < 0 ? y + ny : (y >= ny ? y - ny : y);
+        const Rows<L> rows(yw, 0, nx, ny, 1);
         const long long c = rows.base[1][1] + xs;
-        const R ps = sc_psi_of<S, ABS>(p, fin, rows, xs, c, v, cls, fl);
-        psi_s[(ty + 1) * PX + tx + 1] = ps;
-        if (own) p.psi[c] = ps;
-    }
-    for (int k = ty * TX + tx; k < RING; k += TX * TY) {
-        int lx, ly;
-        if (k < PX) {
-            lx = k;
-            ly = 0;
-        } else if (k < 2 * PX) {
-            lx = k - PX;
-            ly = TY + 1;
-        } else if (k < 2 * PX + TY) {
-            lx = 0;
-            ly = k - 2 * PX + 1;
-        } else {
-            lx = PX - 1;
-            ly = k - 2 * PX - TY + 1;
-        }
-        const int xr = wrap(x0 + lx - 1, nx), yr = wrap(y0 + ly - 1, ny);
-        const Rows<L> rows(yr, z, nx, ny, p.nz);
+        sc_pull_cell<S, ABS>(p, fin, rows, xs, c, v, cls, fl);
         R w[9];
-        int c2;
-        uint32_t f2;
-        psi_s[ly * PX + lx] = sc_psi_of<S, ABS>(p, fin, rows, xr, rows.base[1][1] + xr, w, c2, f2);
+        int c2 = 0;
+        uint32_t f2 = 0;
+        if (tx < 2) sc_pull_cell<S, ABS>(p, fin, rows, xe, rows.base[1][1] + xe, w, c2, f2);
+        const R ps = sc_psi_from<S, ABS>(p, v, cls, fl);
+        ring[y & 3][tx + 1] = ps;
+        if (own_x && y >= ys && y < ye) p.psi[c] = ps;
+        if (tx < 2) ring[y & 3][le] = sc_psi_from<S, ABS>(p, w, c2, f2);
+    };
+    R vc[9], vn[9];
+    int cc = 0, cn = 0;
+    uint32_t fc = 0, fn = 0;
+    psi_row(ys - 1, vn, cn, fn);  // the row above the strip: psi only
+    psi_row(ys, vc, cc, fc);
+#pragma unroll 1
+    for (int y = ys; y < ye; ++y) {
+        psi_row(y + 1, vn, cn, fn);  // the next row (the row below the strip on the last pass)
+        __syncthreads();
+        if (own_x) {
+            const long long c = (long long)y * nx + x;
+            R Fx, Fy;
+            sc_force_from(p, [&](int dx, int dy) { return ring[(y + dy) & 3][tx + 1 + dx]; }, Fx, Fy);
+            sc_collide_store<S, ABS>(p, c, vc, cc, fc, Fx, Fy);
+        }
+        static_for<9>([&](auto I) { vc[I] = vn[I]; });
+        cc = cn;
+        fc = fn;
     }
-    __syncthreads();
-    if (!own) return;
-    const long long c = ((long long)z * ny + y) * nx + x;
-    R Fx, Fy;
-    sc_force_from(p, [&](int dx, int dy) { return psi_s[(ty + 1 + dy) * PX + tx + 1 + dx]; }, Fx, Fy);
-    sc_collide_store<S, ABS>(p, c, v, cls, fl, Fx, Fy);
 }
 
 // ---- macroscopic fields ------------------------------------------------------------------

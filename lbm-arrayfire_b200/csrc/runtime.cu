@@ -197,7 +197,7 @@ StepParams<double>& params_of<double>(lbm_ctx* c) {
 // multiple of 16 bytes.  Rows wider than 1024 cells go by segments (k_step_rows_seg).
 static bool rows_eligible(const lbm_ctx* c) {
     const lbm_desc& d = c->d;
-    if (d.collision == LBM_SHANCHEN) return d.lattice == LBM_D2Q9;  // the fused one-pass kernel: any shape
+    if (d.collision == LBM_SHANCHEN) return d.lattice == LBM_D2Q9;  // the one-pass window kernel: any shape
     const bool coll_ok = d.lattice == LBM_D3Q27 ? (d.collision == LBM_BGK || d.collision == LBM_MRT)
                                                : d.collision == LBM_BGK;
     // work items (row groups or row segments) are counted in 32 bits
@@ -304,8 +304,29 @@ static void dispatch_rows(const lbm_ctx* c, F&& f) {
         by_storage(Tag<D3Q27>{});
 }
 
+#ifndef LBM_SCW_HMAX
+#define LBM_SCW_HMAX 0  // > 0: at most this many rows per strip (several waves of CTAs on large lattices)
+#endif
 static int prepare_rows(lbm_ctx* c) {
-    if (c->d.collision == LBM_SHANCHEN) return LBM_OK;  // k_step_sc_fused: static shared memory, grid from the shape
+    if (c->d.collision == LBM_SHANCHEN) {
+        // k_step_sc_window: strips of rows sized so that one wave of CTAs covers the lattice (A/B:
+        // capping the strip height at 16/32/64 rows for several waves was slower or equal)
+        int per_sm = 0, sms = 0, rc = LBM_OK;
+        const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
+        dispatch_storage(c->d.storage, [&](auto tag) {
+            using S = typename decltype(tag)::type;
+            auto kern = abs_arith ? k_step_sc_window<S, true> : k_step_sc_window<S, false>;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kScwTX, 0) != cudaSuccess)
+                rc = set_error(LBM_ERR_CUDA, "occupancy query failed");
+        });
+        if (rc) return rc;
+        LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->d.device));
+        const long long gx = (c->d.nx + kScwTX - 1) / kScwTX;
+        const long long target = std::max(1LL, (long long)std::max(per_sm, 1) * sms);
+        const long long h = std::max<long long>(4, (c->d.ny * gx + target - 1) / target);
+        c->rows_rpg = (int)(LBM_SCW_HMAX > 0 ? std::min<long long>(h, LBM_SCW_HMAX) : h);
+        return LBM_OK;
+    }
     int rc = LBM_OK;
     dispatch_rows(c, [&](auto lt, auto st, auto co, auto pi) {
         using L = typename decltype(lt)::type;
@@ -318,8 +339,6 @@ static int prepare_rows(lbm_ctx* c) {
 // Launch one time step reading buffer `from` and writing the other one.
 static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
     if (c->kernel_used == LBM_KERNEL_ROWS && c->d.collision == LBM_SHANCHEN) {
-        const dim3 fb(kScTX, kScTY), fg((unsigned)((c->d.nx + kScTX - 1) / kScTX),
-                                        (unsigned)((c->d.ny + kScTY - 1) / kScTY), (unsigned)c->d.nz);
         const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
         dispatch_storage(c->d.storage, [&](auto tag) {
             using S = typename decltype(tag)::type;
@@ -327,10 +346,12 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
             StepParams<R> p = params_of<R>(c);
             p.fin = c->f[from];
             p.fout = c->f[from ^ 1];
+            const int h = c->rows_rpg;
+            const dim3 wg((unsigned)((c->d.nx + kScwTX - 1) / kScwTX), (unsigned)((c->d.ny + h - 1) / h), 1);
             if (abs_arith)
-                k_step_sc_fused<S, true><<<fg, fb, 0, s>>>(p);
+                k_step_sc_window<S, true><<<wg, kScwTX, 0, s>>>(p, h);
             else
-                k_step_sc_fused<S, false><<<fg, fb, 0, s>>>(p);
+                k_step_sc_window<S, false><<<wg, kScwTX, 0, s>>>(p, h);
         });
         return;
     }
@@ -418,10 +439,7 @@ static int autotune(lbm_ctx* c) {
         c->kernel_used = LBM_KERNEL_PLAIN;
         return LBM_OK;
     }
-    // Shan-Chen: the one-pass kernel only when pinned (LBM_KERNEL_ROWS).  On the L2-resident 1024^2
-    // lattice it measured 41.1-41.6k vs 43.0-43.4k MLUPS for the two passes in FP32 (47.3k vs 46.1k in
-    // BF16S), while single-buffer trials here ranked it first.
-    const bool try_rows = c->kernel == LBM_KERNEL_AUTO && rows_eligible(c) && c->d.collision != LBM_SHANCHEN;
+    const bool try_rows = c->kernel == LBM_KERNEL_AUTO && rows_eligible(c);
     const std::string key = tune_key(c) + (try_rows ? "/rows" : "/plain");
     {
         std::lock_guard<std::mutex> g(g_tune_mu);

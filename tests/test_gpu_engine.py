@@ -379,10 +379,10 @@ def test_row_pipeline_segmented_wide_rows_equal_plain(storage, case):
 @pytest.mark.parametrize("shape,solid", [((128, 128), False), ((100, 50), True), ((20, 10), False),
                                          ((48, 36), True)])
 def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
-    """The one-pass Shan-Chen kernel (KERNEL_ROWS: psi of each tile and its ring recomputed in shared
-    memory) against the two-pass kernels (KERNEL_PLAIN: psi through global memory): bit-identical
-    populations and fields, on full and partial tiles, a lattice narrower than a tile, and with solid
-    (bounce-back, set-density) cells."""
+    """The one-pass Shan-Chen kernel (KERNEL_ROWS: a window sliding down y, psi of the next row in a
+    shared ring) against the two-pass kernels (KERNEL_PLAIN: psi through global memory): bit-identical
+    populations and fields, on full and partial column strips, a lattice narrower than a strip, and
+    with solid (bounce-back, set-density) cells."""
     if arith == lb.ARITH_ABSOLUTE and storage == lb.F16S:
         pytest.skip("absolute arithmetic is F32/F64 only")
     d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, storage, shape, omega=1.0, sc_G=-4.5, arithmetic=arith)
