@@ -574,10 +574,13 @@ __global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepPar
 #ifndef LBM_SCW_TX
 #define LBM_SCW_TX 128
 #endif
+#ifndef LBM_SCW_MINB
+#define LBM_SCW_MINB 8  // resident CTAs per SM asked of the compiler (FP64 storage: 4, up to 128 registers)
+#endif
 constexpr int kScwTX = LBM_SCW_TX;
 
 template <class S, bool ABS>
-__global__ void __launch_bounds__(kScwTX) k_step_sc_window(const __grid_constant__ StepParams<typename Codec<S>::Real> p,
+__global__ void __launch_bounds__(kScwTX, sizeof(typename Codec<S>::Real) == 8 ? 4 : LBM_SCW_MINB) k_step_sc_window(const __grid_constant__ StepParams<typename Codec<S>::Real> p,
                                                            int rows_per_strip) {
     using L = D2Q9;
     using R = typename Codec<S>::Real;
