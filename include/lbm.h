@@ -194,8 +194,10 @@ int   lbm_get_kernel(const lbm_ctx* c);              /* the family in use (PLAIN
  * format and layout, e.g. from lbm_device_populations), with no allocation of any kind: the scratch
  * (one partial per block + the result) is a fixed array in the library's device image, held by every
  * GPU that loads the library until the process exits (640 KB).
- *  - At most LBM_NOALLOC_MAX_CELLS cells; larger lattices are rejected with LBM_ERR_INVALID.
- *  - The first call on each device looks up the array's device address (cudaGetSymbolAddress); make
+ *  - At most LBM_NOALLOC_MAX_CELLS cells (nx * ny * nz, bounded without overflow); larger lattices
+ *    are rejected with LBM_ERR_INVALID.
+ *  - Every call looks up the array's device address on the current device (cudaGetSymbolAddress,
+ *    which allocates nothing); the first call on a device may load the library's device code, so make
  *    that first call before any stream capture.
  *  - Every call shares the one array, so calls that overlap on the GPU (other host threads, other
  *    streams) race; serialise them.  The call synchronises `stream` (a cudaStream_t, NULL = default).

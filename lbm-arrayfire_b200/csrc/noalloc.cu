@@ -8,8 +8,6 @@
 // block plus the folded result) lives in a fixed array of the library's device image instead of a
 // per-context buffer.  The array exists on every device that loads the library and stays allocated
 // until the process exits; it holds kMaxPartials + 1 entries of 40 bytes (640 KB).
-#include <mutex>
-
 #include "internal.h"
 #include "kernels.cuh"
 
@@ -20,29 +18,20 @@ constexpr int kThreads = 256;
 constexpr long long kCellsPerBlock = 4096;  // 16 cells per thread
 constexpr int kMaxPartials = 16384;         // -> LBM_NOALLOC_MAX_CELLS cells
 static_assert(kCellsPerBlock * kMaxPartials == LBM_NOALLOC_MAX_CELLS, "scratch capacity and header limit differ");
-constexpr int kMaxDevices = 64;
 
 // [0, kMaxPartials): one partial per block; [kMaxPartials]: the folded result of the call.
 // Every entry a call reads was written earlier in the same call, so nothing has to be cleared.
 static __device__ __align__(256) Sums g_noalloc_scratch[kMaxPartials + 1];
 
-std::mutex g_mu;
-Sums* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device.  In host code the array's name is
-// only a host-side stand-in, so the address is looked up once per device with that device current.
+// Device address of the scratch array on the current device.  In host code the array's name is only a
+// host-side stand-in, so the address is looked up with the device current, on every call: the lookup
+// allocates nothing, and a cached address would go stale if the context were destroyed and recreated
+// (cudaDeviceReset), when the library's module is loaded again and the array may move.
 int scratch_address(Sums** out) {
-    int dev = 0;
-    LBM_CK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return set_error(LBM_ERR_INVALID, "device ordinal beyond 63");
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(noalloc scratch)");
-        g_scratch_addr[dev] = static_cast<Sums*>(p);
-    }
-    *out = g_scratch_addr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(noalloc scratch)");
+    *out = static_cast<Sums*>(p);
     return LBM_OK;
 }
 
@@ -82,12 +71,13 @@ extern "C" int lbm_sums_fp64_noalloc(const void* populations, int lattice, int s
     if (nx < 1 || ny < 1 || nz < 1 || (lattice == LBM_D2Q9 && nz != 1))
         return set_error(LBM_ERR_INVALID, "bad lattice extents");
     if (storage_scale < 0.0) return set_error(LBM_ERR_INVALID, "storage_scale must be >= 0");
-    const long long N = (long long)nx * ny * nz;
-    if (nx > LBM_NOALLOC_MAX_CELLS || ny > LBM_NOALLOC_MAX_CELLS || nz > LBM_NOALLOC_MAX_CELLS ||
-        N > LBM_NOALLOC_MAX_CELLS)
+    // bound the product by division first: each extent alone may pass while nx * ny * nz wraps
+    const long long cap = LBM_NOALLOC_MAX_CELLS;
+    if (nx > cap || ny > cap / nx || nz > cap / (nx * ny))
         return set_error(LBM_ERR_INVALID,
                          "lattice has more than LBM_NOALLOC_MAX_CELLS (67,108,864) cells: the fixed scratch "
                          "array of lbm_sums_fp64_noalloc is too small; use lbm_sums_fp64");
+    const long long N = (long long)nx * ny * nz;
     Sums* scratch = nullptr;
     int rc = scratch_address(&scratch);
     if (rc) return rc;

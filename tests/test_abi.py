@@ -183,3 +183,17 @@ def test_null_handles_are_rejected():
     assert L.lbm_steps_done(None) == -1
     L.lbm_destroy(None)
     L.lbm_batch_destroy(None)
+
+
+@pytest.mark.parametrize("ext", [(1 << 22, 1 << 22, 1 << 22), (1 << 26, 1 << 26, 1 << 12),
+                                 (1 << 25, 3, 1), (8193, 8192, 1), (1 << 13, 1 << 13, 2)])
+def test_noalloc_rejects_extent_products_beyond_its_scratch(ext):
+    # each extent alone is within LBM_NOALLOC_MAX_CELLS, the product is not (some of them wrap a
+    # 64-bit product to 0 or to a small positive count): rejected before any device work
+    nx, ny, nz = ext
+    out = np.zeros(4)
+    lattice = lb.D2Q9 if nz == 1 else lb.D3Q27
+    rc = lb.lib().lbm_sums_fp64_noalloc(C.c_void_p(16), lattice, lb.F32, nx, ny, nz, 0.0, None,
+                                        C.c_void_p(out.ctypes.data))
+    assert rc == -1
+    assert b"LBM_NOALLOC_MAX_CELLS" in lb.lib().lbm_last_error()
