@@ -190,17 +190,25 @@ def gpu_id_for_smi(torch, dev):
 # CPU restatement (oracle) timings: the cpu_baseline object and the reference arm
 # ---------------------------------------------------------------------------------------------
 def oracle_problem_for(workload, n_side):
+    """The workload's problem for the CPU restatement, built on the oracle side only (oracle/problems.py
+    restates the reference drivers' set-up): the reference arm never loads the engine library.
+    n_side: cube side of a D3Q27 sample (None: the configuration's own size)."""
     sys.path.insert(0, str(ROOT / "oracle"))
-    sys.path.insert(0, str(ROOT / "tests"))
-    import lbm_b200 as lb
-    from helpers import oracle_problem
+    import problems as P
 
-    fn = WORKLOADS[workload][0]
-    if workload.startswith("d3q27"):
-        d, m = fn(lb, lb.F32, n_side)
-    else:
-        d, m = fn(lb, lb.F32)
-    return oracle_problem(d, m), d
+    if workload == "d3q27_mrt_gs_lid_256":
+        return P.config_mrt_lid((n_side or 256,) * 3)
+    if workload == "d3q27_bgk_lid_256":
+        return P.config_bgk_lid3d((n_side or 256,) * 3)
+    if workload == "d2q9_channel_1024x256":
+        return P.config_channel()
+    if workload == "d2q9_lid_128":
+        return P.config_lid128()
+    if workload == "d2q9_shanchen_1024":
+        return P.config_shanchen()
+    if workload == "d2q9_lid_8192":
+        return P.cavity2d(8192, 8192, 0.1, P.omega_from_re(0.1, 8192, 1000.0, 1))
+    raise KeyError(workload)
 
 
 def oracle_mlups(workload, target_s, cube=None):
@@ -208,7 +216,7 @@ def oracle_mlups(workload, target_s, cube=None):
     import oracle as O
 
     side = cube or 64
-    p, d = oracle_problem_for(workload, side)
+    p = oracle_problem_for(workload, side)
     F0 = O.init_equilibrium(p)
     t = time.perf_counter()
     O.run(p, F0, 1, dtype=np.float32)
@@ -250,9 +258,9 @@ def run_reference(args, rank, world):
     budget_cells = mlups0 * 1e6 * args.ref_seconds / max(1, args.steps + args.warmup)
     if args.workload.startswith("d3q27"):
         side = int(max(8, min(256, math.floor(budget_cells ** (1 / 3)))))
-        p, d = oracle_problem_for(args.workload, side)
+        p = oracle_problem_for(args.workload, side)
     else:
-        p, d = oracle_problem_for(args.workload, None)
+        p = oracle_problem_for(args.workload, None)
     F = O.init_equilibrium(p)
     if args.warmup:
         F, _, _ = O.run(p, F, args.warmup, dtype=np.float32)
@@ -275,17 +283,16 @@ def run_reference(args, rank, world):
 
 def run_reference_ensemble(args, world, O):
     """Reference arm of config 5: the CPU restatement on the smallest member of each lattice family
-    (a D2Q9 lid and a D3Q27 channel of the ensemble), K steps each; MLUPS = cells x steps / time."""
-    sys.path.insert(0, str(ROOT / "tests"))
-    import lbm_b200 as lb
-    from helpers import oracle_problem
+    (a D2Q9 lid and a D3Q27 channel of the ensemble), K steps each; MLUPS = cells x steps / time.  The
+    members come from oracle/problems.py (the same seeded list the engine side draws)."""
+    import problems as P
 
-    members = ensemble_members(lb, lb.F32)
+    spec = P.ensemble_spec(3)
     picks = []
-    for lat in (lb.D2Q9, lb.D3Q27):
-        d, m, name = min((x for x in members if x[0].lattice == lat), key=lambda x: x[0].cells)
-        picks.append((oracle_problem(d, m), name, d.shape))
-    cells = steps_done = 0
+    for fam in ("d2q9", "d3q27"):
+        name, shape, omega = min((s for s in spec if s[0].startswith(fam)), key=lambda s: int(np.prod(s[1])))
+        picks.append((P.ensemble_problem(name, shape, omega), name, shape))
+    cells = 0
     dt = 0.0
     for p, _, _ in picks:
         F = O.init_equilibrium(p)

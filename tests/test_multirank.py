@@ -103,3 +103,27 @@ def test_reference_arm_under_torchrun_prints_one_line_from_rank_zero():
     rec = json.loads(lines[0])
     assert rec["impl"] == "reference" and rec["n_gpus"] == 2 and rec["value"] > 0
     assert rec["e2e"]["h2d_bytes_per_step"] == 0 and rec["cpu_baseline"]["kind"] == "port"
+
+
+_REF_ARM_PROBE = r"""
+import json, sys
+sys.argv = ["bench.py", "--impl", "reference", "--workload", WORKLOAD, "--steps", "2", "--warmup", "0",
+            "--ref-seconds", "1"]
+sys.path.insert(0, ROOT)
+import bench
+bench.main()
+maps = open("/proc/self/maps").read()
+print(json.dumps({"engine_loaded": "liblbm_b200" in maps, "oracle_loaded": "liblbm_oracle" in maps,
+                  "engine_module": "lbm_b200" in sys.modules, "tests_module": "helpers" in sys.modules}))
+"""
+
+
+@pytest.mark.parametrize("workload", ["d2q9_lid_128", "d3q27_mrt_gs_lid_256", "ensemble_config5"])
+def test_reference_arm_loads_only_the_oracle(workload):
+    code = f"WORKLOAD = {workload!r}\nROOT = {str(ROOT)!r}\n" + _REF_ARM_PROBE
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=str(ROOT))
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(ln) for ln in out.stdout.splitlines() if ln.startswith("{")]
+    rec, probe = lines[0], lines[-1]
+    assert rec["impl"] == "reference" and rec["value"] > 0
+    assert probe == {"engine_loaded": False, "oracle_loaded": True, "engine_module": False, "tests_module": False}
