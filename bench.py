@@ -406,34 +406,227 @@ def e2e_measure(torch, lb, args, storage, dev, world):
             "api": "lbm_set_populations (pinned host F32) + lbm_step(K) + lbm_get_macros (pinned host F32)"}
 
 
-def accuracy(lb, args):
-    """rel. L2 velocity/density error of FP32 and FP16-shifted storage against the FP64 run of the
-    same collision, on a 256x64x64 lattice of the default workload (same rates and lid) after 1000
-    steps.  nx = 256 puts FP32/FP16S on the same kernel family as the headline (the row pipeline);
-    FP64 runs the one-cell-per-thread kernel."""
-    if not args.workload.startswith("d3q27_mrt"):
-        return None
-    res = {}
+# ---------------------------------------------------------------------------------------------
+# accuracy of FP32 and 16-bit storage against the FP64 run of the same kernels, every configuration
+# ---------------------------------------------------------------------------------------------
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    den = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (den if den > 0 else 1.0))
+
+
+def solid_cells(lb, d, m):
+    """Cells whose class bounces back (the reference's ON nodes)."""
+    if m is None:
+        return np.zeros(d.cells, dtype=bool)
+    flags = np.array([c[0] for c in lb.classes_of(d)])
+    return (flags[np.asarray(m).ravel()] & lb.BOUNCE) != 0
+
+
+def start_channel(lb, lat, d, m, u_in=0.04, seed=1, noise=1e-4):
+    """Config 2's start: equilibrium of rho = 1, u = (u_in + U(-noise, noise), 0) in the fluid (numpy
+    PCG64 seeded), rho = u = 0 in solid cells."""
+    solid = solid_cells(lb, d, m)
+    rng = np.random.default_rng(seed)
+    ux = np.where(solid, 0.0, u_in + rng.uniform(-noise, noise, d.cells))
+    lat.init_equilibrium(np.where(solid, 0.0, 1.0), np.concatenate([ux, np.zeros(d.cells)]))
+
+
+def start_shanchen(lb, lat, d, m, rho0=0.693, amp=0.01, seed=2):
+    """Config 3's start: rho = rho0 + U(-amp, amp) per cell (numpy PCG64 seeded), u = 0."""
+    rng = np.random.default_rng(seed)
+    lat.init_equilibrium(rho0 + rng.uniform(-amp, amp, d.cells))
+
+
+def acc_run(lb, wl, storage, steps, start=None, shape=None, hook=None):
+    """One run of a workload from its start state; returns fields, FP64 mass before/after, family."""
+    fn = WORKLOADS[wl][0]
+    d, m = fn(lb, storage, shape) if shape is not None else fn(lb, storage)
+    with lb.Lattice(d, m) as lat:
+        if start:
+            start(lb, lat, d, m)
+        m0 = lat.sums()[0]
+        extra = hook(lat, steps) if hook else lat.step(steps)
+        lat.sync()
+        rho, u = lat.macros()
+        m1 = lat.sums()[0]
+        fam = KERNEL_NAMES.get(lat.kernel(), "unknown")
+    return {"d": d, "m": m, "rho": rho, "u": u, "mass0": m0, "mass1": m1, "family": fam, "extra": extra}
+
+
+def field_errors(lb, runs, ref, names):
+    """rel. L2 of u and rho (non-solid cells) of each run against the reference run, and the FP64
+    mass drift of each run over its steps."""
+    d, m = runs[ref]["d"], runs[ref]["m"]
+    keep = ~solid_cells(lb, d, m)
+    n = d.cells
+    vel = lambda u: np.concatenate([u[k * n:(k + 1) * n][keep] for k in range(d.dim)])  # noqa: E731
+    out = {}
+    for name in names:
+        r = runs[name]
+        out[f"rel_l2_u_{name}_vs_f64"] = rel_l2(vel(r["u"]), vel(runs[ref]["u"]))
+        out[f"rel_l2_rho_{name}_vs_f64"] = rel_l2(r["rho"][keep], runs[ref]["rho"][keep])
+    for name, r in runs.items():
+        out[f"mass_drift_{name}"] = (r["mass1"] - r["mass0"]) / r["mass0"]
+    out["kernel_family"] = {name: r["family"] for name, r in runs.items()}
+    return out
+
+
+def acc_cavity128(lb):
+    """Config 1: D2Q9 lid 128^2, Re 100, 10,000 steps from rest; also the reference's own FP32
+    arithmetic (ABSOLUTE mode) against the same FP64 run."""
     runs = {}
-    families = {}
-    for st in (lb.F64, lb.F32, lb.F16S):
-        d, m = wl_mrt256(lb, st, (256, 64, 64))
-        with lb.Lattice(d, m) as lat:
-            apply_kernel_choice(lb, lat, args)
-            lat.step(1000)
-            rho, u = lat.macros()
-            families[STORAGE_NAMES[st]] = KERNEL_NAMES.get(lat.kernel(), "unknown")
-        runs[st] = (rho, u, m)
-    rho64, u64, m = runs[lb.F64]
-    fluid = np.tile(m != 1, 3)
-    for st, name in ((lb.F32, "f32"), (lb.F16S, "f16s")):
-        rho, u, _ = runs[st]
-        res[f"rel_l2_u_{name}_vs_f64"] = float(np.linalg.norm(u[fluid] - u64[fluid]) / np.linalg.norm(u64[fluid]))
-        res[f"rel_l2_rho_{name}_vs_f64"] = float(np.linalg.norm(rho[m != 1] - rho64[m != 1]) /
-                                                  np.linalg.norm(rho64[m != 1]))
-    res["lattice"] = "256x64x64 (same rates and lid), 1000 steps"
-    res["kernel_family"] = families
-    return res
+    for name, st in (("f64", lb.F64), ("f32", lb.F32), ("f16s", lb.F16S)):
+        runs[name] = acc_run(lb, "d2q9_lid_128", st, 10000)
+    d, m = wl_cavity128(lb, lb.F32)
+    d.arithmetic = lb.ARITH_ABSOLUTE
+    with lb.Lattice(d, m) as lat:
+        m0 = lat.sums()[0]
+        lat.step(10000)
+        rho, u = lat.macros()
+        runs["f32_reference_arithmetic"] = {"d": d, "m": m, "rho": rho, "u": u, "mass0": m0,
+                                            "mass1": lat.sums()[0], "family": "plain"}
+    out = field_errors(lb, runs, "f64", ["f32", "f16s", "f32_reference_arithmetic"])
+    out["steps"] = 10000
+    return out
+
+
+def channel_hook(probe, avg_steps=20000, every=100):
+    """Steps to the end; over the last avg_steps samples u every `every` steps: the time-averaged
+    velocity field and u_y at a probe point behind the cylinder (the shedding signal)."""
+    def hook(lat, steps):
+        lat.step(steps - avg_steps)
+        acc = None
+        sig = []
+        for _ in range(avg_steps // every):
+            lat.step(every)
+            _, u = lat.macros()
+            acc = u.copy() if acc is None else acc + u
+            sig.append(u[lat.n + probe])
+        return {"u_mean": acc / (avg_steps // every), "probe": np.array(sig), "every": every}
+    return hook
+
+
+def shedding_period(sig, every):
+    """Mean spacing of the upward zero crossings of the mean-free signal (linear interpolation), in
+    steps; None with fewer than two crossings."""
+    x = sig - sig.mean()
+    t = [k + x[k] / (x[k] - x[k + 1]) for k in range(len(x) - 1) if x[k] < 0 <= x[k + 1]]
+    if len(t) < 2:
+        return None
+    return float((t[-1] - t[0]) / (len(t) - 1) * every)
+
+
+def acc_channel(lb, steps=50000):
+    """Config 2: D2Q9 channel 1024x256, 50,000 steps from the seeded start.  The vortex street is a limit
+    cycle whose phase depends on every rounding since the start, so beside the instantaneous fields it
+    compares what the flow settles into: the velocity field averaged over the last 20,000 steps and the
+    shedding frequency (Strouhal number St = f d / U) at a probe 100 cells behind the cylinder on the
+    centre line."""
+    probe = 128 * 1024 + 300
+    runs = {}
+    for name, st in (("f64", lb.F64), ("f32", lb.F32), ("f16s", lb.F16S)):
+        runs[name] = acc_run(lb, "d2q9_channel_1024x256", st, steps, start=start_channel, hook=channel_hook(probe))
+    out = field_errors(lb, runs, "f64", ["f32", "f16s"])
+    d, m = runs["f64"]["d"], runs["f64"]["m"]
+    keep = np.tile(~solid_cells(lb, d, m), 2)
+    ref = runs["f64"]["extra"]["u_mean"][keep]
+    for name in ("f32", "f16s"):
+        out[f"rel_l2_u_mean_{name}_vs_f64"] = rel_l2(runs[name]["extra"]["u_mean"][keep], ref)
+    for name, r in runs.items():
+        T = shedding_period(r["extra"]["probe"], r["extra"]["every"])
+        out[f"strouhal_{name}"] = None if T is None else 40.0 / (T * 0.04)
+        out[f"probe_uy_rms_{name}"] = float(np.std(r["extra"]["probe"]))
+    out["steps"] = steps
+    out["note"] = ("u_mean: velocity averaged over the last 20,000 steps; Strouhal from the u_y zero crossings "
+                   "at (300, 128)")
+    return out
+
+
+def sc_statistics(rho, n):
+    """Phase-separation statistics of a density field: the mean densities of the dense and the light
+    phase (cells above / below the global mean), the dense-phase fraction, and the domain length
+    2 pi sum S(k) / sum |k| S(k) from the structure factor of the density."""
+    r = rho.reshape(n, n)
+    mean = r.mean()
+    dense = r > mean
+    S = np.abs(np.fft.fft2(r - mean)) ** 2
+    k = 2 * np.pi * np.fft.fftfreq(n)
+    kk = np.sqrt(k[:, None] ** 2 + k[None, :] ** 2)
+    S[0, 0] = 0.0
+    return {"rho_dense": float(r[dense].mean()), "rho_light": float(r[~dense].mean()),
+            "dense_fraction": float(dense.mean()), "domain_length": float(2 * np.pi * S.sum() / (kk * S).sum())}
+
+
+def acc_shanchen(lb, steps=20000):
+    """Config 3: D2Q9 Shan-Chen 1024^2, 20,000 steps from the seeded start.  Spinodal decomposition
+    amplifies every rounding difference (the pattern of domains differs in each run), so beside the
+    pointwise error the phases' statistics are compared: dense/light densities, dense fraction and
+    domain length; the FP64 mass drift of each run is its conservation error."""
+    runs = {}
+    for name, st in (("f64", lb.F64), ("f32", lb.F32), ("bf16s", lb.BF16S)):
+        runs[name] = acc_run(lb, "d2q9_shanchen_1024", st, steps, start=start_shanchen)
+    out = field_errors(lb, runs, "f64", ["f32", "bf16s"])
+    for name, r in runs.items():
+        out[f"stats_{name}"] = sc_statistics(r["rho"], 1024)
+    out["steps"] = steps
+    return out
+
+
+def acc_mrt256(lb, steps=5000, shape=(256, 256, 256)):
+    """Config 4: D3Q27 MRT (Gram-Schmidt) lid cavity 256^3, 5,000 steps from rest."""
+    runs = {}
+    for name, st in (("f64", lb.F64), ("f32", lb.F32), ("f16s", lb.F16S)):
+        runs[name] = acc_run(lb, "d3q27_mrt_gs_lid_256", st, steps, shape=shape)
+    out = field_errors(lb, runs, "f64", ["f32", "f16s"])
+    out["steps"] = steps
+    out["lattice"] = "x".join(map(str, shape))
+    return out
+
+
+def acc_ensemble(lb, steps=1000):
+    """Config 5: the F16S batch (one launch per step over every member) against each member's FP64 run
+    (stepped alone), after `steps` steps: per-member rel. L2 of u; max, median and the pooled value."""
+    members = ensemble_members(lb, lb.F16S)
+    batch = lb.Batch([d for d, _, _ in members], [m for _, m, _ in members])
+    batch.step(steps)
+    batch.sync()
+    members64 = ensemble_members(lb, lb.F64)
+    errs, num, den = [], 0.0, 0.0
+    for k, (d, m, name) in enumerate(members):
+        _, u16 = batch.macros(k)
+        dd, mm, _ = members64[k]
+        with lb.Lattice(dd, mm) as lat:
+            lat.step(steps)
+            _, u64 = lat.macros()
+        keep = np.tile(~solid_cells(lb, dd, mm), d.dim)
+        errs.append(rel_l2(u16[keep], u64[keep]))
+        num += float(np.sum((u16[keep] - u64[keep]) ** 2))
+        den += float(np.sum(u64[keep] ** 2))
+    batch.close()
+    return {"rel_l2_u_f16s_vs_f64_max": max(errs), "rel_l2_u_f16s_vs_f64_median": float(np.median(errs)),
+            "rel_l2_u_f16s_vs_f64_pooled": float(np.sqrt(num / den)), "members": len(members), "steps": steps,
+            "worst_member": members[int(np.argmax(errs))][2]}
+
+
+ACCURACY = {
+    "d2q9_lid_128": acc_cavity128,
+    "d2q9_channel_1024x256": acc_channel,
+    "d2q9_shanchen_1024": acc_shanchen,
+    "d3q27_mrt_gs_lid_256": acc_mrt256,
+    "ensemble_config5": acc_ensemble,
+}
+
+
+def accuracy_all(lb, which):
+    """Accuracy block of the default run: every configuration at its own size and step count."""
+    out = {}
+    for name in which:
+        t = time.perf_counter()
+        out[name] = ACCURACY[name](lb)
+        out[name]["seconds"] = time.perf_counter() - t
+    return out
 
 
 def barrier(torch, world):
@@ -580,6 +773,53 @@ def run_ensemble(args, rank, world, local_rank):
     return out
 
 
+# ---------------------------------------------------------------------------------------------
+# the other configurations' throughput (lines beside the headline)
+# ---------------------------------------------------------------------------------------------
+STORAGES = {"f16s": 1, "f32": 0, "bf16s": 2, "f64": 3}
+
+# (workload, 16-bit storage of the configuration, timed steps)
+SMALL_CONFIGS = (("d2q9_lid_128", "f16s", 20000), ("d2q9_channel_1024x256", "f16s", 4000),
+                 ("d2q9_shanchen_1024", "bf16s", 2000))
+
+
+def config_lines(torch, lb, args, dev, world):
+    """MLUPS of configs 1-3 (16-bit storage and FP32) and of the config-5 ensemble, each timed like the
+    headline (CUDA events on the lattice's stream after warm-up).  Configs 1-3 are L2-resident (their
+    populations fit the 126 MB L2), so no HBM roofline applies to them; their achieved GB/s is stated
+    against the algorithmic bytes."""
+    import copy
+
+    out = {}
+    for wl, st16, steps in SMALL_CONFIGS:
+        rec = {}
+        for stn in (st16, "f32"):
+            a = copy.copy(args)
+            a.workload, a.steps, a.warmup = wl, steps, max(args.warmup, 3)
+            a.kernel, a.block, a.dims, a.size = "auto", 0, "", 0
+            d, lat, el, _ = measure(torch, lb, a, STORAGES[stn], dev, world)
+            fam = KERNEL_NAMES.get(lat.kernel(), "unknown")
+            lat.close()
+            del lat
+            rec[stn] = {"value": d.cells * steps / el / 1e6, "unit": "MLUPS", "ms_per_step": el * 1e3 / steps,
+                        "kernel_family": fam,
+                        "achieved_gbs": algorithmic_bytes_per_cell(d) * d.cells * steps / el / 1e9}
+            rec["lattice"] = list(d.shape)
+            rec["l2"] = (f"L2-resident ({d.cells * d.q * storage_bytes(STORAGES[stn]) * 2 / 1e6:.1f} MB of "
+                         f"populations in both buffers at {stn}); no flush")
+        rec[f"speedup_{st16}_vs_f32"] = rec[st16]["value"] / rec["f32"]["value"]
+        rec["steps"] = steps
+        out[wl] = rec
+    a = copy.copy(args)
+    a.workload, a.storage = "ensemble_config5", "f16s"
+    e = run_ensemble(a, 0, world, dev)
+    keep = ("value", "unit", "ms_per_step", "roofline", "fp32_batched", "speedup_f16s_vs_f32", "sequential_plain",
+            "speedup_batched_vs_sequential", "clocks", "gpu_launches", "steps")
+    out["ensemble_config5"] = {k: e[k] for k in keep if k in e}
+    out["ensemble_config5"]["config"] = {k: e["config"][k] for k in ("members", "cells", "storage", "l2", "batch_mode")}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -640,10 +880,10 @@ def run_ours(args, rank, world, local_rank):
         out[f"speedup_{STORAGE_NAMES[head_storage]}_vs_f32"] = value / v32
     if not args.no_e2e:
         out["e2e"] = e2e_measure(torch, lb, args, head_storage, dev, world)
+    if rank == 0 and world == 1 and not args.no_configs:
+        out["configs"] = config_lines(torch, lb, args, dev, world)
     if rank == 0 and world == 1 and not args.no_accuracy:
-        acc = accuracy(lb, args)
-        if acc:
-            out["accuracy"] = acc
+        out["accuracy"] = accuracy_all(lb, args.accuracy.split(",") if args.accuracy else list(ACCURACY))
     if rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle as O
@@ -669,6 +909,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--accuracy", default="", help="comma-separated configurations of the accuracy block "
+                    f"(default: all of {','.join(ACCURACY)})")
+    ap.add_argument("--accuracy-only", action="store_true", help="print the accuracy block alone and exit")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' throughput lines")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=150.0, help="time budget of the reference arm")
     ap.add_argument("--size", type=int, default=0,
@@ -690,6 +934,13 @@ def main():
         return
     import torch
 
+    if args.accuracy_only:
+        import lbm_b200 as lb
+
+        torch.cuda.set_device(local_rank)
+        print(json.dumps(accuracy_all(lb, args.accuracy.split(",") if args.accuracy else list(ACCURACY))),
+              flush=True)
+        return
     if world > 1:
         import datetime
 

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "arith.cuh"
 #include "codec.cuh"
@@ -194,17 +195,39 @@ __device__ __forceinline__ R feq_abs_i(R rho, R usq15, R ux, R uy, R uz) {
 // evaluated once per pair of opposite directions: the symmetric part is shared and the
 // momentum-carrying part is exactly antisymmetric.  sc: storage scale of the result (power of two).
 // Every multiply-add is explicit (mad): the rounding is fixed by the source (arith.cuh).
-template <class L, class R>
+//
+// EXACTW (FP32 storage): each weight is applied as a sum of two floats, w = hi + lo (hi the float
+// nearest w, lo the float nearest the remainder), as mad(hi, x, lo * x).  No float equals 1/9, 2/27,
+// ...: with the nearest floats alone the weights' moments miss their exact values by ~1e-8 (e.g.
+// 3 sum_i w_i c_ix^2 = 9 fl(1/9) = 1 + 7.5e-9 for D2Q9), so every collision scales the momentum by
+// 1 + omega * 7.5e-9 while the mass (rho - 1 = sum of deviations) stays put.  That systematic error
+// drifts u linearly (the 128^2 lid cavity: rel. L2 1.8e-5 from the FP64 run after 10,000 steps).  The
+// reference's own FP32 arithmetic scales mass and momentum alike (its density drifts instead, 8e-5
+// there).  The two-float weights make the moments exact to ~1e-15; the rounding left is unbiased.
+// 16-bit storage rounds each population far more coarsely than that bias, FP64 weights are exact to
+// 1e-17: both keep the single multiply.
+template <class L, bool EXACTW, class R>
 __device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz, R sc, R (&fe)[L::Q]) {
     const R nusq15 = R(-1.5) * mad(uz, uz, mad(uy, uy, ux * ux));
     const R rho3 = R(3) * rho;
     const R rho45 = R(4.5) * rho;
     const R base = mad(rho, nusq15, drho);
+    // w_i (times sc) applied to x: one multiply, or hi + lo by one multiply-add (EXACTW)
+    auto wmul = [&](auto I, R x) {
+        constexpr int i = decltype(I)::value;
+        if constexpr (EXACTW) {
+            constexpr R hi = R(L::w(i));
+            constexpr R lo = R(L::w(i) - double(hi));
+            return mad(hi * sc, x, (lo * sc) * x);
+        } else {
+            return (R(L::w(i)) * sc) * x;
+        }
+    };
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
         constexpr int o = L::opp(i);
         if constexpr (i == 0) {
-            fe[0] = (R(L::w(0)) * sc) * base;
+            fe[0] = wmul(I, base);
         } else if constexpr (i < o) {
             constexpr int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
             // c.u from its first nonzero term (no 0 + x)
@@ -213,16 +236,15 @@ __device__ __forceinline__ void equilibrium_dev(R rho, R drho, R ux, R uy, R uz,
             if constexpr (cx != 0 && cy == -1) eu = eu - uy;
             if constexpr ((cx != 0 || cy != 0) && cz == 1) eu = eu + uz;
             if constexpr ((cx != 0 || cy != 0) && cz == -1) eu = eu - uz;
-            const R w = R(L::w(i)) * sc;
-            const R sym = w * mad(rho45, eu * eu, base);
-            const R anti = w * (rho3 * eu);
+            const R sym = wmul(I, mad(rho45, eu * eu, base));
+            const R anti = wmul(I, rho3 * eu);
             fe[i] = sym + anti;
             fe[o] = sym - anti;
         }
     });
 }
 
-template <class L, bool ABS, class R>
+template <class L, bool ABS, bool EXACTW, class R>
 __device__ __forceinline__ void equilibrium_v(R rho, R drho, R ux, R uy, R uz, R sc, R (&feq)[L::Q]) {
     if constexpr (ABS) {
         const R usq15 = R(1.5) * (ux * ux + uy * uy + uz * uz);
@@ -231,15 +253,19 @@ __device__ __forceinline__ void equilibrium_v(R rho, R drho, R ux, R uy, R uz, R
             feq[i] = feq_abs_i<L, i>(rho, usq15, ux, uy, uz);
         });
     } else {
-        equilibrium_dev<L, R>(rho, drho, ux, uy, uz, sc, feq);
+        equilibrium_dev<L, EXACTW, R>(rho, drho, ux, uy, uz, sc, feq);
     }
 }
+
+// Storage types whose equilibrium applies the weights as two floats (equilibrium_dev).
+template <class S>
+constexpr bool kExactWeights = std::is_same_v<S, float>;
 
 // feq_i = w_i rho (1 + 3 eu + 4.5 eu^2 - 1.5 u^2) (absolute values, used to initialise)
 template <class L, class R>
 __device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R (&feq)[L::Q]) {
     R dev[L::Q];
-    equilibrium_dev<L, R>(rho, rho - R(1), ux, uy, uz, R(1), dev);
+    equilibrium_dev<L, false, R>(rho, rho - R(1), ux, uy, uz, R(1), dev);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
         feq[i] = R(L::w(i)) + dev[i];
@@ -282,14 +308,14 @@ __device__ __forceinline__ void cell_class(const uint8_t* __restrict__ mask, con
 // F = omega FEQ + (1 - omega) F_streamed (cpp/d2q9_bgk_lid.cpp:153), the class overwrites before it
 // and the full-way bounce-back after it (:155).  P supplies cls, omega, one_m_omega.  Deviations
 // are in storage units: sc / isc are the storage scale and its inverse (1 for ABS).
-template <class L, bool ABS, class P, class R>
+template <class L, bool ABS, bool EXACTW, class P, class R>
 __device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, const R (&v)[L::Q], R sc, R isc,
                                             R (&out)[L::Q]) {
     R rho, drho, ux, uy, uz;
     moments<L, ABS>(v, sc, isc, rho, drho, ux, uy, uz);
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
     R fe[L::Q];
-    equilibrium_v<L, ABS>(rho, drho, ux, uy, uz, sc, fe);
+    equilibrium_v<L, ABS, EXACTW>(rho, drho, ux, uy, uz, sc, fe);
     const R omega = R(p.omega), one_m = R(p.one_m_omega);
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
@@ -322,7 +348,7 @@ __device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, 
     R sc, isc;
     storage_scale<S>(p, sc, isc);
     R out[L::Q];
-    bgk_collide<L, ABS>(p, cls, fl, v, sc, isc, out);
+    bgk_collide<L, ABS, kExactWeights<S>>(p, cls, fl, v, sc, isc, out);
     store_cell<L, S, ABS>(fout, p, c, out);
 }
 
@@ -379,7 +405,7 @@ __device__ __forceinline__ void mrt_post(R (&T)[27], R rho, R drho, R ux, R uy, 
     });
 }
 
-template <int BASIS, class P, class R>
+template <int BASIS, bool EXACTW, class P, class R>
 __device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R (&T)[27], R sc, R isc,
                                             R (&out)[27]) {
     using L = D3Q27;
@@ -387,7 +413,7 @@ __device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R 
     mrt_pre<BASIS>(T, isc, rho, drho, ux, uy, uz);
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 3);
     mrt_post<BASIS>(T, rho, drho, ux, uy, uz, p.mrt, out);
-    if (fl & kEquilibrium) equilibrium_dev<L, R>(rho, drho, ux, uy, uz, sc, out);
+    if (fl & kEquilibrium) equilibrium_dev<L, EXACTW, R>(rho, drho, ux, uy, uz, sc, out);
 }
 
 template <int BASIS, class S>
@@ -416,7 +442,7 @@ __global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepPa
     R sc, isc;
     storage_scale<S>(p, sc, isc);
     R out[27];
-    mrt_collide<BASIS>(p, cls, fl, T, sc, isc, out);
+    mrt_collide<BASIS, kExactWeights<S>>(p, cls, fl, T, sc, isc, out);
     if (fl & kBounce) {
         // reload the streamed deviations (the transform overwrote them in place)
         R v[27];
@@ -527,7 +553,7 @@ __device__ __forceinline__ void sc_collide_store(const StepParams<R>& p, long lo
         vy = uy + Fy * k;
     }
     R fe[9];
-    equilibrium_v<L, ABS>(rho, drho, vx, vy, R(0), sc, fe);
+    equilibrium_v<L, ABS, kExactWeights<S>>(rho, drho, vx, vy, R(0), sc, fe);
     R out[9];
     static_for<9>([&](auto I) {
         constexpr int i = I;

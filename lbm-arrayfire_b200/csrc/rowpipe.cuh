@@ -252,14 +252,14 @@ __device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t*
     }
     R out[Q];
     if constexpr (COLL == 0) {
-        bgk_collide<L, false>(p, cls, fl, v, sc, isc, out);
+        bgk_collide<L, false, kExactWeights<S>>(p, cls, fl, v, sc, isc, out);
     } else {
         R T[27];
         static_for<27>([&](auto I) {
             constexpr int i = I;
             T[L::slot(i)] = v[i];
         });
-        mrt_collide<COLL == 1 ? kMrtRef : kMrtGramSchmidt>(p, cls, fl, T, sc, isc, out);
+        mrt_collide<COLL == 1 ? kMrtRef : kMrtGramSchmidt, kExactWeights<S>>(p, cls, fl, T, sc, isc, out);
         if (fl & kBounce) {
             static_for<Q - 1>([&](auto I) {
                 constexpr int i = I + 1;
