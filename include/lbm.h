@@ -185,6 +185,17 @@ enum lbm_kernel { LBM_KERNEL_AUTO = 0, LBM_KERNEL_PLAIN = 1, LBM_KERNEL_ROWS = 2
 int   lbm_set_kernel(lbm_ctx* c, int kind);
 int   lbm_get_kernel(const lbm_ctx* c);              /* the family in use (PLAIN or ROWS), or AUTO before the first step */
 
+/* ---- test hook of the bounded device-side waits (no counterpart in the reference) --------
+ * Arms a one-shot stall of the row pipeline so that tests can drive its bounded mbarrier waits to
+ * their limit without any fault: the next lbm_step launches its first step on its own, the producer
+ * of that launch issues no copies for work item `item` (a row group or row segment in the order the
+ * persistent CTAs take them; item 0 is the first stage of CTA 0), and every wait of that launch gives
+ * up after `wait_clocks` SM clocks (2^10 .. 2^32; 2^21 is about a millisecond).  The consumers waiting
+ * for that stage time out, then its producer; the launch returns and lbm_sync reports LBM_ERR_TIMEOUT
+ * once (it clears the error word).  The populations written by that step are invalid: set or
+ * re-initialise them before stepping on.  Needs lbm_set_kernel(c, LBM_KERNEL_ROWS) (BGK or MRT).   */
+int  lbm_test_stall_next_step(lbm_ctx* c, int64_t item, int64_t wait_clocks);
+
 /* ---- conservation sums without allocation -----------------------------------------------
  * No counterpart in the reference.  For callers that cannot let a library call cudaMalloc or
  * cudaFree — applications whose device memory belongs to another allocator (a framework's caching

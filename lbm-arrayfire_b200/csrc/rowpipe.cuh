@@ -23,8 +23,12 @@
 // Compared with the one-cell-per-thread kernel this removes the per-population 64-bit load-address
 // arithmetic and decouples memory latency from occupancy.
 //
-// Every wait on an mbarrier is bounded (about two seconds); a warp that times out records
-// kRowPipeTimeout in *err and returns (consumers after a bounded wait for copies into their stages).
+// Every wait on an mbarrier is bounded (about two seconds, WaitLimits); a warp that times out records
+// kRowPipeTimeout in *err and returns.  Consumers first wait (bounded, 2^28 clocks at most) for the
+// copies already issued into their later stages.  Once any consumer warp has left, the stage it held is
+// never released, so the producer issues nothing more and itself times out on that stage.  The one case
+// left open: a copy that has not landed when that last bounded wait gives up (a DRAM read stalled for
+// over 0.1 s) would still be in flight into the CTA's shared memory after it exits.
 // No multicast: every copy moves data of this GPU's own memory into this CTA's shared memory.
 #pragma once
 
@@ -35,6 +39,17 @@
 namespace lbm {
 
 constexpr int kRowPipeTimeout = 1;
+
+// Limits of a launch's mbarrier waits.  In production skip = ~0u (every work item is issued) and every
+// wait gives up after `limit` = 2^32 clocks (about two seconds).  The test hook lbm_test_stall_next_step
+// sets skip to one work item, whose copies the producer then never issues (nothing is in flight for it,
+// so nothing can fault), and a short limit: the consumers waiting for that stage give up, then the
+// producer, and the launch returns with kRowPipeTimeout in the error word.
+struct WaitLimits {
+    unsigned skip;
+    long long limit;
+};
+constexpr WaitLimits kProductionWaits{~0u, 1LL << 32};
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -294,7 +309,8 @@ __device__ __forceinline__ void row_cell_wrap(const P& p, const S* st, const uin
 // Stage s holds, for direction i, the group's source rows at in[(s * Q + i) * SB + b * nx].
 template <class L, class S, int PITCH, int COLL>
 __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, RowPipeShape<L, S, PITCH>::CTAS)
-    k_step_rows(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int rows, int* __restrict__ err) {
+    k_step_rows(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int rows, int* __restrict__ err,
+                  const WaitLimits wl) {
     using R = typename Codec<S>::Real;
     using Sh = RowPipeShape<L, S, PITCH>;
     constexpr int Q = L::Q;
@@ -324,6 +340,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
 
     // Issue the bulk loads of group g into stage s (one warp; lanes 0..Q-1 one direction each).
     auto issue = [&](unsigned g, int s) {
+        if (g == wl.skip) return;  // test hook: this item's stage is never filled
         const int y0 = (int)(g % ugy) * B, z = (int)(g / ugy);
         const int nb = ny - y0 < B ? ny - y0 : B;
         if (lane == 0)
@@ -358,7 +375,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
             if (first + s * stride < groups) issue(first + s * stride, s);
         for (unsigned k = 0; first + (k + NS) * stride < groups; ++k) {
             const int s = (int)(k % NS);
-            if (!mbar_wait_sleep<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1))) {
+            if (!mbar_wait_sleep<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1), wl.limit)) {
                 if (lane == 0) atomicExch(err, kRowPipeTimeout);
                 return;
             }
@@ -376,11 +393,13 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     for (unsigned k = 0; first + k * stride < groups; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
-        if (!mbar_wait_sleep<Sh::CONSUMER_SLEEP>(&full[s], (uint32_t)((k / NS) & 1))) {
+        if (!mbar_wait_sleep<Sh::CONSUMER_SLEEP>(&full[s], (uint32_t)((k / NS) & 1), wl.limit)) {
             if (lane == 0) atomicExch(err, kRowPipeTimeout);
             // wait, briefly and bounded, for copies that may still land in this CTA's stages
             for (int j = 1; j < NS && first + (k + j) * stride < groups; ++j)
-                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1), 1LL << 28)) break;
+                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1),
+                                       wl.limit < (1LL << 28) ? wl.limit : (1LL << 28)))
+                    break;
             return;
         }
         const int y0 = (int)(g % ugy) * B, z = (int)(g / ugy);
@@ -415,7 +434,8 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
 // index j holds x = x0 - HALO + j.
 template <class L, class S, int COLL>
 __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS + 32, RowPipeShape<L, S, kSegPitch, true>::CTAS)
-    k_step_rows_seg(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int segw, int* __restrict__ err) {
+    k_step_rows_seg(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int segw, int* __restrict__ err,
+                  const WaitLimits wl) {
     using R = typename Codec<S>::Real;
     using Sh = RowPipeShape<L, S, kSegPitch, true>;
     constexpr int Q = L::Q;
@@ -444,6 +464,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
 
     auto issue = [&](unsigned g, int s) {
+        if (g == wl.skip) return;  // test hook: this item's stage is never filled
         const unsigned row = g / useg;
         const int seg = (int)(g - row * useg);
         const int z = (int)(row / uny), y = (int)(row - (unsigned)z * uny);
@@ -487,7 +508,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
             if (first + s * stride < groups) issue(first + s * stride, s);
         for (unsigned k = 0; first + (k + NS) * stride < groups; ++k) {
             const int s = (int)(k % NS);
-            if (!mbar_wait_sleep<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1))) {
+            if (!mbar_wait_sleep<Sh::PRODUCER_SLEEP>(&empty[s], (uint32_t)((k / NS) & 1), wl.limit)) {
                 if (lane == 0) atomicExch(err, kRowPipeTimeout);
                 return;
             }
@@ -500,10 +521,12 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
     for (unsigned k = 0; first + k * stride < groups; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
-        if (!mbar_wait_sleep<Sh::CONSUMER_SLEEP>(&full[s], (uint32_t)((k / NS) & 1))) {
+        if (!mbar_wait_sleep<Sh::CONSUMER_SLEEP>(&full[s], (uint32_t)((k / NS) & 1), wl.limit)) {
             if (lane == 0) atomicExch(err, kRowPipeTimeout);
             for (int j = 1; j < NS && first + (k + j) * stride < groups; ++j)
-                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1), 1LL << 28)) break;
+                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1),
+                                       wl.limit < (1LL << 28) ? wl.limit : (1LL << 28)))
+                    break;
             return;
         }
         const unsigned row = g / useg;

@@ -128,6 +128,9 @@ struct lbm_ctx {
     int rows_grid = 0;             // persistent grid of the row pipeline
     int rows_rpg = 1;              // its rows per group (segmented rows: the segment width)
     int* err = nullptr;            // device error word of the row pipeline
+    WaitLimits waits = kProductionWaits;  // the row pipeline's wait limits for the next launch
+    bool stall_armed = false;      // lbm_test_stall_next_step: the next step launches with `stall`
+    WaitLimits stall = kProductionWaits;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int gsteps = 0;
     bool has_prev = false;
@@ -217,12 +220,13 @@ template <class L, class S, int PITCH, int COLL>
 static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s) {
     if (rows_segmented(c)) {
         using Sh = RowPipeShape<L, S, kSegPitch, true>;
-        k_step_rows_seg<L, S, COLL><<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err);
+        k_step_rows_seg<L, S, COLL><<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err,
+                                                                                              c->waits);
         return;
     }
     using Sh = RowPipeShape<L, S, PITCH>;
     auto kern = k_step_rows<L, S, PITCH, COLL>;
-    kern<<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err);  // + producer warp
+    kern<<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err, c->waits);  // + producer warp
 }
 
 template <class L, class S, int PITCH, int COLL>
@@ -774,6 +778,16 @@ int lbm_step(lbm_ctx* c, int64_t nsteps) {
     }
     LBM_CK(cudaEventRecord(c->e0, c->stream));
     long long n = nsteps;
+    if (c->stall_armed) {
+        // the armed test stall: one direct launch with its wait limits, before any graph (which
+        // captures the production limits)
+        c->stall_armed = false;
+        c->waits = c->stall;
+        launch_step(c, c->cur, c->stream, c->block);
+        c->waits = kProductionWaits;
+        c->cur ^= 1;
+        --n;
+    }
     if (n >= 2) {
         if (!c->gsteps) {
             int rc = build_graphs(c);
@@ -1002,5 +1016,18 @@ int lbm_set_kernel(lbm_ctx* c, int kind) {
 }
 
 int lbm_get_kernel(const lbm_ctx* c) { return c ? c->kernel_used : 0; }
+
+int lbm_test_stall_next_step(lbm_ctx* c, int64_t item, int64_t wait_clocks) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    if (item < 0 || item >= 0xffffffffLL) return set_error(LBM_ERR_INVALID, "work item out of range");
+    if (wait_clocks < (1LL << 10) || wait_clocks > (1LL << 32))
+        return set_error(LBM_ERR_INVALID, "wait_clocks must be in [2^10, 2^32]");
+    if (c->kernel != LBM_KERNEL_ROWS || c->d.collision == LBM_SHANCHEN)
+        return set_error(LBM_ERR_STATE,
+                         "the stall applies to the row pipeline's bulk-copy stages: pin LBM_KERNEL_ROWS (BGK/MRT) first");
+    c->stall = WaitLimits{(unsigned)item, (long long)wait_clocks};
+    c->stall_armed = true;
+    return LBM_OK;
+}
 
 }  // extern "C"

@@ -115,6 +115,7 @@ _SIGS = {
     "lbm_get_block": (C.c_int, [_P]),
     "lbm_set_kernel": (C.c_int, [_P, C.c_int]),
     "lbm_get_kernel": (C.c_int, [_P]),
+    "lbm_test_stall_next_step": (C.c_int, [_P, C.c_int64, C.c_int64]),
     "lbm_sums_fp64_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_double, _P, _P]),
     "lbm_batch_create": (C.c_int, [_DP, C.c_int, C.POINTER(_P)]),
     "lbm_batch_destroy": (None, [_P]),
@@ -349,6 +350,11 @@ class Lattice:
 
     def kernel(self) -> int:
         return lib().lbm_get_kernel(self._h)
+
+    def test_stall_next_step(self, item: int = 0, wait_clocks: int = 1 << 21):
+        """Test hook: the next step's row pipeline leaves work item `item` unfilled and gives its waits
+        `wait_clocks` clocks; lbm_sync then reports LBM_ERR_TIMEOUT (see lbm_test_stall_next_step)."""
+        _check(lib().lbm_test_stall_next_step(self._h, item, wait_clocks))
 
     def device_populations(self):
         nbytes = C.c_size_t()
