@@ -20,7 +20,7 @@ def build():
 
 def test_drivers_build_and_link():
     build()
-    for name in ("d2q9_bgk_lid", "d3q27_mrt_lid"):
+    for name in ("d2q9_bgk_lid", "d3q27_mrt_lid", "d2q9_bgk_channel", "d3q27_bgk_lid"):
         assert (BIN / name).exists()
 
 
@@ -62,3 +62,52 @@ def test_d3q27_mrt_driver_runs_and_reports(tmp_path):
     assert f.size == 4 * 32 ** 3 and np.isfinite(f).all()
     ux = f[32 ** 3:2 * 32 ** 3].reshape(32, 32, 32, order="F")
     assert ux[16, 16, 30] > 0.0  # the lid on the z top drags the fluid below it along +x
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("config_mode", [False, True])
+def test_d2q9_channel_driver_matches_oracle(tmp_path, config_mode):
+    """cpp/d2q9_bgk_channel_packed.cpp's geometry rules at 140 x 60 (cylinder at (nx/5 + 1, ny/2 + ny/30),
+    radius ny/10 + 1, Re 220, u_max 0.1), 300 iterations through the driver against the FP64 oracle."""
+    from helpers import O, P, rel_l2
+
+    build()
+    dump = tmp_path / "fields.bin"
+    args = [str(BIN / "d2q9_bgk_channel"), "140", "60", "300", "--dump", str(dump)] + (["--config"] if config_mode else [])
+    out = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert "Iterations: 300" in out.stdout
+    nx, ny = 140, 60
+    f = np.fromfile(dump, dtype=np.float64)
+    n = nx * ny
+    rho, u = f[:n], f[n:]
+    ox, oy, r = nx // 5 + 1, ny // 2 + ny // 30, ny // 10 + 1
+    p = P.channel2d(nx, ny, 0.1, ox, oy, r, 1.0 / (3 * (0.1 * 2 * r / 220.0) + 0.5), config_mode)
+    _, rho_o, u_o = O.run(p, P.channel_start_state(p, 0.1), 300)
+    flags = np.array([c[0] for c in p.classes])[np.asarray(p.mask)]
+    fluid = (flags & O.BOUNCE) == 0
+    assert rel_l2(rho[fluid], rho_o[fluid]) < 1e-5
+    uf = np.tile(fluid, 2)
+    assert rel_l2(u[uf], u_o[uf]) < 1e-5
+
+
+@pytest.mark.gpu
+def test_d3q27_bgk_driver_matches_oracle(tmp_path):
+    """cpp/d3q27_bgk_lid.cpp's cavity (lid 0.1 on the z top, Re 150 on nx) at 24 x 20 x 18, 200
+    iterations through the driver against the FP64 oracle."""
+    from helpers import O, P, rel_l2
+
+    build()
+    dump = tmp_path / "fields.bin"
+    out = subprocess.run([str(BIN / "d3q27_bgk_lid"), "24", "20", "18", "200", "--dump", str(dump)],
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert "Iterations: 200" in out.stdout
+    n = 24 * 20 * 18
+    f = np.fromfile(dump, dtype=np.float64)
+    rho, u = f[:n], f[n:]
+    p = P.cavity3d(24, 20, 18, 0.1, omega=P.omega_from_re(0.1, 24, 150.0, 0))
+    _, rho_o, u_o = O.run(p, P.rest_state(p), 200)
+    fluid = np.asarray(p.mask) == 0
+    assert rel_l2(rho[fluid], rho_o[fluid]) < 1e-5
+    assert rel_l2(u[np.tile(fluid, 3)], u_o[np.tile(fluid, 3)]) < 1e-5
