@@ -46,6 +46,7 @@ struct StepParams {
     R* u_out;
     ClassTable<R> cls;
     MrtCoef<R> mrt;
+    Mrt2Coef<R> mrt2;
 };
 
 // Row base offsets of the 3 (D2Q9) or 9 (D3Q27) neighbour rows of (y, z), wrap included.
@@ -416,6 +417,129 @@ __device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R 
     if (fl & kEquilibrium) equilibrium_dev<L, EXACTW, R>(rho, drho, ux, uy, uz, sc, out);
 }
 
+// ---- two-rate MRT (Gram-Schmidt basis) -----------------------------------------------------
+// With the rows of M orthogonal (M M^T = D diagonal, M^-1 = M^T D^-1) and meq = M feq, a rate vector
+// with two values -- s_v on the shear rows, s_o on every other row -- turns the collision
+// f* = M^-1 (m - S (m - meq)) into
+//   f* = f - s_o (f - feq) - (s_v - s_o) sum_{k in shear} M_k (m_k - meq_k) / D_k,
+// the same map, evaluated without the full forward and inverse transforms: the moments needed are rho,
+// j and the five shear moments (a partial tensor transform, 79 adds instead of 108), the equilibrium
+// comes per pair of opposite directions as in BGK, and the shear correction is even in c, so each pair
+// shares it.  In storage units on deviations like mrt_collide (the shear moments of w are zero).  The
+// shear rows (Gram-Schmidt): cx cy, cx cz, cy cz (|row|^2 = 12), 3(cx^2 - cy^2) (108) and
+// 3(cx^2 + cy^2 - 2 cz^2) (324); their equilibrium moments rho ux uy, rho ux uz, rho uy uz,
+// 3 rho (ux^2 - uy^2), 3 rho (ux^2 + uy^2 - 2 uz^2).  v: streamed deviations in direction order (kept:
+// bounce-back reads them).  Used for 16-bit storage when the rates have that structure (the benchmark
+// cavity's); the general collision stays for every other case.
+template <class P, class R>
+__device__ __forceinline__ void mrt2_collide(const P& p, int cls, uint32_t fl, const R (&v)[27], R sc, R isc,
+                                             R (&out)[27]) {
+    using L = D3Q27;
+    // x lines: (cy, cz) = line l = yb + 3 zc; X0 = sum, X1 = c-moment, X2 = (3c^2 - 2)-moment
+    R X0[9], X1[9], X2[9];
+    static_for<9>([&](auto Lc) {
+        constexpr int l = Lc;
+        constexpr int cy = l % 3 - 1, cz = l / 3 - 1;
+        constexpr int im = L::dir_of(-1, cy, cz), i0 = L::dir_of(0, cy, cz), ip = L::dir_of(1, cy, cz);
+        const R sum2 = v[im] + v[ip];
+        X1[l] = v[ip] - v[im];
+        X0[l] = sum2 + v[i0];
+        X2[l] = minus_twice(sum2, v[i0]);
+    });
+    // y lines per z
+    R Y00[3], Y01[3], Y02[3], Y10[3], Y11[3], Y20[3];
+    static_for<3>([&](auto Zc) {
+        constexpr int z = Zc;
+        const R s0 = X0[3 * z] + X0[3 * z + 2];
+        Y00[z] = s0 + X0[3 * z + 1];
+        Y01[z] = X0[3 * z + 2] - X0[3 * z];
+        Y02[z] = minus_twice(s0, X0[3 * z + 1]);
+        Y10[z] = (X1[3 * z] + X1[3 * z + 2]) + X1[3 * z + 1];
+        Y11[z] = X1[3 * z + 2] - X1[3 * z];
+        Y20[z] = (X2[3 * z] + X2[3 * z + 2]) + X2[3 * z + 1];
+    });
+    // z: the ten moments
+    const R sz = Y00[0] + Y00[2];
+    const R m000 = sz + Y00[1], m001 = Y00[2] - Y00[0], m002 = minus_twice(sz, Y00[1]);
+    const R m100 = (Y10[0] + Y10[2]) + Y10[1], m101 = Y10[2] - Y10[0];
+    const R m010 = (Y01[0] + Y01[2]) + Y01[1], m011 = Y01[2] - Y01[0];
+    const R m110 = (Y11[0] + Y11[2]) + Y11[1];
+    const R m200 = (Y20[0] + Y20[2]) + Y20[1];
+    const R m020 = (Y02[0] + Y02[2]) + Y02[1];
+    // cell quantities (as mrt_pre) and the class overwrites
+    R drho = m000 * isc;
+    R rho = R(1) + drho;
+    const R inv = isc / rho;
+    R ux = m100 * inv, uy = m010 * inv, uz = m001 * inv;
+    if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 3);
+    const Mrt2Coef<R>& k = p.mrt2;
+    // non-equilibrium parts of the shear moments, scaled by (s_v - s_o) / |row|^2
+    const R rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
+    const R nsc = -sc, n3sc = R(-3) * sc;
+    const R q4 = rux * ux, q5 = ruy * uy, q6 = ruz * uz;
+    const R a = k.kxy * mad(nsc, rux * uy, m110);
+    const R b = k.kxy * mad(nsc, rux * uz, m101);
+    const R c = k.kxy * mad(nsc, ruy * uz, m011);
+    const R e8 = k.k8 * mad(n3sc, q4 - q5, m200 - m020);
+    const R e9 = k.k9 * mad(n3sc, minus_twice(q4 + q5, q6), minus_twice(m200 + m020, m002));
+    // shear correction of each direction class (even in c)
+    const R cfx = e8 + e9, cfy = e9 - e8, cfz = R(-2) * e9;
+    const R exy = e9 + e9, exz = e8 - e9;
+    // equilibrium parts per weight class: s_o w sc (drho + rho (4.5 eu^2 - 1.5 u^2)) +- s_o w sc 3 rho eu
+    const R nusq15 = R(-1.5) * mad(uz, uz, mad(uy, uy, ux * ux));
+    const R base = mad(rho, nusq15, drho);
+    R wb[4], w45[4], w3[4];
+    static_for<4>([&](auto Cc) {
+        constexpr int cc = Cc;
+        wb[cc] = k.sw[cc] * base;
+        if constexpr (cc > 0) {
+            w45[cc] = k.sw45[cc] * rho;
+            w3[cc] = k.sw3[cc] * rho;
+        }
+    });
+    const R om1 = k.om1;
+    out[0] = mad(om1, v[0], wb[0]);
+    static_for<27>([&](auto I) {
+        constexpr int i = I;
+        constexpr int o = L::opp(i);
+        if constexpr (i > 0 && i < o) {
+            constexpr int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
+            constexpr int nz = (cx != 0) + (cy != 0) + (cz != 0);  // 1 face, 2 edge, 3 corner
+            R eu = cx != 0 ? (cx == 1 ? ux : -ux) : (cy != 0 ? (cy == 1 ? uy : -uy) : (cz == 1 ? uz : -uz));
+            if constexpr (cx != 0 && cy == 1) eu = eu + uy;
+            if constexpr (cx != 0 && cy == -1) eu = eu - uy;
+            if constexpr ((cx != 0 || cy != 0) && cz == 1) eu = eu + uz;
+            if constexpr ((cx != 0 || cy != 0) && cz == -1) eu = eu - uz;
+            R corr;
+            if constexpr (nz == 1) {
+                corr = cx != 0 ? cfx : (cy != 0 ? cfy : cfz);
+            } else if constexpr (nz == 2) {
+                if constexpr (cz == 0)
+                    corr = cx * cy == 1 ? exy + a : exy - a;
+                else if constexpr (cy == 0)
+                    corr = cx * cz == 1 ? exz + b : exz - b;
+                else
+                    corr = cy * cz == 1 ? c - cfx : -(c + cfx);
+            } else {
+                const R t1 = cx * cy == 1 ? a : -a;
+                const R t2 = cx * cz == 1 ? t1 + b : t1 - b;
+                corr = cy * cz == 1 ? t2 + c : t2 - c;
+            }
+            const R sym = mad(w45[nz], eu * eu, wb[nz]) - corr;
+            const R anti = w3[nz] * eu;
+            out[i] = mad(om1, v[i], sym + anti);
+            out[o] = mad(om1, v[o], sym - anti);
+        }
+    });
+    if (fl & kEquilibrium) equilibrium_dev<L, false, R>(rho, drho, ux, uy, uz, sc, out);
+    if (fl & kBounce) {
+        static_for<26>([&](auto I) {
+            constexpr int i = I + 1;
+            out[L::opp(i)] = v[i];
+        });
+    }
+}
+
 template <int BASIS, class S>
 __global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D3Q27;
@@ -453,6 +577,29 @@ __global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepPa
             out[L::opp(i)] = v[i];
         });
     }
+    store_cell<L, S, false>(static_cast<S*>(p.fout), p, c, out);
+}
+
+// The plain (one thread per cell) step kernel of the two-rate collision.
+template <class S>
+__global__ void __launch_bounds__(256) k_step_mrt2(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
+    using L = D3Q27;
+    using R = typename Codec<S>::Real;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= p.nx) return;
+    const Rows<L> rows(blockIdx.y, blockIdx.z, p.nx, p.ny, p.nz);
+    const long long c = rows.base[1][1] + x;
+    const S* __restrict__ fin = static_cast<const S*>(p.fin);
+    R v[27];
+    pull<L, S, false>(fin, p, rows, x, v);
+    int cls;
+    uint32_t fl;
+    cell_class(p.mask, p.cls, c, cls, fl);
+    if (fl & kZeroGradXp) pull_zerograd<L, S, false>(fin, p, rows, x, v);
+    R sc, isc;
+    storage_scale<S>(p, sc, isc);
+    R out[27];
+    mrt2_collide(p, cls, fl, v, sc, isc, out);
     store_cell<L, S, false>(static_cast<S*>(p.fout), p, c, out);
 }
 

@@ -72,6 +72,12 @@ struct D3Q27 {
     }
     // Tensor slot of direction i: (cx+1) + 3 (cy+1) + 9 (cz+1).  Used by the factorised MRT.
     LBM_HD static constexpr int slot(int i) { return (cx(i) + 1) + 3 * (cy(i) + 1) + 9 * (cz(i) + 1); }
+    // The direction with velocity (x, y, z).
+    LBM_HD static constexpr int dir_of(int x, int y, int z) {
+        for (int i = 0; i < Q; ++i)
+            if (cx(i) == x && cy(i) == y && cz(i) == z) return i;
+        return -1;
+    }
 };
 
 }  // namespace lbm

@@ -166,6 +166,18 @@ struct MrtCoef {
     R alpha[27], beta[27], A[9], B[9];
 };
 
+// Coefficients of the two-rate Gram-Schmidt collision (mrt2_collide in kernels.cuh): every row relaxes
+// at s_o except the five shear rows (4-6: cx cy, cx cz, cy cz; 8, 9: the traceless second-order
+// mixes), which relax at s_v.  Storage units folded in (sc: the storage scale).
+//   om1        1 - s_o
+//   kxy, k8, k9  (s_v - s_o) / |row|^2 for the off-diagonal rows (12), row 8 (108 / 3) and row 9 (324 / 3)
+//   sw[c]      s_o w_c sc for the weight classes c = rest, face, edge, corner; sw45 = 4.5 sw, sw3 = 3 sw
+template <class R>
+struct Mrt2Coef {
+    R om1, kxy, k8, k9;
+    R sw[4], sw45[4], sw3[4];
+};
+
 // First quantity with a nonzero coefficient in the equilibrium moment of slot t (11: none).
 LBM_HD constexpr int mrt_meq_first(int basis, int t) {
     for (int k = 0; k < 11; ++k)

@@ -268,6 +268,8 @@ __device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t*
     R out[Q];
     if constexpr (COLL == 0) {
         bgk_collide<L, false, kExactWeights<S>>(p, cls, fl, v, sc, isc, out);
+    } else if constexpr (COLL == 3) {
+        mrt2_collide(p, cls, fl, v, sc, isc, out);
     } else {
         R T[27];
         static_for<27>([&](auto I) {
@@ -301,7 +303,8 @@ __device__ __forceinline__ void row_cell_wrap(const P& p, const S* st, const uin
     row_cell<L, S, SB, COLL>(p, st, mrow, x, xm, xp, x, x, sc, isc, orow);
 }
 
-// COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt).  Deviation arithmetic.
+// COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt), 3 = two-rate MRT (Gram-Schmidt,
+// mrt2_collide).  Deviation arithmetic.
 // Requires nx <= PITCH with nx * sizeof(S) a multiple of 16 bytes; `rows` = rows per group
 // (RowPipeShape::rows_per_group).  Block = CR x THREADS consumer threads + one producer warp.
 //   full[s]   tx-count barrier, completed by the bulk loads of stage s

@@ -136,6 +136,7 @@ struct lbm_ctx {
     bool has_prev = false;
     long long steps = 0;
     double scale = 1.0;
+    bool mrt2 = false;             // two-rate Gram-Schmidt MRT (mrt2_collide) in use
     StepParams<float> pf{};
     StepParams<double> pd{};
 };
@@ -179,8 +180,34 @@ static StepParams<R> make_params(const lbm_ctx* c) {
             p.mrt.A[t] = R(k.A[t]);
             p.mrt.B[t] = R(k.B[t] * es);
         }
+        if (c->mrt2) {
+            const double so = d.mrt_s[0], sv = d.mrt_s[4], dv = sv - so;
+            p.mrt2.om1 = R(1.0 - so);
+            p.mrt2.kxy = R(dv / 12.0);
+            p.mrt2.k8 = R(dv / 36.0);
+            p.mrt2.k9 = R(dv / 108.0);
+            const double wc[4] = {D3Q27::w(0), D3Q27::w(1), D3Q27::w(7), D3Q27::w(19)};  // rest, face, edge, corner
+            for (int k2 = 0; k2 < 4; ++k2) {
+                p.mrt2.sw[k2] = R(so * wc[k2] * es);
+                p.mrt2.sw45[k2] = R(4.5 * so * wc[k2] * es);
+                p.mrt2.sw3[k2] = R(3.0 * so * wc[k2] * es);
+            }
+        }
     }
     return p;
+}
+
+// The two-rate collision (mrt2_collide) applies: Gram-Schmidt basis, 16-bit storage, and rates with one
+// value on the shear rows 4-6, 8, 9 and one on every other row.
+static bool mrt2_applies(const lbm_desc& d) {
+    if (d.collision != LBM_MRT || d.mrt_basis != LBM_MRT_GRAM_SCHMIDT) return false;
+    if (d.storage != LBM_F16S && d.storage != LBM_BF16S) return false;
+    const double so = d.mrt_s[0], sv = d.mrt_s[4];
+    for (int r = 0; r < 27; ++r) {
+        const bool shear = r == 4 || r == 5 || r == 6 || r == 8 || r == 9;
+        if (d.mrt_s[r] != (shear ? sv : so)) return false;
+    }
+    return true;
 }
 
 template <class R>
@@ -272,7 +299,7 @@ static int prepare_rows_t(lbm_ctx* c) {
 // f(lattice tag, storage tag, collision constant, pitch constant)
 template <class F>
 static void dispatch_rows(const lbm_ctx* c, F&& f) {
-    const int coll = c->d.collision == LBM_BGK ? 0 : (c->d.mrt_basis == LBM_MRT_REF ? 1 : 2);
+    const int coll = c->d.collision == LBM_BGK ? 0 : c->mrt2 ? 3 : (c->d.mrt_basis == LBM_MRT_REF ? 1 : 2);
     auto by_pitch = [&](auto lt, auto st, auto co) {
         const long long nx = c->d.nx;
         if (nx <= 128)
@@ -291,7 +318,12 @@ static void dispatch_rows(const lbm_ctx* c, F&& f) {
             switch (coll) {
                 case 0: by_pitch(lt, st, std::integral_constant<int, 0>{}); break;
                 case 1: by_pitch(lt, st, std::integral_constant<int, 1>{}); break;
-                default: by_pitch(lt, st, std::integral_constant<int, 2>{}); break;
+                case 2: by_pitch(lt, st, std::integral_constant<int, 2>{}); break;
+                default:
+                    // the two-rate collision exists for 16-bit storage only (mrt2_applies)
+                    if constexpr (sizeof(typename decltype(st)::type) == 2)
+                        by_pitch(lt, st, std::integral_constant<int, 3>{});
+                    break;
             }
         }
     };
@@ -394,7 +426,9 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
                 }
                 break;
             case LBM_MRT:  // deviation arithmetic only (validate_desc)
-                if (c->d.mrt_basis == LBM_MRT_REF)
+                if (c->mrt2) {
+                    if constexpr (sizeof(S) == 2) k_step_mrt2<S><<<grid, blk, 0, s>>>(p);
+                } else if (c->d.mrt_basis == LBM_MRT_REF)
                     k_step_mrt<kMrtRef, S><<<grid, blk, 0, s>>>(p);
                 else
                     k_step_mrt<kMrtGramSchmidt, S><<<grid, blk, 0, s>>>(p);
@@ -644,6 +678,7 @@ int lbm_create(const lbm_desc* d, lbm_ctx** out) {
             return set_error(LBM_ERR_CUDA, "mask upload failed");
         }
     }
+    c->mrt2 = mrt2_applies(c->d);
     c->pf = make_params<float>(c);
     c->pd = make_params<double>(c);
     rc = lbm_init_equilibrium(c, nullptr, nullptr);

@@ -239,7 +239,7 @@ def test_duct3d_config_mode_parity():
 
 
 @pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.BF16S])
-@pytest.mark.parametrize("coll", ["bgk_cavity", "bgk_duct", "mrt_ref", "mrt_gs"])
+@pytest.mark.parametrize("coll", ["bgk_cavity", "bgk_duct", "mrt_ref", "mrt_gs", "mrt_gs_general"])
 def test_row_pipeline_equals_plain_kernel(storage, coll):
     """The bulk-copy row pipeline and the one-cell-per-thread kernel run the same collision code on
     the same inputs: results must be bit-identical (lid, solid, equilibrium-inlet, zero-gradient)."""
@@ -253,7 +253,9 @@ def test_row_pipeline_equals_plain_kernel(storage, coll):
                                 u=np.concatenate([np.where(solid, 0.0, 0.04), np.zeros(2 * m.size)]))
     else:
         basis = lb.MRT_REF if coll == "mrt_ref" else lb.MRT_GRAM_SCHMIDT
-        d = lb.make_desc(lb.D3Q27, lb.MRT, storage, (256, 9, 8), mrt_s=lb.mrt_rates(1.8, 1.2), mrt_basis=basis)
+        # two rates (16-bit storage: the two-rate collision) or three (the general one)
+        rates = lb.mrt_rates(1.8, 1.2) if coll != "mrt_gs_general" else lb.mrt_reference_rates()
+        d = lb.make_desc(lb.D3Q27, lb.MRT, storage, (256, 9, 8), mrt_s=rates, mrt_basis=basis)
         m = lb.setup_cavity3d(d, 0.05)
         F0 = np.repeat(lb.velocities(lb.D3Q27)[3], d.cells)
     out = {}
