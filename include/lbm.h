@@ -218,15 +218,18 @@ int  lbm_sums_fp64_noalloc(const void* populations, int lattice, int storage, in
                            int64_t nz, double storage_scale, void* stream, double out[4]);
 
 /* ---- batched ensemble -------------------------------------------------------------------
- * Many independent lattices (any mix of D2Q9/D3Q27 BGK, sizes and rates, one storage type)
- * advanced by one persistent kernel launch per lattice family and step over a work table (row
- * groups staged by bulk copies for members with nx a multiple of 16 up to 1024, one-thread-per-cell
- * tiles for the others); nsteps of those are captured in a CUDA graph and replayed.  Every member
+ * Many independent lattices (any mix of D2Q9/D3Q27 BGK, sizes and rates, one storage type) advanced
+ * together: every step is one persistent kernel launch over a work table that holds the row groups of
+ * all members of both families (staged by bulk copies; members with nx a multiple of 16 up to 1024),
+ * plus, only if some member's rows cannot be copied that way, one tile launch per family for those
+ * (one thread per cell).  nsteps of those are captured in a CUDA graph and replayed.  Every member
  * gives the same populations as stepping it alone.                                               */
 int  lbm_batch_create(const lbm_desc* descs, int n, lbm_batch** out);
 void lbm_batch_destroy(lbm_batch* b);
 int  lbm_batch_size(const lbm_batch* b);
 int  lbm_batch_step(lbm_batch* b, int64_t nsteps);
+/* Wait for the batch's stream; LBM_ERR_TIMEOUT (once; the error word is cleared) if a bounded wait of
+ * the row pipeline gave up. */
 int  lbm_batch_sync(lbm_batch* b);
 int  lbm_batch_get_populations(lbm_batch* b, int k, void* dst, int dtype, int memory);
 int  lbm_batch_set_populations(lbm_batch* b, int k, const void* src, int dtype, int memory);
@@ -236,12 +239,21 @@ int64_t lbm_batch_cells(const lbm_batch* b);
 void* lbm_batch_stream(lbm_batch* b);
 /* Tile shape chosen by the autotuner (cells per tile along x, tiles launched per step). */
 int  lbm_batch_tile_info(const lbm_batch* b, int* tile_x, int64_t* n_tiles);
-/* Work distribution: AUTO (default) times both on the first step; TILES steps every member with
- * the one-thread-per-cell tile kernel; ROWS uses the row pipeline for every eligible member.
+/* The configuration in use after the first step: kernel launches per step, and the per-direction copy
+ * size the autotuner chose for the one-launch row groups (D2Q9, D3Q27; 0 when not in that mode).     */
+int  lbm_batch_plan(const lbm_batch* b, int* launches_per_step, int* group_bytes_d2q9, int* group_bytes_d3q27);
+/* Work distribution: AUTO (default) times the candidates on the first step; TILES steps every member
+ * with the one-thread-per-cell tile kernel; ROWS uses one row-pipeline launch over the eligible members
+ * of both families; ROWS_PER_FAMILY one row-pipeline launch per family (kept for comparison).
  * lbm_batch_get_mode reports the choice in use (AUTO before the first step).                     */
-enum lbm_batch_mode { LBM_BATCH_AUTO = 0, LBM_BATCH_TILES = 1, LBM_BATCH_ROWS = 2 };
+enum lbm_batch_mode { LBM_BATCH_AUTO = 0, LBM_BATCH_TILES = 1, LBM_BATCH_ROWS = 2, LBM_BATCH_ROWS_PER_FAMILY = 3 };
 int  lbm_batch_set_mode(lbm_batch* b, int mode);
 int  lbm_batch_get_mode(const lbm_batch* b);
+/* Test hook of the row pipeline's bounded waits (no counterpart in the reference), as
+ * lbm_test_stall_next_step: the next lbm_batch_step launches one step on its own in which work item
+ * `item` of each row work table is never filled and every wait gives up after `wait_clocks` clocks;
+ * lbm_batch_sync then reports LBM_ERR_TIMEOUT once.  Needs a row mode in use (after a first step).  */
+int  lbm_batch_test_stall_next_step(lbm_batch* b, int64_t item, int64_t wait_clocks);
 
 /* ---- problem set-up helpers (the reference's loop-invariant state, layer L3) --------------
  * Each fills mask[N] (column-major) and the descriptor's class table so that the per-cell

@@ -51,6 +51,7 @@ pub const LBM_KERNEL_ROWS: c_int = 2;
 pub const LBM_BATCH_AUTO: c_int = 0;
 pub const LBM_BATCH_TILES: c_int = 1;
 pub const LBM_BATCH_ROWS: c_int = 2;
+pub const LBM_BATCH_ROWS_PER_FAMILY: c_int = 3;
 
 pub const LBM_MAX_CLASSES: usize = 16;
 pub const LBM_CELL_BOUNCE: u32 = 0x01;
@@ -154,8 +155,11 @@ extern "C" {
     pub fn lbm_batch_cells(b: *const lbm_batch) -> i64;
     pub fn lbm_batch_stream(b: *mut lbm_batch) -> *mut c_void;
     pub fn lbm_batch_tile_info(b: *const lbm_batch, tile_x: *mut c_int, n_tiles: *mut i64) -> c_int;
+    pub fn lbm_batch_plan(b: *const lbm_batch, launches_per_step: *mut c_int, group_bytes_d2q9: *mut c_int,
+                          group_bytes_d3q27: *mut c_int) -> c_int;
     pub fn lbm_batch_set_mode(b: *mut lbm_batch, mode: c_int) -> c_int;
     pub fn lbm_batch_get_mode(b: *const lbm_batch) -> c_int;
+    pub fn lbm_batch_test_stall_next_step(b: *mut lbm_batch, item: i64, wait_clocks: i64) -> c_int;
 
     pub fn lbm_setup_cavity2d(d: *mut lbm_desc, mask: *mut u8, u_lid: c_double) -> c_int;
     pub fn lbm_setup_cavity3d(d: *mut lbm_desc, mask: *mut u8, u_lid: c_double) -> c_int;

@@ -58,9 +58,9 @@ struct MemberCell {
     const ClassTable<R>& cls;
 };
 
-// One row group of one member: rows y0 .. y0 + nb - 1 at z.
+// One row group of one member: rows y0 .. y0 + nb - 1 at z; fam 0 = D2Q9, 1 = D3Q27.
 struct RowItem {
-    int lat, y0, z, nb;
+    int lat, y0, z, nb, fam;
 };
 
 // Shared memory of k_batch_rows: the row pipeline's stages plus one class table per stage.
@@ -74,7 +74,7 @@ constexpr size_t batch_rows_smem() {
 template <class L, class S, int PITCH>
 __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, RowPipeShape<L, S, PITCH>::CTAS)
     k_batch_rows(const BatchLattice<typename Codec<S>::Real>* __restrict__ lats, const RowItem* __restrict__ items,
-                 long long n_items, int parity, int* __restrict__ err) {
+                 long long n_items, int parity, int* __restrict__ err, const WaitLimits wl) {
     using R = typename Codec<S>::Real;
     using Sh = RowPipeShape<L, S, PITCH>;
     constexpr int Q = L::Q;
@@ -99,6 +99,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     const unsigned first = blockIdx.x, stride = gridDim.x, nit = (unsigned)n_items;
 
     auto issue = [&](unsigned g, int s) {
+        if (g == wl.skip) return;  // test hook: this item's stage is never filled
         const RowItem it = items[g];
         const BatchLattice<R>& m = lats[it.lat];
         const int nx = m.nx, ny = m.ny, nz = m.nz, nb = it.nb;
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
             if (first + s * stride < nit) issue(first + s * stride, s);
         for (unsigned k = 0; first + (k + NS) * stride < nit; ++k) {
             const int s = (int)(k % NS);
-            if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1))) {
+            if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1), wl.limit)) {
                 if (lane == 0) atomicExch(err, kRowPipeTimeout);
                 return;
             }
@@ -149,10 +150,12 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     for (unsigned k = 0; first + k * stride < nit; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
-        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1))) {
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1), wl.limit)) {
             if (lane == 0) atomicExch(err, kRowPipeTimeout);
             for (unsigned j = 1; j < NS && first + (k + j) * stride < nit; ++j)
-                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1), 1LL << 28)) break;
+                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1),
+                                       wl.limit < (1LL << 28) ? wl.limit : (1LL << 28)))
+                    break;
             return;
         }
         const RowItem it = items[g];
@@ -180,6 +183,145 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
             if (x >= nx) {
                 x -= nx;
                 ++b;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+    }
+}
+
+// The whole ensemble in one persistent launch: one work table holds the row groups of both lattice
+// families, and every CTA has the D3Q27 shape (RowPipeShape<D3Q27, S, PITCH>: consumer count, stage
+// size, stages).  A stage keeps 27 direction slots of SB elements; a D2Q9 group fills the first 9 (its
+// rows sized by the host so that nb * nx <= SB), a D3Q27 group all of them; the mask rows and the
+// member's class table follow as in k_batch_rows.  Lanes 0 .. Q-1 of the producer copy the directions,
+// lane 27 the mask rows, lane 28 the class table.  Each consumer runs the collision of the item's family
+// (both are compiled into the kernel; the register budget is D3Q27's).
+template <class S, int PITCH>
+__global__ void __launch_bounds__(RowPipeShape<D3Q27, S, PITCH>::CONSUMERS + 32, RowPipeShape<D3Q27, S, PITCH>::CTAS)
+    k_batch_rows_mix(const BatchLattice<typename Codec<S>::Real>* __restrict__ lats,
+                     const RowItem* __restrict__ items, long long n_items, int parity, int* __restrict__ err,
+                     const WaitLimits wl) {
+    using R = typename Codec<S>::Real;
+    using Sh = RowPipeShape<D3Q27, S, PITCH>;
+    constexpr int NS = Sh::NS;
+    constexpr int SB = Sh::SB;
+    constexpr int CONS = Sh::CONSUMERS;
+    constexpr int W = CONS / 32;
+    static_assert(NS <= 8, "barriers occupy the first 128 bytes");
+    static_assert(CONS + 32 <= 2048 && PITCH <= 1024, "the reciprocal quotients below need numerators < 2^11, nx <= 1024");
+    constexpr unsigned long long kCy3 = pack_c<D3Q27>(false), kCz3 = pack_c<D3Q27>(true), kCy2 = pack_c<D2Q9>(false);
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* empty = full + NS;
+    S* in = reinterpret_cast<S*>(smem + 128);                                  // [NS][27][SB]
+    uint8_t* mask_st = reinterpret_cast<uint8_t*>(in + (size_t)NS * 27 * SB);  // [NS][SB]
+    using CT = ClassTable<R>;
+    static_assert(sizeof(CT) % 16 == 0 && (Sh::smem_bytes() % 16) == 0, "class-table copies need 16-byte multiples");
+    CT* cls_st = reinterpret_cast<CT*>(smem + Sh::smem_bytes());               // [NS]
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const unsigned first = blockIdx.x, stride = gridDim.x, nit = (unsigned)n_items;
+
+    auto issue = [&](unsigned g, int s) {
+        if (g == wl.skip) return;  // test hook: this item's stage is never filled
+        const RowItem it = items[g];
+        const BatchLattice<R>& m = lats[it.lat];
+        const int nx = m.nx, ny = m.ny, nz = m.nz, nb = it.nb;
+        const int Q = it.fam ? 27 : 9;
+        const uint32_t row_bytes = (uint32_t)(nx * sizeof(S));
+        if (lane == 0)
+            mbar_arrive_expect_tx(&full[s], (uint32_t)(Q * nb) * row_bytes + (m.mask ? (uint32_t)(nb * nx) : 0u) +
+                                                (uint32_t)sizeof(CT));
+        __syncwarp();
+        if (lane < Q) {
+            const int cy = (int)(((it.fam ? kCy3 : kCy2) >> (2 * lane)) & 3) - 1;
+            const int cz = it.fam ? (int)((kCz3 >> (2 * lane)) & 3) - 1 : 0;
+            int zs = it.z - cz;
+            zs = zs < 0 ? zs + nz : (zs >= nz ? zs - nz : zs);
+            int ys = it.y0 - cy;
+            ys = ys < 0 ? ys + ny : (ys >= ny ? ys - ny : ys);
+            const int run = ny - ys < nb ? ny - ys : nb;
+            const S* plane = static_cast<const S*>(m.f[parity]) + (long long)lane * m.N + (long long)zs * ny * nx;
+            S* dst = in + ((long long)s * 27 + lane) * SB;
+            bulk_load(dst, plane + (long long)ys * nx, (uint32_t)run * row_bytes, &full[s]);
+            if (run < nb) bulk_load(dst + run * nx, plane, (uint32_t)(nb - run) * row_bytes, &full[s]);
+        } else if (lane == 27 && m.mask) {
+            bulk_load(mask_st + s * SB, m.mask + ((long long)it.z * ny + it.y0) * nx, (uint32_t)(nb * nx), &full[s]);
+        } else if (lane == 28) {
+            bulk_load(cls_st + s, &m.cls, (uint32_t)sizeof(CT), &full[s]);
+        }
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], W);
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid >= CONS) {  // producer warp
+        for (int s = 0; s < NS; ++s)
+            if (first + s * stride < nit) issue(first + s * stride, s);
+        for (unsigned k = 0; first + (k + NS) * stride < nit; ++k) {
+            const int s = (int)(k % NS);
+            if (!mbar_wait_bounded(&empty[s], (uint32_t)((k / NS) & 1), wl.limit)) {
+                if (lane == 0) atomicExch(err, kRowPipeTimeout);
+                return;
+            }
+            issue(first + (k + NS) * stride, s);
+        }
+        return;
+    }
+    for (unsigned k = 0; first + k * stride < nit; ++k) {
+        const unsigned g = first + k * stride;
+        const int s = (int)(k % NS);
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / NS) & 1), wl.limit)) {
+            if (lane == 0) atomicExch(err, kRowPipeTimeout);
+            for (unsigned j = 1; j < NS && first + (k + j) * stride < nit; ++j)
+                if (!mbar_wait_bounded(&full[(k + j) % NS], (uint32_t)(((k + j) / NS) & 1),
+                                       wl.limit < (1LL << 28) ? wl.limit : (1LL << 28)))
+                    break;
+            return;
+        }
+        const RowItem it = items[g];
+        const BatchLattice<R>& m = lats[it.lat];
+        const int nx = m.nx;
+        R sc, isc;
+        storage_scale<S>(m, sc, isc);
+        const MemberCell<R> mc{m.N, m.omega, m.one_m_omega, cls_st[s]};
+        const S* st = in + (long long)s * 27 * SB;
+        const uint8_t* ms = m.mask ? mask_st + s * SB : nullptr;
+        S* out0 = static_cast<S*>(m.f[parity ^ 1]) + ((long long)it.z * m.ny + it.y0) * nx;
+        // cells of the group, flattened (row b, column x), CONS apart (as k_batch_rows)
+        const float inv_nx = __frcp_rn((float)nx);
+        int b = (int)(((float)tid + 0.5f) * inv_nx), x = tid - b * nx;
+        const int cq = (int)(((float)CONS + 0.5f) * inv_nx), cr = CONS - cq * nx;
+        const int nb = it.nb;
+        if (it.fam) {
+#pragma unroll 1
+            while (b < nb) {
+                row_cell_wrap<D3Q27, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
+                                               out0 + (long long)b * nx);
+                x += cr;
+                b += cq;
+                if (x >= nx) {
+                    x -= nx;
+                    ++b;
+                }
+            }
+        } else {
+#pragma unroll 1
+            while (b < nb) {
+                row_cell_wrap<D2Q9, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
+                                              out0 + (long long)b * nx);
+                x += cr;
+                b += cq;
+                if (x >= nx) {
+                    x -= nx;
+                    ++b;
+                }
             }
         }
         __syncwarp();
@@ -225,7 +367,17 @@ struct lbm_batch {
     RowItem* items_d[2] = {nullptr, nullptr};
     long long n_items[2] = {0, 0};
     int rows_grid[2] = {0, 0};
+    // the one-launch table of both families (k_batch_rows_mix), used when `mixed`
+    bool mixed = false;
+    int mix_pitch = 0;
+    RowItem* mix_items_d = nullptr;
+    long long mix_n = 0;
+    int mix_grid = 0;
+    int group_bytes[2] = {0, 0};     // copy-size targets of its row groups (D2Q9, D3Q27)
     int* err = nullptr;              // device error word of the row pipeline
+    WaitLimits waits = kProductionWaits;  // wait limits of the next row-pipeline launches
+    bool stall_armed = false;        // lbm_batch_test_stall_next_step
+    WaitLimits stall = kProductionWaits;
 };
 
 namespace lbm {
@@ -271,6 +423,24 @@ static void batch_rows_dispatch(const lbm_batch* b, int fam, F&& f) {
         by_storage(BTag<D3Q27>{});
 }
 
+// f(storage tag, pitch constant) for the one-launch kernel (pitch b->mix_pitch)
+template <class F>
+static void batch_mix_dispatch(const lbm_batch* b, F&& f) {
+    auto by_pitch = [&](auto st) {
+        switch (b->mix_pitch) {
+            case 128: f(st, std::integral_constant<int, 128>{}); break;
+            case 256: f(st, std::integral_constant<int, 256>{}); break;
+            case 512: f(st, std::integral_constant<int, 512>{}); break;
+            default: f(st, std::integral_constant<int, 1024>{}); break;
+        }
+    };
+    switch (b->storage) {
+        case LBM_F32: by_pitch(BTag<float>{}); break;
+        case LBM_F16S: by_pitch(BTag<__half>{}); break;
+        default: by_pitch(BTag<__nv_bfloat16>{}); break;
+    }
+}
+
 // Work tables of the row pipeline: per family, the row groups of its eligible members.
 static int batch_build_rows(lbm_batch* b) {
     int sms = 0;
@@ -295,7 +465,7 @@ static int batch_build_rows(lbm_batch* b) {
                 const int rpg = Sh::rows_per_group((int)d.nx);
                 for (int z = 0; z < (int)d.nz; ++z)
                     for (int y0 = 0; y0 < (int)d.ny; y0 += rpg)
-                        items.push_back(RowItem{k, y0, z, (int)std::min<long long>(rpg, d.ny - y0)});
+                        items.push_back(RowItem{k, y0, z, (int)std::min<long long>(rpg, d.ny - y0), fam});
             }
             auto kern = k_batch_rows<L, S, PITCH>;
             constexpr size_t smem = batch_rows_smem<L, S, PITCH>();
@@ -322,6 +492,66 @@ static int batch_build_rows(lbm_batch* b) {
         }
         LBM_CK(cudaMemcpy(b->items_d[fam], items.data(), sizeof(RowItem) * items.size(), cudaMemcpyHostToDevice));
     }
+    return LBM_OK;
+}
+
+// The one-launch work table (k_batch_rows_mix): the row groups of every eligible member of both
+// families.  The stage pitch is the widest eligible row of the ensemble; a group's rows are sized for
+// `scale` times the per-family copy target (RowPipeShape::kGroupBytes, per direction) and never exceed a
+// stage (nb * nx <= SB).  The scale is the autotuner's cells-per-thread knob: a group of nb rows gives
+// each consumer thread nb * nx / CONSUMERS cells per stage.
+static int batch_build_mixed(lbm_batch* b, double scale) {
+    int sms = 0;
+    LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    long long maxnx = 0;
+    for (int k = 0; k < (int)b->descs.size(); ++k)
+        if (batch_row_member(b, k)) maxnx = std::max<long long>(maxnx, b->descs[k].nx);
+    if (!maxnx) return set_error(LBM_ERR_UNSUPPORTED, "no member fits the row pipeline");
+    b->mix_pitch = pitch_for(maxnx);
+    std::vector<RowItem> items;
+    int rc = LBM_OK;
+    auto build = [&](auto st, auto pi) {
+        using S = typename decltype(st)::type;
+        constexpr int PITCH = decltype(pi)::value;
+        using Sh = RowPipeShape<D3Q27, S, PITCH>;
+        const int target[2] = {(int)(RowPipeShape<D2Q9, S, PITCH>::kGroupBytes * scale), (int)(Sh::kGroupBytes * scale)};
+        b->group_bytes[0] = target[0];
+        b->group_bytes[1] = target[1];
+        for (int k = 0; k < (int)b->descs.size(); ++k) {
+            if (!batch_row_member(b, k)) continue;
+            const lbm_desc& d = b->descs[k];
+            const int fam = d.lattice == LBM_D2Q9 ? 0 : 1;
+            int rpg = target[fam] / (int)(d.nx * sizeof(S));
+            rpg = std::max(1, std::min<int>(rpg, (int)(Sh::SB / d.nx)));
+            for (int z = 0; z < (int)d.nz; ++z)
+                for (int y0 = 0; y0 < (int)d.ny; y0 += rpg)
+                    items.push_back(RowItem{k, y0, z, (int)std::min<long long>(rpg, d.ny - y0), fam});
+        }
+        auto kern = k_batch_rows_mix<S, PITCH>;
+        constexpr size_t smem = batch_rows_smem<D3Q27, S, PITCH>();
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            rc = set_error(LBM_ERR_CUDA, "row pipeline shared-memory attribute");
+            return;
+        }
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, smem) != cudaSuccess ||
+            per_sm < 1) {
+            rc = set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
+            return;
+        }
+        b->mix_grid = (int)std::min<long long>((long long)items.size(), (long long)per_sm * sms);
+    };
+    batch_mix_dispatch(b, build);
+    if (rc) return rc;
+    if (items.size() >= (1ull << 31)) return set_error(LBM_ERR_UNSUPPORTED, "row work table over 2^31 items");
+    if (b->mix_items_d) cudaFree(b->mix_items_d);
+    b->mix_items_d = nullptr;
+    b->mix_n = (long long)items.size();
+    if (cudaMalloc(&b->mix_items_d, sizeof(RowItem) * items.size()) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(LBM_ERR_NOMEM, "row work table allocation failed");
+    }
+    LBM_CK(cudaMemcpy(b->mix_items_d, items.data(), sizeof(RowItem) * items.size(), cudaMemcpyHostToDevice));
     return LBM_OK;
 }
 
@@ -362,6 +592,17 @@ static void batch_launch(lbm_batch* b, int parity, cudaStream_t s) {
             k_batch_bgk<D3Q27, S><<<(unsigned)b->n_tiles[1], b->tile_x, 0, s>>>(lats, b->tiles_d[1], parity);
     });
     if (!b->use_rows) return;
+    if (b->mixed) {
+        batch_mix_dispatch(b, [&](auto st, auto pi) {
+            using S = typename decltype(st)::type;
+            using R = typename Codec<S>::Real;
+            constexpr int PITCH = decltype(pi)::value;
+            using Sh = RowPipeShape<D3Q27, S, PITCH>;
+            k_batch_rows_mix<S, PITCH><<<b->mix_grid, Sh::CONSUMERS + 32, batch_rows_smem<D3Q27, S, PITCH>(), s>>>(
+                static_cast<const BatchLattice<R>*>(b->lats_d), b->mix_items_d, b->mix_n, parity, b->err, b->waits);
+        });
+        return;
+    }
     for (int fam = 0; fam < 2; ++fam) {
         if (!b->n_items[fam]) continue;
         batch_rows_dispatch(b, fam, [&](auto lt, auto st, auto pi) {
@@ -371,7 +612,8 @@ static void batch_launch(lbm_batch* b, int parity, cudaStream_t s) {
             using Sh = RowPipeShape<L, S, decltype(pi)::value>;
             k_batch_rows<L, S, decltype(pi)::value><<<b->rows_grid[fam], Sh::CONSUMERS + 32,
                                                       batch_rows_smem<L, S, decltype(pi)::value>(), s>>>(
-                static_cast<const BatchLattice<R>*>(b->lats_d), b->items_d[fam], b->n_items[fam], parity, b->err);
+                static_cast<const BatchLattice<R>*>(b->lats_d), b->items_d[fam], b->n_items[fam], parity, b->err,
+                b->waits);
         });
     }
 }
@@ -394,9 +636,15 @@ static int batch_build_graphs(lbm_batch* b) {
     return LBM_OK;
 }
 
-// Configuration: time one step of each candidate (reads the current buffers, writes the others):
-// the tile kernel alone at tile widths 64/128/256, then the row pipeline for the eligible members
-// with the best tile width for the rest.  LBM_BATCH_* modes in lbm_batch_set_mode pin a choice.
+// Configuration: time a step of each candidate on the real buffers (reads the current buffers, writes
+// the others) and keep the fastest.  The candidates are the halo strategy and the cells per thread:
+//   - tiles: every member on the one-thread-per-cell tile kernel (halos read straight from global
+//     memory through L1/L2), tile widths 64 / 128 / 256;
+//   - rows, one launch: the eligible members' row groups staged by bulk copies (halos in shared memory)
+//     in one work table of both families (k_batch_rows_mix), group sizes 0.5x / 1x / 2x the per-family
+//     copy target (the cells each consumer thread takes per stage), the best tile width for the rest;
+//   - rows per family: one row-pipeline launch per lattice family (k_batch_rows), for comparison.
+// lbm_batch_set_mode pins TILES, ROWS (one launch) or ROWS_PER_FAMILY.
 static int batch_autotune(lbm_batch* b) {
     cudaEvent_t e0, e1;
     LBM_CK(cudaEventCreate(&e0));
@@ -414,37 +662,66 @@ static int batch_autotune(lbm_batch* b) {
     for (int k = 0; k < (int)b->descs.size(); ++k) any_rows = any_rows || batch_row_member(b, k);
     float best = 1e30f;
     int best_tx = 128;
-    bool best_rows = false;
-    if (b->mode != LBM_BATCH_ROWS || !any_rows) {
-        b->use_rows = false;
-        for (int tx : {64, 128, 256}) {
-            int rc = batch_build_tiles(b, tx);
+    int best_kind = 0;  // 0 tiles, 1 rows (one launch), 2 rows per family
+    double best_scale = 1.0;
+    int rc = LBM_OK;
+    b->use_rows = false;
+    b->mixed = false;
+    for (int tx : {64, 128, 256}) {
+        if (b->mode != LBM_BATCH_AUTO && b->mode != LBM_BATCH_TILES && tx != 128) continue;
+        rc = batch_build_tiles(b, tx);
+        float ms = 0;
+        if (!rc) rc = time_step(ms);
+        if (rc) return rc;
+        if (ms < best && (b->mode == LBM_BATCH_AUTO || b->mode == LBM_BATCH_TILES || !any_rows)) {
+            best = ms;
+            best_tx = tx;
+        }
+    }
+    if (any_rows && (b->mode == LBM_BATCH_AUTO || b->mode == LBM_BATCH_ROWS)) {
+        b->use_rows = true;
+        b->mixed = true;
+        if ((rc = batch_build_tiles(b, best_tx))) return rc;
+        for (double scale : {0.5, 1.0, 2.0}) {
+            rc = batch_build_mixed(b, scale);
             float ms = 0;
             if (!rc) rc = time_step(ms);
             if (rc) return rc;
-            if (ms < best) {
+            if (ms < best || (b->mode == LBM_BATCH_ROWS && best_kind != 1)) {
                 best = ms;
-                best_tx = tx;
+                best_kind = 1;
+                best_scale = scale;
             }
         }
     }
-    if (any_rows && b->mode != LBM_BATCH_TILES) {
+    if (any_rows && (b->mode == LBM_BATCH_AUTO || b->mode == LBM_BATCH_ROWS_PER_FAMILY)) {
         b->use_rows = true;
-        int rc = batch_build_rows(b);
+        b->mixed = false;
+        rc = batch_build_rows(b);
         if (!rc) rc = batch_build_tiles(b, best_tx);
         float ms = 0;
         if (!rc) rc = time_step(ms);
         if (rc) return rc;
-        if (ms < best || b->mode == LBM_BATCH_ROWS) {
+        if (ms < best || (b->mode == LBM_BATCH_ROWS_PER_FAMILY && best_kind != 2)) {
             best = ms;
-            best_rows = true;
+            best_kind = 2;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     LBM_CK(cudaGetLastError());
-    b->use_rows = best_rows;
+    b->use_rows = best_kind != 0;
+    b->mixed = best_kind == 1;
+    if (best_kind == 1 && (rc = batch_build_mixed(b, best_scale))) return rc;
+    if (best_kind == 2 && (rc = batch_build_rows(b))) return rc;
     return batch_build_tiles(b, best_tx);
+}
+
+// Kernel launches per step of the configuration in use.
+static int batch_launches(const lbm_batch* b) {
+    int n = (b->n_tiles[0] > 0) + (b->n_tiles[1] > 0);
+    if (b->use_rows) n += b->mixed ? (b->mix_n > 0) : (b->n_items[0] > 0) + (b->n_items[1] > 0);
+    return n;
 }
 
 static void batch_free(lbm_batch* b) {
@@ -458,6 +735,7 @@ static void batch_free(lbm_batch* b) {
     cudaFree(b->tiles_d[1]);
     cudaFree(b->items_d[0]);
     cudaFree(b->items_d[1]);
+    cudaFree(b->mix_items_d);
     cudaFree(b->err);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -576,6 +854,15 @@ int lbm_batch_step(lbm_batch* b, int64_t nsteps) {
         if (rc) return rc;
     }
     long long n = nsteps;
+    if (b->stall_armed) {
+        // the armed test stall: one direct launch with its wait limits, before any graph
+        b->stall_armed = false;
+        b->waits = b->stall;
+        batch_launch(b, b->parity, b->stream);
+        b->waits = kProductionWaits;
+        b->parity ^= 1;
+        --n;
+    }
     if (n >= 2) {
         if (!b->gsteps) {
             int rc = batch_build_graphs(b);
@@ -603,13 +890,37 @@ int lbm_batch_sync(lbm_batch* b) {
     LBM_CK(cudaStreamSynchronize(b->stream));
     int e = 0;
     LBM_CK(cudaMemcpy(&e, b->err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) return set_error(LBM_ERR_TIMEOUT, "a row-pipeline barrier wait ran out (the step did not complete)");
+    if (e) {
+        LBM_CK(cudaMemset(b->err, 0, sizeof(int)));
+        return set_error(LBM_ERR_TIMEOUT, "a row-pipeline barrier wait ran out (the step did not complete)");
+    }
+    return LBM_OK;
+}
+
+int lbm_batch_test_stall_next_step(lbm_batch* b, int64_t item, int64_t wait_clocks) {
+    if (!b) return set_error(LBM_ERR_INVALID, "batch is NULL");
+    if (item < 0 || item >= 0xffffffffLL) return set_error(LBM_ERR_INVALID, "work item out of range");
+    if (wait_clocks < (1LL << 10) || wait_clocks > (1LL << 32))
+        return set_error(LBM_ERR_INVALID, "wait_clocks must be in [2^10, 2^32]");
+    if (!b->tile_x || !b->use_rows)
+        return set_error(LBM_ERR_STATE, "the stall applies to the row pipeline: step once in a row mode first");
+    b->stall = WaitLimits{(unsigned)item, (long long)wait_clocks};
+    b->stall_armed = true;
+    return LBM_OK;
+}
+
+int lbm_batch_plan(const lbm_batch* b, int* launches_per_step, int* group_bytes_d2q9, int* group_bytes_d3q27) {
+    if (!b) return set_error(LBM_ERR_INVALID, "batch is NULL");
+    if (launches_per_step) *launches_per_step = b->tile_x ? batch_launches(b) : 0;
+    if (group_bytes_d2q9) *group_bytes_d2q9 = b->mixed ? b->group_bytes[0] : 0;
+    if (group_bytes_d3q27) *group_bytes_d3q27 = b->mixed ? b->group_bytes[1] : 0;
     return LBM_OK;
 }
 
 int lbm_batch_set_mode(lbm_batch* b, int mode) {
     if (!b) return set_error(LBM_ERR_INVALID, "batch is NULL");
-    if (mode != LBM_BATCH_AUTO && mode != LBM_BATCH_TILES && mode != LBM_BATCH_ROWS)
+    if (mode != LBM_BATCH_AUTO && mode != LBM_BATCH_TILES && mode != LBM_BATCH_ROWS &&
+        mode != LBM_BATCH_ROWS_PER_FAMILY)
         return set_error(LBM_ERR_INVALID, "unknown batch mode");
     LBM_CK(cudaSetDevice(b->device));
     LBM_CK(cudaStreamSynchronize(b->stream));
@@ -622,7 +933,7 @@ int lbm_batch_set_mode(lbm_batch* b, int mode) {
 int lbm_batch_get_mode(const lbm_batch* b) {
     if (!b) return set_error(LBM_ERR_INVALID, "batch is NULL");
     if (!b->tile_x) return LBM_BATCH_AUTO;
-    return b->use_rows ? LBM_BATCH_ROWS : LBM_BATCH_TILES;
+    return !b->use_rows ? LBM_BATCH_TILES : b->mixed ? LBM_BATCH_ROWS : LBM_BATCH_ROWS_PER_FAMILY;
 }
 
 int lbm_batch_get_populations(lbm_batch* b, int k, void* dst, int dtype, int memory) {

@@ -35,7 +35,7 @@ STORAGE_BYTES = {F32: 4, F16S: 2, BF16S: 2, F64: 8}  # bytes of one stored popul
 MRT_REF, MRT_GRAM_SCHMIDT = 0, 1
 ARITH_DEVIATION, ARITH_ABSOLUTE = 0, 1
 KERNEL_AUTO, KERNEL_PLAIN, KERNEL_ROWS = 0, 1, 2
-BATCH_AUTO, BATCH_TILES, BATCH_ROWS = 0, 1, 2
+BATCH_AUTO, BATCH_TILES, BATCH_ROWS, BATCH_ROWS_PER_FAMILY = 0, 1, 2, 3
 DTYPE_F32, DTYPE_F64 = 0, 1
 HOST, DEVICE = 0, 1
 BOUNCE, SET_RHO, SET_UX, SET_UY, SET_UZ, EQUILIBRIUM, ZEROGRAD_XP = 1, 2, 4, 8, 16, 32, 64
@@ -131,6 +131,8 @@ _SIGS = {
     "lbm_batch_cells": (C.c_int64, [_P]),
     "lbm_batch_stream": (_P, [_P]),
     "lbm_batch_tile_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
+    "lbm_batch_plan": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "lbm_batch_test_stall_next_step": (C.c_int, [_P, C.c_int64, C.c_int64]),
     "lbm_setup_cavity2d": (C.c_int, [_DP, _P, C.c_double]),
     "lbm_setup_cavity3d": (C.c_int, [_DP, _P, C.c_double]),
     "lbm_setup_channel2d": (C.c_int, [_DP, _P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]),
@@ -495,11 +497,22 @@ class Batch:
         return lib().lbm_batch_stream(self._h) or 0
 
     def set_mode(self, mode: int):
-        """BATCH_AUTO (time both), BATCH_TILES (tile kernel only) or BATCH_ROWS (row pipeline)."""
+        """BATCH_AUTO (time the candidates), BATCH_TILES (tile kernel only), BATCH_ROWS (one row-pipeline
+        launch for both families) or BATCH_ROWS_PER_FAMILY (one row-pipeline launch per family)."""
         _check(lib().lbm_batch_set_mode(self._h, mode))
 
     def mode(self) -> int:
         return lib().lbm_batch_get_mode(self._h)
+
+    def plan(self):
+        """(kernel launches per step, D2Q9 and D3Q27 row-group copy bytes of the one-launch mode)."""
+        n, g2, g3 = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().lbm_batch_plan(self._h, C.byref(n), C.byref(g2), C.byref(g3)))
+        return n.value, g2.value, g3.value
+
+    def test_stall_next_step(self, item: int = 0, wait_clocks: int = 1 << 21):
+        """Test hook: the next step leaves row work item `item` unfilled (lbm_batch_test_stall_next_step)."""
+        _check(lib().lbm_batch_test_stall_next_step(self._h, item, wait_clocks))
 
     def tile_info(self):
         tx = C.c_int()

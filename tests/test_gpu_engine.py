@@ -162,7 +162,7 @@ def test_external_stream():
         assert np.array_equal(lat2.get_populations(np.float32), a)
 
 
-@pytest.mark.parametrize("mode", [lb.BATCH_TILES, lb.BATCH_ROWS])
+@pytest.mark.parametrize("mode", [lb.BATCH_TILES, lb.BATCH_ROWS, lb.BATCH_ROWS_PER_FAMILY])
 @pytest.mark.parametrize("storage", [lb.F32, lb.F16S])
 def test_batch_equals_individual_lattices(storage, mode):
     """Every member of a batch (tile kernel, or row pipeline for the members whose rows the bulk copies
@@ -201,8 +201,9 @@ def test_batch_equals_individual_lattices(storage, mode):
     b.close()
 
 
+@pytest.mark.parametrize("mode", [lb.BATCH_ROWS, lb.BATCH_ROWS_PER_FAMILY])
 @pytest.mark.parametrize("storage", [lb.F32, lb.BF16S])
-def test_batch_rows_many_groups_equal_individual(storage):
+def test_batch_rows_many_groups_equal_individual(storage, mode):
     """Row-pipeline batch with ~10x more row groups than resident CTAs (every CTA cycles its stage ring
     over groups of different members and widths): each member equals the lattice stepped alone."""
     members = []
@@ -213,10 +214,12 @@ def test_batch_rows_many_groups_equal_individual(storage):
         d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (n, n), omega=1.7)
         members.append((d, lb.setup_cavity2d(d, 0.1)))
     b = lb.Batch([x[0] for x in members], [x[1] for x in members])
-    b.set_mode(lb.BATCH_ROWS)
+    b.set_mode(mode)
     b.step(9)
     b.sync()
-    assert b.mode() == lb.BATCH_ROWS
+    assert b.mode() == mode
+    # every member's rows can be copied: one launch per step in the one-launch mode
+    assert b.plan()[0] == (1 if mode == lb.BATCH_ROWS else 2)
     for k, (d, m) in enumerate(members):
         with lb.Lattice(d, m) as lat:
             lat.step(9)
@@ -431,3 +434,39 @@ def test_row_pipeline_needs_eligible_shape():
     d, m, F0 = cavity3d(n=(112, 8, 8), storage=lb.F16S)
     a, b = _rows_vs_plain(d, m, F0, 7)
     assert np.array_equal(a, b)
+
+
+def test_batch_one_launch_autotuned_and_stall_recovers():
+    """AUTO picks among tiles, one launch for both families and one launch per family; a stalled row
+    stage (test hook) makes lbm_batch_sync report LBM_ERR_TIMEOUT once, and the batch steps on
+    correctly after its populations are set again."""
+    members = []
+    for n in (64, 128):
+        d, m, F0 = cavity2d(n=n, u_lid=0.1, re=300, storage=lb.F16S)
+        members.append((d, m, F0))
+    d, m, F0 = cavity3d(n=(64, 24, 20), u_lid=0.05, omega=1.2, storage=lb.F16S)
+    members.append((d, m, F0))
+    b = lb.Batch([x[0] for x in members], [x[1] for x in members])
+    for k, (_, _, F0) in enumerate(members):
+        b.set_populations(k, np.asarray(F0, dtype=np.float64))
+    b.step(2)
+    b.sync()
+    assert b.mode() in (lb.BATCH_TILES, lb.BATCH_ROWS, lb.BATCH_ROWS_PER_FAMILY)
+    b.set_mode(lb.BATCH_ROWS)
+    b.step(1)
+    b.sync()
+    launches, g2, g3 = b.plan()
+    assert launches == 1 and g2 > 0 and g3 > 0
+    b.test_stall_next_step(item=3, wait_clocks=1 << 21)
+    b.step(2)
+    assert lb.lib().lbm_batch_sync(b._h) == -8
+    assert lb.lib().lbm_batch_sync(b._h) == 0
+    for k, (_, _, F0) in enumerate(members):
+        b.set_populations(k, np.asarray(F0, dtype=np.float64))
+    b.step(21)
+    for k, (d, m, F0) in enumerate(members):
+        with lb.Lattice(d, m) as lat:
+            lat.set_populations(np.asarray(F0, dtype=np.float64))
+            lat.step(21)
+            assert np.array_equal(b.get_populations(k, np.float32), lat.get_populations(np.float32)), k
+    b.close()
