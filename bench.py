@@ -439,10 +439,13 @@ def start_shanchen(lb, lat, d, m, rho0=0.693, amp=0.01, seed=2):
     lat.init_equilibrium(rho0 + rng.uniform(-amp, amp, d.cells))
 
 
-def acc_run(lb, wl, storage, steps, start=None, shape=None, hook=None):
-    """One run of a workload from its start state; returns fields, FP64 mass before/after, family."""
+def acc_run(lb, wl, storage, steps, start=None, shape=None, hook=None, nearest=False):
+    """One run of a workload from its start state; returns fields, FP64 mass before/after, family.
+    nearest: 16-bit storage rounds to nearest instead of stochastically (the default)."""
     fn = WORKLOADS[wl][0]
     d, m = fn(lb, storage, shape) if shape is not None else fn(lb, storage)
+    if nearest:
+        d.rounding = lb.ROUND_NEAREST
     with lb.Lattice(d, m) as lat:
         if start:
             start(lb, lat, d, m)
@@ -479,6 +482,7 @@ def acc_cavity128(lb):
     runs = {}
     for name, st in (("f64", lb.F64), ("f32", lb.F32), ("f16s", lb.F16S)):
         runs[name] = acc_run(lb, "d2q9_lid_128", st, 10000)
+    runs["f16s_nearest"] = acc_run(lb, "d2q9_lid_128", lb.F16S, 10000, nearest=True)
     d, m = wl_cavity128(lb, lb.F32)
     d.arithmetic = lb.ARITH_ABSOLUTE
     with lb.Lattice(d, m) as lat:
@@ -487,7 +491,7 @@ def acc_cavity128(lb):
         rho, u = lat.macros()
         runs["f32_reference_arithmetic"] = {"d": d, "m": m, "rho": rho, "u": u, "mass0": m0,
                                             "mass1": lat.sums()[0], "family": "plain"}
-    out = field_errors(lb, runs, "f64", ["f32", "f16s", "f32_reference_arithmetic"])
+    out = field_errors(lb, runs, "f64", ["f32", "f16s", "f16s_nearest", "f32_reference_arithmetic"])
     out["steps"] = 10000
     return out
 
@@ -528,11 +532,13 @@ def acc_channel(lb, steps=50000):
     runs = {}
     for name, st in (("f64", lb.F64), ("f32", lb.F32), ("f16s", lb.F16S)):
         runs[name] = acc_run(lb, "d2q9_channel_1024x256", st, steps, start=start_channel, hook=channel_hook(probe))
-    out = field_errors(lb, runs, "f64", ["f32", "f16s"])
+    runs["f16s_nearest"] = acc_run(lb, "d2q9_channel_1024x256", lb.F16S, steps, start=start_channel,
+                                   hook=channel_hook(probe), nearest=True)
+    out = field_errors(lb, runs, "f64", ["f32", "f16s", "f16s_nearest"])
     d, m = runs["f64"]["d"], runs["f64"]["m"]
     keep = np.tile(~solid_cells(lb, d, m), 2)
     ref = runs["f64"]["extra"]["u_mean"][keep]
-    for name in ("f32", "f16s"):
+    for name in ("f32", "f16s", "f16s_nearest"):
         out[f"rel_l2_u_mean_{name}_vs_f64"] = rel_l2(runs[name]["extra"]["u_mean"][keep], ref)
     for name, r in runs.items():
         T = shedding_period(r["extra"]["probe"], r["extra"]["every"])
@@ -567,7 +573,8 @@ def acc_shanchen(lb, steps=20000):
     runs = {}
     for name, st in (("f64", lb.F64), ("f32", lb.F32), ("bf16s", lb.BF16S)):
         runs[name] = acc_run(lb, "d2q9_shanchen_1024", st, steps, start=start_shanchen)
-    out = field_errors(lb, runs, "f64", ["f32", "bf16s"])
+    runs["bf16s_nearest"] = acc_run(lb, "d2q9_shanchen_1024", lb.BF16S, steps, start=start_shanchen, nearest=True)
+    out = field_errors(lb, runs, "f64", ["f32", "bf16s", "bf16s_nearest"])
     for name, r in runs.items():
         out[f"stats_{name}"] = sc_statistics(r["rho"], 1024)
     out["steps"] = steps
@@ -579,7 +586,8 @@ def acc_mrt256(lb, steps=5000, shape=(256, 256, 256)):
     runs = {}
     for name, st in (("f64", lb.F64), ("f32", lb.F32), ("f16s", lb.F16S)):
         runs[name] = acc_run(lb, "d3q27_mrt_gs_lid_256", st, steps, shape=shape)
-    out = field_errors(lb, runs, "f64", ["f32", "f16s"])
+    runs["f16s_nearest"] = acc_run(lb, "d3q27_mrt_gs_lid_256", lb.F16S, steps, shape=shape, nearest=True)
+    out = field_errors(lb, runs, "f64", ["f32", "f16s", "f16s_nearest"])
     out["steps"] = steps
     out["lattice"] = "x".join(map(str, shape))
     return out

@@ -28,7 +28,7 @@ static int layout(void) {
     FIELD(lbm_desc, storage);
     FIELD(lbm_desc, mrt_basis);
     FIELD(lbm_desc, arithmetic);
-    FIELD(lbm_desc, reserved0);
+    FIELD(lbm_desc, rounding);
     FIELD(lbm_desc, nx);
     FIELD(lbm_desc, ny);
     FIELD(lbm_desc, nz);

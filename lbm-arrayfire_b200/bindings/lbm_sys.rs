@@ -41,6 +41,8 @@ pub const LBM_MRT_REF: c_int = 0;
 pub const LBM_MRT_GRAM_SCHMIDT: c_int = 1;
 pub const LBM_ARITH_DEVIATION: c_int = 0;
 pub const LBM_ARITH_ABSOLUTE: c_int = 1;
+pub const LBM_ROUND_STOCHASTIC: c_int = 0;
+pub const LBM_ROUND_NEAREST: c_int = 1;
 pub const LBM_DTYPE_F32: c_int = 0;
 pub const LBM_DTYPE_F64: c_int = 1;
 pub const LBM_HOST: c_int = 0;
@@ -82,7 +84,7 @@ pub struct lbm_desc {
     pub storage: i32,
     pub mrt_basis: i32,
     pub arithmetic: i32,
-    pub reserved0: i32,
+    pub rounding: i32,
     pub nx: i64,
     pub ny: i64,
     pub nz: i64,
@@ -190,7 +192,7 @@ const _: () = assert!(std::mem::offset_of!(lbm_desc, collision) == 4);
 const _: () = assert!(std::mem::offset_of!(lbm_desc, storage) == 8);
 const _: () = assert!(std::mem::offset_of!(lbm_desc, mrt_basis) == 12);
 const _: () = assert!(std::mem::offset_of!(lbm_desc, arithmetic) == 16);
-const _: () = assert!(std::mem::offset_of!(lbm_desc, reserved0) == 20);
+const _: () = assert!(std::mem::offset_of!(lbm_desc, rounding) == 20);
 const _: () = assert!(std::mem::offset_of!(lbm_desc, nx) == 24);
 const _: () = assert!(std::mem::offset_of!(lbm_desc, ny) == 32);
 const _: () = assert!(std::mem::offset_of!(lbm_desc, nz) == 40);

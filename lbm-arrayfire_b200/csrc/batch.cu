@@ -1,14 +1,17 @@
 // batch.cu — an ensemble of independent BGK lattices (any mix of D2Q9 and D3Q27 extents and
-// rates, one storage type) advanced together.  Each step is one persistent kernel per lattice family
-// over a work table, so lattices of very different sizes share the SMs without per-lattice launches:
-//   - row pipeline (k_batch_rows): items are (lattice, first row, z, rows) groups staged in shared
-//     memory by bulk copies, for members whose rows the copies can move (nx a multiple of 16, at most
-//     1024); the shared-memory row pitch is the family's widest such row, narrower members put more
-//     rows into a stage and every consumer thread takes cells of the flattened group;
+// rates, one storage type) advanced together, so lattices of very different sizes share the SMs
+// without per-lattice launches.  Each step is one persistent kernel over a work table:
+//   - row pipeline, one launch (k_batch_rows_mix): items are (lattice, first row, z, rows, family)
+//     groups of both lattice families staged in shared memory by bulk copies, for the members whose
+//     rows the copies can move (nx a multiple of 16, at most 1024); the stage pitch is the widest such
+//     row, narrower members put more rows into a stage and every consumer thread takes cells of the
+//     flattened group;
+//   - row pipeline per family (k_batch_rows): the same with one launch and table per lattice family
+//     (kept for comparison);
 //   - tile kernel (k_batch_bgk): a tile is one row segment (lattice, y, z, x0) of `tile_x` cells, one
 //     thread per cell, for the other members (or all of them, if the autotuner finds that faster).
-// Chunks of steps are captured in a CUDA graph and replayed.  The autotuner times the tile widths and
-// the row pipeline on the real buffers.
+// Chunks of steps are captured in a CUDA graph and replayed.  The autotuner times the candidates on
+// the real buffers.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -30,8 +33,19 @@ struct BatchLattice {
     long long N;
     R omega, one_m_omega;
     R scale, inv_scale;
+    int sr;                         // 16-bit storage: stochastic rounding (1) or to nearest (0)
     alignas(16) ClassTable<R> cls;  // 16-byte aligned: the row pipeline bulk-copies it into shared memory
 };
+
+// The batch's rounding seed for a launch reading buffer `parity` (one counter pair for the whole batch,
+// advanced once per step; a member stepped alone from the same start draws the same words).
+template <class S>
+__device__ __forceinline__ uint32_t batch_seed(unsigned* tick, int parity, bool designated) {
+    if constexpr (!Codec<S>::kScaled)
+        return 0u;
+    else
+        return step_seed(tick, parity, designated);
+}
 
 struct Tile {
     int lat, y, z, x0;
@@ -39,13 +53,17 @@ struct Tile {
 
 template <class L, class S>
 __global__ void __launch_bounds__(256) k_batch_bgk(const BatchLattice<typename Codec<S>::Real>* __restrict__ lats,
-                                                   const Tile* __restrict__ tiles, int parity) {
+                                                   const Tile* __restrict__ tiles, int parity, unsigned* tick,
+                                                   int advance) {
     using R = typename Codec<S>::Real;
     const Tile t = tiles[blockIdx.x];
     const BatchLattice<R>& p = lats[t.lat];
     const int x = t.x0 + threadIdx.x;
+    // every launch of a step reads the counter; the first one (advance) moves it on
+    const uint32_t seed = batch_seed<S>(tick, parity, advance && (blockIdx.x | threadIdx.x) == 0);
     if (x >= p.nx) return;
-    bgk_cell<L, S, false>(p, static_cast<const S*>(p.f[parity]), static_cast<S*>(p.f[parity ^ 1]), x, t.y, t.z);
+    bgk_cell<L, S, false>(p, static_cast<const S*>(p.f[parity]), static_cast<S*>(p.f[parity ^ 1]), x, t.y, t.z,
+                          Rounding{seed, p.sr != 0});
 }
 
 // A member's per-cell parameters for one row group: the scalars in registers (the stores of the group
@@ -74,7 +92,8 @@ constexpr size_t batch_rows_smem() {
 template <class L, class S, int PITCH>
 __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, RowPipeShape<L, S, PITCH>::CTAS)
     k_batch_rows(const BatchLattice<typename Codec<S>::Real>* __restrict__ lats, const RowItem* __restrict__ items,
-                 long long n_items, int parity, int* __restrict__ err, const WaitLimits wl) {
+                 long long n_items, int parity, int* __restrict__ err, const WaitLimits wl, unsigned* tick,
+                 int advance) {
     using R = typename Codec<S>::Real;
     using Sh = RowPipeShape<L, S, PITCH>;
     constexpr int Q = L::Q;
@@ -147,6 +166,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         }
         return;
     }
+    const uint32_t seed = batch_seed<S>(tick, parity, advance && (blockIdx.x | tid) == 0);
     for (unsigned k = 0; first + k * stride < nit; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
@@ -167,6 +187,8 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         const S* st = in + (long long)s * Q * SB;
         const uint8_t* ms = m.mask ? mask_st + s * SB : nullptr;
         S* out0 = static_cast<S*>(m.f[parity ^ 1]) + ((long long)it.z * m.ny + it.y0) * nx;
+        const uint32_t cell0 = (uint32_t)(((long long)it.z * m.ny + it.y0) * nx);
+        const Rounding rnd{seed, m.sr != 0};
         // cells of the group, flattened (row b, column x), CONS apart.  tid / nx and CONS / nx by a
         // float reciprocal: exact here (numerators below 2^11, nx <= 1024: the quotient's distance to
         // the next integer, at least 1/(2 nx), is far above the rounding error)
@@ -177,7 +199,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
 #pragma unroll 1
         while (b < nb) {
             row_cell_wrap<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
-                                       out0 + (long long)b * nx);
+                                       out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
             x += cr;
             b += cq;
             if (x >= nx) {
@@ -201,7 +223,7 @@ template <class S, int PITCH>
 __global__ void __launch_bounds__(RowPipeShape<D3Q27, S, PITCH>::CONSUMERS + 32, RowPipeShape<D3Q27, S, PITCH>::CTAS)
     k_batch_rows_mix(const BatchLattice<typename Codec<S>::Real>* __restrict__ lats,
                      const RowItem* __restrict__ items, long long n_items, int parity, int* __restrict__ err,
-                     const WaitLimits wl) {
+                     const WaitLimits wl, unsigned* tick, int advance) {
     using R = typename Codec<S>::Real;
     using Sh = RowPipeShape<D3Q27, S, PITCH>;
     constexpr int NS = Sh::NS;
@@ -274,6 +296,7 @@ __global__ void __launch_bounds__(RowPipeShape<D3Q27, S, PITCH>::CONSUMERS + 32,
         }
         return;
     }
+    const uint32_t seed = batch_seed<S>(tick, parity, advance && (blockIdx.x | tid) == 0);
     for (unsigned k = 0; first + k * stride < nit; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
@@ -294,6 +317,8 @@ __global__ void __launch_bounds__(RowPipeShape<D3Q27, S, PITCH>::CONSUMERS + 32,
         const S* st = in + (long long)s * 27 * SB;
         const uint8_t* ms = m.mask ? mask_st + s * SB : nullptr;
         S* out0 = static_cast<S*>(m.f[parity ^ 1]) + ((long long)it.z * m.ny + it.y0) * nx;
+        const uint32_t cell0 = (uint32_t)(((long long)it.z * m.ny + it.y0) * nx);
+        const Rounding rnd{seed, m.sr != 0};
         // cells of the group, flattened (row b, column x), CONS apart (as k_batch_rows)
         const float inv_nx = __frcp_rn((float)nx);
         int b = (int)(((float)tid + 0.5f) * inv_nx), x = tid - b * nx;
@@ -303,7 +328,7 @@ __global__ void __launch_bounds__(RowPipeShape<D3Q27, S, PITCH>::CONSUMERS + 32,
 #pragma unroll 1
             while (b < nb) {
                 row_cell_wrap<D3Q27, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
-                                               out0 + (long long)b * nx);
+                                               out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
                 x += cr;
                 b += cq;
                 if (x >= nx) {
@@ -315,7 +340,7 @@ __global__ void __launch_bounds__(RowPipeShape<D3Q27, S, PITCH>::CONSUMERS + 32,
 #pragma unroll 1
             while (b < nb) {
                 row_cell_wrap<D2Q9, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
-                                              out0 + (long long)b * nx);
+                                              out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
                 x += cr;
                 b += cq;
                 if (x >= nx) {
@@ -375,6 +400,7 @@ struct lbm_batch {
     int mix_grid = 0;
     int group_bytes[2] = {0, 0};     // copy-size targets of its row groups (D2Q9, D3Q27)
     int* err = nullptr;              // device error word of the row pipeline
+    unsigned* tick = nullptr;        // the rounding's step counter pair (device)
     WaitLimits waits = kProductionWaits;  // wait limits of the next row-pipeline launches
     bool stall_armed = false;        // lbm_batch_test_stall_next_step
     WaitLimits stall = kProductionWaits;
@@ -581,15 +607,22 @@ static int batch_build_tiles(lbm_batch* b, int tile_x) {
     return LBM_OK;
 }
 
+// One step of the whole ensemble: the tile launches (members the row copies cannot move), then the row
+// pipeline.  The first launch of the step advances the rounding counter (`advance`).
 static void batch_launch(lbm_batch* b, int parity, cudaStream_t s) {
+    int advance = 1;
     batch_dispatch(b->storage, [&](auto tag) {
         using S = typename decltype(tag)::type;
         using R = typename Codec<S>::Real;
         const auto* lats = static_cast<const BatchLattice<R>*>(b->lats_d);
         if (b->n_tiles[0])
-            k_batch_bgk<D2Q9, S><<<(unsigned)b->n_tiles[0], b->tile_x, 0, s>>>(lats, b->tiles_d[0], parity);
+            k_batch_bgk<D2Q9, S><<<(unsigned)b->n_tiles[0], b->tile_x, 0, s>>>(lats, b->tiles_d[0], parity, b->tick,
+                                                                             advance);
+        advance = advance && !b->n_tiles[0];
         if (b->n_tiles[1])
-            k_batch_bgk<D3Q27, S><<<(unsigned)b->n_tiles[1], b->tile_x, 0, s>>>(lats, b->tiles_d[1], parity);
+            k_batch_bgk<D3Q27, S><<<(unsigned)b->n_tiles[1], b->tile_x, 0, s>>>(lats, b->tiles_d[1], parity, b->tick,
+                                                                              advance);
+        advance = advance && !b->n_tiles[1];
     });
     if (!b->use_rows) return;
     if (b->mixed) {
@@ -599,7 +632,8 @@ static void batch_launch(lbm_batch* b, int parity, cudaStream_t s) {
             constexpr int PITCH = decltype(pi)::value;
             using Sh = RowPipeShape<D3Q27, S, PITCH>;
             k_batch_rows_mix<S, PITCH><<<b->mix_grid, Sh::CONSUMERS + 32, batch_rows_smem<D3Q27, S, PITCH>(), s>>>(
-                static_cast<const BatchLattice<R>*>(b->lats_d), b->mix_items_d, b->mix_n, parity, b->err, b->waits);
+                static_cast<const BatchLattice<R>*>(b->lats_d), b->mix_items_d, b->mix_n, parity, b->err, b->waits,
+                b->tick, advance);
         });
         return;
     }
@@ -613,7 +647,8 @@ static void batch_launch(lbm_batch* b, int parity, cudaStream_t s) {
             k_batch_rows<L, S, decltype(pi)::value><<<b->rows_grid[fam], Sh::CONSUMERS + 32,
                                                       batch_rows_smem<L, S, decltype(pi)::value>(), s>>>(
                 static_cast<const BatchLattice<R>*>(b->lats_d), b->items_d[fam], b->n_items[fam], parity, b->err,
-                b->waits);
+                b->waits, b->tick, advance);
+            advance = 0;
         });
     }
 }
@@ -737,6 +772,7 @@ static void batch_free(lbm_batch* b) {
     cudaFree(b->items_d[1]);
     cudaFree(b->mix_items_d);
     cudaFree(b->err);
+    cudaFree(b->tick);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -778,7 +814,9 @@ int lbm_batch_create(const lbm_desc* descs, int n, lbm_batch** out) {
         batch_free(b);
         return set_error(LBM_ERR_CUDA, "stream creation failed");
     }
-    if (cudaMalloc(&b->err, sizeof(int)) != cudaSuccess || cudaMemset(b->err, 0, sizeof(int)) != cudaSuccess) {
+    if (cudaMalloc(&b->err, sizeof(int)) != cudaSuccess || cudaMemset(b->err, 0, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->tick, 2 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(b->tick, 0, 2 * sizeof(unsigned)) != cudaSuccess) {
         cudaGetLastError();
         batch_free(b);
         return set_error(LBM_ERR_NOMEM, "error word allocation failed");
@@ -803,6 +841,7 @@ int lbm_batch_create(const lbm_desc* descs, int n, lbm_batch** out) {
             const double sc = d.storage_scale > 0 ? d.storage_scale : default_scale(d.storage);
             L.scale = R(sc);
             L.inv_scale = R(1.0 / sc);
+            L.sr = d.rounding == LBM_ROUND_STOCHASTIC ? 1 : 0;
             for (int c = 0; c < kMaxClasses; ++c) {
                 const bool used = c < d.n_classes;
                 L.cls.flags[c] = used ? d.classes[c].flags : 0u;

@@ -44,6 +44,9 @@ struct StepParams {
     R* psi;               // Shan-Chen psi field (N)
     R* rho_out;           // macro kernel outputs
     R* u_out;
+    unsigned* tick;       // the step counter pair of the rounding (see step_rounding)
+    int parity;           // the input buffer of this launch: it reads tick[parity], writes tick[parity ^ 1]
+    int sr;               // 16-bit storage: 1 stochastic rounding, 0 round to nearest
     ClassTable<R> cls;
     MrtCoef<R> mrt;
     Mrt2Coef<R> mrt2;
@@ -273,15 +276,75 @@ __device__ __forceinline__ void equilibrium(R rho, R ux, R uy, R uz, R (&feq)[L:
     });
 }
 
-template <class L, class S, bool ABS, class P, class R>
-__device__ __forceinline__ void store_cell(S* __restrict__ fout, const P& p, long long c, const R (&out)[L::Q]) {
-    static_for<L::Q>([&](auto I) {
-        constexpr int i = I;
-        if constexpr (ABS)
-            Codec<S>::store(fout + (long long)i * p.N + c, out[i], R(L::w(i)), R(p.scale));
+// How a launch rounds 16-bit stores: to nearest, or stochastically (sr) with random words hashed from
+// the cell index and the step.  The step index lives on the device as a pair tick[2]: a launch reading
+// buffer `parity` takes t = tick[parity] and one designated thread writes tick[parity ^ 1] = t + 1,
+// which only the next launch reads.  Steps replayed from a CUDA graph, single launches, the autotuner's
+// trial launches (they rewrite the same t + 1) and every kernel family therefore round with the same
+// random words for the same step and cell: results stay bit-identical across them.
+struct Rounding {
+    uint32_t seed;
+    bool sr;
+};
+// The step's seed for a launch reading buffer `parity` (advances the counter pair, see above).
+__device__ __forceinline__ uint32_t step_seed(unsigned* tick, int parity, bool designated) {
+    const unsigned t = tick[parity];
+    if (designated) tick[parity ^ 1] = t + 1u;
+    return mix32(t * 0x9e3779b9u + 0x7f4a7c15u);
+}
+template <class S>
+__device__ __forceinline__ Rounding step_rounding(unsigned* tick, int parity, int sr, bool designated) {
+    if constexpr (!Codec<S>::kScaled) {
+        return Rounding{0u, false};
+    } else {
+        if (!sr) return Rounding{0u, false};
+        return Rounding{step_seed(tick, parity, designated), true};
+    }
+}
+
+// The 16-bit store of a cell's outputs (raw, storage units) at fo[i * N]: directions in pairs through
+// one paired conversion; stochastic rounding draws one 32-bit word per pair from the cell's hash.
+template <class L, class S, class R>
+__device__ __forceinline__ void store16(S* __restrict__ fo, long long N, const R (&out)[L::Q], const Rounding& rnd,
+                                        uint32_t cell) {
+    constexpr int NP = (L::Q + 1) / 2;
+    auto put = [&](auto K, uint32_t w) {
+        constexpr int i = 2 * decltype(K)::value, j = i + 1;
+        fo[(long long)i * N] = Pair16<S>::hi(w);
+        if constexpr (j < L::Q) fo[(long long)j * N] = Pair16<S>::lo(w);
+    };
+    auto second = [&](auto K) -> float {
+        constexpr int j = 2 * decltype(K)::value + 1;
+        if constexpr (j < L::Q)
+            return out[j];
         else
-            fout[(long long)i * p.N + c] = Codec<S>::enc(out[i], R(L::w(i)));
-    });
+            return 0.0f;
+    };
+    if (rnd.sr) {
+        const uint32_t h = mix32(cell ^ rnd.seed);
+        static_for<NP>([&](auto K) {
+            constexpr uint32_t salt = 0x9e3779b9u * (uint32_t)(decltype(K)::value + 1);
+            put(K, Pair16<S>::rs(out[2 * K], second(K), h ^ salt));
+        });
+    } else {
+        static_for<NP>([&](auto K) { put(K, Pair16<S>::rn(out[2 * K], second(K))); });
+    }
+}
+
+template <class L, class S, bool ABS, class P, class R>
+__device__ __forceinline__ void store_cell(S* __restrict__ fout, const P& p, long long c, const R (&out)[L::Q],
+                                           const Rounding& rnd) {
+    if constexpr (!ABS && Codec<S>::kScaled) {
+        store16<L, S>(fout + c, p.N, out, rnd, (uint32_t)c);
+    } else {
+        static_for<L::Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (ABS)
+                Codec<S>::store(fout + (long long)i * p.N + c, out[i], R(L::w(i)), R(p.scale));
+            else
+                fout[(long long)i * p.N + c] = Codec<S>::enc(out[i], R(L::w(i)));
+        });
+    }
 }
 
 // Storage scale and its inverse for raw deviations: the codec's scale for the 16-bit codecs,
@@ -336,7 +399,7 @@ __device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, co
 // member of an ensemble).
 template <class L, class S, bool ABS, class P>
 __device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, S* __restrict__ fout, int x, int y,
-                                         int z) {
+                                         int z, const Rounding& rnd) {
     using R = typename Codec<S>::Real;
     const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
     const long long c = rows.base[1][1] + x;
@@ -350,14 +413,16 @@ __device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, 
     storage_scale<S>(p, sc, isc);
     R out[L::Q];
     bgk_collide<L, ABS, kExactWeights<S>>(p, cls, fl, v, sc, isc, out);
-    store_cell<L, S, ABS>(fout, p, c, out);
+    store_cell<L, S, ABS>(fout, p, c, out, rnd);
 }
 
 template <class L, class S, bool ABS>
 __global__ void __launch_bounds__(512) k_step_bgk(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
-    bgk_cell<L, S, ABS>(p, static_cast<const S*>(p.fin), static_cast<S*>(p.fout), x, blockIdx.y, blockIdx.z);
+    const bool designated = (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0;
+    const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, designated);
+    bgk_cell<L, S, ABS>(p, static_cast<const S*>(p.fin), static_cast<S*>(p.fout), x, blockIdx.y, blockIdx.z, rnd);
 }
 
 // ---- MRT (D3Q27) -------------------------------------------------------------------------
@@ -577,7 +642,9 @@ __global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepPa
             out[L::opp(i)] = v[i];
         });
     }
-    store_cell<L, S, false>(static_cast<S*>(p.fout), p, c, out);
+    const bool designated = (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0;
+    const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, designated);
+    store_cell<L, S, false>(static_cast<S*>(p.fout), p, c, out, rnd);
 }
 
 // The plain (one thread per cell) step kernel of the two-rate collision.
@@ -600,7 +667,9 @@ __global__ void __launch_bounds__(256) k_step_mrt2(const __grid_constant__ StepP
     storage_scale<S>(p, sc, isc);
     R out[27];
     mrt2_collide(p, cls, fl, v, sc, isc, out);
-    store_cell<L, S, false>(static_cast<S*>(p.fout), p, c, out);
+    const bool designated = (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0;
+    const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, designated);
+    store_cell<L, S, false>(static_cast<S*>(p.fout), p, c, out, rnd);
 }
 
 // ---- Shan-Chen (D2Q9) --------------------------------------------------------------------
@@ -686,7 +755,7 @@ __device__ __forceinline__ void sc_force(const StepParams<R>& p, const Rows<D2Q9
 // bounce-back, store.
 template <class S, bool ABS, class R>
 __device__ __forceinline__ void sc_collide_store(const StepParams<R>& p, long long c, const R (&v)[9], int cls,
-                                                 uint32_t fl, R Fx, R Fy) {
+                                                 uint32_t fl, R Fx, R Fy, const Rounding& rnd) {
     using L = D2Q9;
     R sc, isc;
     storage_scale<S>(p, sc, isc);
@@ -712,7 +781,7 @@ __device__ __forceinline__ void sc_collide_store(const StepParams<R>& p, long lo
             out[L::opp(i)] = v[i];
         });
     }
-    store_cell<L, S, ABS>(static_cast<S*>(p.fout), p, c, out);
+    store_cell<L, S, ABS>(static_cast<S*>(p.fout), p, c, out, rnd);
 }
 
 // Second pass of the two-pass Shan-Chen step (psi from k_sc_psi in global memory).
@@ -734,7 +803,9 @@ __global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepPar
     if (fl & kZeroGradXp) pull_zerograd<L, S, ABS>(fin, p, rows, x, v);
     R Fx, Fy;
     sc_force(p, rows, x, c, Fx, Fy);
-    sc_collide_store<S, ABS>(p, c, v, cls, fl, Fx, Fy);
+    const bool designated = (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0;
+    const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, designated);
+    sc_collide_store<S, ABS>(p, c, v, cls, fl, Fx, Fy, rnd);
 }
 
 // The whole Shan-Chen step in one pass, as a window sliding down y.  A CTA owns a strip of kScwTX
@@ -787,6 +858,7 @@ __global__ void __launch_bounds__(kScwTX, sizeof(typename Codec<S>::Real) == 8 ?
         if (own_x && y >= ys && y < ye) p.psi[c] = ps;
         if (tx < 2) ring[y & 3][le] = sc_psi_from<S, ABS>(p, w, c2, f2);
     };
+    const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, (blockIdx.x | blockIdx.y | threadIdx.x) == 0);
     R vc[9], vn[9];
     int cc = 0, cn = 0;
     uint32_t fc = 0, fn = 0;
@@ -800,7 +872,7 @@ __global__ void __launch_bounds__(kScwTX, sizeof(typename Codec<S>::Real) == 8 ?
             const long long c = (long long)y * nx + x;
             R Fx, Fy;
             sc_force_from(p, [&](int dx, int dy) { return ring[(y + dy) & 3][tx + 1 + dx]; }, Fx, Fy);
-            sc_collide_store<S, ABS>(p, c, vc, cc, fc, Fx, Fy);
+            sc_collide_store<S, ABS>(p, c, vc, cc, fc, Fx, Fy, rnd);
         }
         static_for<9>([&](auto I) { vc[I] = vn[I]; });
         cc = cn;

@@ -247,7 +247,7 @@ constexpr int kSegPitch = 1024;
 template <class L, class S, int SB, int COLL, class P>
 __device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t* mrow, int x, int xm, int xp,
                                          int mi, int ox, typename Codec<S>::Real sc, typename Codec<S>::Real isc,
-                                         S* orow) {
+                                         S* orow, const Rounding& rnd, uint32_t cell) {
     using R = typename Codec<S>::Real;
     constexpr int Q = L::Q;
     R v[Q];
@@ -288,19 +288,24 @@ __device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t*
         }
     }
     S* __restrict__ fo = orow + ox;
-    static_for<Q>([&](auto I) {
-        constexpr int i = I;
-        fo[(long long)i * p.N] = Codec<S>::enc(out[i], R(L::w(i)));
-    });
+    if constexpr (Codec<S>::kScaled) {
+        store16<L, S>(fo, p.N, out, rnd, cell);
+    } else {
+        static_for<Q>([&](auto I) {
+            constexpr int i = I;
+            fo[(long long)i * p.N] = Codec<S>::enc(out[i], R(L::w(i)));
+        });
+    }
 }
 
-// A cell of a whole staged row of width nx (periodic in x).
+// A cell of a whole staged row of width nx (periodic in x); row0: the cell index of the row's x = 0.
 template <class L, class S, int SB, int COLL, class P>
 __device__ __forceinline__ void row_cell_wrap(const P& p, const S* st, const uint8_t* mrow, int x, int nx,
-                                              typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow) {
+                                              typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow,
+                                              const Rounding& rnd, uint32_t row0) {
     const int xm = x == 0 ? nx - 1 : x - 1;
     const int xp = x == nx - 1 ? 0 : x + 1;
-    row_cell<L, S, SB, COLL>(p, st, mrow, x, xm, xp, x, x, sc, isc, orow);
+    row_cell<L, S, SB, COLL>(p, st, mrow, x, xm, xp, x, x, sc, isc, orow, rnd, row0 + (uint32_t)x);
 }
 
 // COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt), 3 = two-rate MRT (Gram-Schmidt,
@@ -389,6 +394,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
 
     R sc, isc;
     storage_scale<S>(p, sc, isc);
+    const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, (blockIdx.x | tid) == 0);
     // cells of a group flattened (row b, column x; staged index b * nx + x), CONSUMERS apart and
     // continued across stages: the cells one stage leaves over go to other threads in the next
     const int cq = Sh::CONSUMERS / nx, cr = Sh::CONSUMERS - cq * nx;
@@ -410,10 +416,11 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         const S* st0 = in + (long long)s * Q * SB;
         const uint8_t* ms0 = has_mask ? mask_st + s * SB : nullptr;
         S* out0 = static_cast<S*>(p.fout) + ((long long)z * ny + y0) * nx;
+        const uint32_t cell0 = (uint32_t)(((long long)z * ny + y0) * nx);
 #pragma unroll 1
         while (b < nb) {
             row_cell_wrap<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, x, nx, sc, isc,
-                                          out0 + (long long)b * nx);
+                                          out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
             x += cr;
             b += cq;
             if (x >= nx) {
@@ -521,6 +528,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
     }
     R sc, isc;
     storage_scale<S>(p, sc, isc);
+    const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, (blockIdx.x | tid) == 0);
     for (unsigned k = 0; first + k * stride < groups; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
@@ -539,9 +547,11 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
         const S* st = in + (long long)s * Q * SB + H;  // staged index of x0 is 0
         const uint8_t* mrow = has_mask ? mask_st + s * SB : nullptr;
         S* orow = static_cast<S*>(p.fout) + (long long)row * nx + x0;
+        const uint32_t cell0 = (uint32_t)((long long)row * nx + x0);
 #pragma unroll 1
         for (int xl = tid; xl < w; xl += Sh::CONSUMERS)
-            row_cell<L, S, SB, COLL>(p, st, mrow, xl, xl - 1, xl + 1, xl, xl, sc, isc, orow);
+            row_cell<L, S, SB, COLL>(p, st, mrow, xl, xl - 1, xl + 1, xl, xl, sc, isc, orow, rnd,
+                                     cell0 + (uint32_t)xl);
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
     }

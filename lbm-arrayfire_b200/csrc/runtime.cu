@@ -128,6 +128,7 @@ struct lbm_ctx {
     int rows_grid = 0;             // persistent grid of the row pipeline
     int rows_rpg = 1;              // its rows per group (segmented rows: the segment width)
     int* err = nullptr;            // device error word of the row pipeline
+    unsigned* tick = nullptr;      // the rounding's step counter pair (step_rounding)
     WaitLimits waits = kProductionWaits;  // the row pipeline's wait limits for the next launch
     bool stall_armed = false;      // lbm_test_stall_next_step: the next step launches with `stall`
     WaitLimits stall = kProductionWaits;
@@ -158,6 +159,8 @@ static StepParams<R> make_params(const lbm_ctx* c) {
     p.inv_scale = R(1.0 / c->scale);
     p.G = R(d.sc_G);
     p.psi = static_cast<R*>(c->psi);
+    p.tick = c->tick;
+    p.sr = d.rounding == LBM_ROUND_STOCHASTIC ? 1 : 0;
     for (int k = 0; k < kMaxClasses; ++k) {
         const bool used = k < d.n_classes;
         p.cls.flags[k] = used ? d.classes[k].flags : 0u;
@@ -382,6 +385,7 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
             StepParams<R> p = params_of<R>(c);
             p.fin = c->f[from];
             p.fout = c->f[from ^ 1];
+            p.parity = from;
             const int h = c->rows_rpg;
             const dim3 wg((unsigned)((c->d.nx + kScwTX - 1) / kScwTX), (unsigned)((c->d.ny + h - 1) / h), 1);
             if (abs_arith)
@@ -399,6 +403,7 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
             StepParams<R> p = params_of<R>(c);
             p.fin = c->f[from];
             p.fout = c->f[from ^ 1];
+            p.parity = from;
             launch_rows_t<L, S, decltype(pi)::value, decltype(co)::value>(c, p, s);
         });
         return;
@@ -410,6 +415,7 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
         StepParams<R> p = params_of<R>(c);
         p.fin = c->f[from];
         p.fout = c->f[from ^ 1];
+        p.parity = from;
         const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
         switch (c->d.collision) {
             case LBM_BGK:
@@ -593,6 +599,7 @@ static void destroy_ctx(lbm_ctx* c) {
     cudaFree(c->partial);
     cudaFree(c->sums_out);
     cudaFree(c->err);
+    cudaFree(c->tick);
     if (c->e0) cudaEventDestroy(c->e0);
     if (c->e1) cudaEventDestroy(c->e1);
     if (c->own) cudaStreamDestroy(c->own);
@@ -652,7 +659,9 @@ int lbm_create(const lbm_desc* d, lbm_ctx** out) {
     bool ok = cudaMalloc(&c->f[0], fbytes) == cudaSuccess && cudaMalloc(&c->f[1], fbytes) == cudaSuccess &&
               cudaMalloc(&c->partial, sizeof(Sums) * c->reduce_blocks) == cudaSuccess &&
               cudaMalloc(&c->sums_out, sizeof(Sums)) == cudaSuccess &&
-              cudaMalloc(&c->err, sizeof(int)) == cudaSuccess && cudaMemset(c->err, 0, sizeof(int)) == cudaSuccess;
+              cudaMalloc(&c->err, sizeof(int)) == cudaSuccess && cudaMemset(c->err, 0, sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&c->tick, 2 * sizeof(unsigned)) == cudaSuccess &&
+              cudaMemset(c->tick, 0, 2 * sizeof(unsigned)) == cudaSuccess;
     if (ok && d->mask) ok = cudaMalloc(&c->mask, (size_t)c->N) == cudaSuccess;
     if (ok && d->collision == LBM_SHANCHEN)
         ok = cudaMalloc(&c->psi, (size_t)c->N * (d->storage == LBM_F64 ? 8 : 4)) == cudaSuccess;

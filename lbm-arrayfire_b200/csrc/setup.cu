@@ -49,6 +49,8 @@ int validate_desc(const lbm_desc* d) {
         return set_error(LBM_ERR_INVALID, "unknown MRT basis");
     if (d->arithmetic != LBM_ARITH_DEVIATION && d->arithmetic != LBM_ARITH_ABSOLUTE)
         return set_error(LBM_ERR_INVALID, "unknown arithmetic mode");
+    if (d->rounding != LBM_ROUND_STOCHASTIC && d->rounding != LBM_ROUND_NEAREST)
+        return set_error(LBM_ERR_INVALID, "unknown rounding mode");
     if (d->arithmetic == LBM_ARITH_ABSOLUTE && d->storage != LBM_F32 && d->storage != LBM_F64)
         return set_error(LBM_ERR_UNSUPPORTED, "absolute arithmetic needs F32 or F64 storage");
     if (d->arithmetic == LBM_ARITH_ABSOLUTE && d->collision == LBM_MRT)

@@ -23,7 +23,7 @@ __all__ = [
     "MRT_REF", "MRT_GRAM_SCHMIDT", "BOUNCE", "SET_RHO", "SET_UX", "SET_UY", "SET_UZ",
     "EQUILIBRIUM", "ZEROGRAD_XP", "velocities", "omega_from_re", "mrt_reference_rates", "mrt_rates",
     "mrt_collide_host", "setup_cavity2d", "setup_cavity3d", "setup_channel2d", "setup_duct3d",
-    "mask_from_index_list", "EXPORTED_SYMBOLS",
+    "mask_from_index_list", "EXPORTED_SYMBOLS", "ROUND_STOCHASTIC", "ROUND_NEAREST",
 ]
 
 LIB_PATH = Path(os.environ.get("LBM_B200_LIB", Path(__file__).resolve().parent / "liblbm_b200.so"))
@@ -34,6 +34,7 @@ F32, F16S, BF16S, F64 = 0, 1, 2, 3
 STORAGE_BYTES = {F32: 4, F16S: 2, BF16S: 2, F64: 8}  # bytes of one stored population
 MRT_REF, MRT_GRAM_SCHMIDT = 0, 1
 ARITH_DEVIATION, ARITH_ABSOLUTE = 0, 1
+ROUND_STOCHASTIC, ROUND_NEAREST = 0, 1
 KERNEL_AUTO, KERNEL_PLAIN, KERNEL_ROWS = 0, 1, 2
 BATCH_AUTO, BATCH_TILES, BATCH_ROWS, BATCH_ROWS_PER_FAMILY = 0, 1, 2, 3
 DTYPE_F32, DTYPE_F64 = 0, 1
@@ -59,7 +60,7 @@ class CellClass(C.Structure):
 class Desc(C.Structure):
     _fields_ = [
         ("lattice", C.c_int32), ("collision", C.c_int32), ("storage", C.c_int32), ("mrt_basis", C.c_int32),
-        ("arithmetic", C.c_int32), ("reserved0", C.c_int32),
+        ("arithmetic", C.c_int32), ("rounding", C.c_int32),
         ("nx", C.c_int64), ("ny", C.c_int64), ("nz", C.c_int64),
         ("omega", C.c_double), ("mrt_s", C.c_double * 27), ("sc_G", C.c_double),
         ("storage_scale", C.c_double), ("n_classes", C.c_int32), ("device", C.c_int32),
@@ -203,12 +204,14 @@ def mrt_rates(sv: float, other: float) -> np.ndarray:
 
 def make_desc(lattice: int, collision: int, storage: int, shape, *, omega: float = 1.0, mrt_s=None,
               mrt_basis: int = MRT_REF, sc_G: float = 0.0, storage_scale: float = 0.0, device: int = 0,
-              arithmetic: int = ARITH_DEVIATION) -> Desc:
+              arithmetic: int = ARITH_DEVIATION, rounding: int = 0) -> Desc:
+    """rounding (16-bit storage): ROUND_STOCHASTIC (0, default) or ROUND_NEAREST (1)."""
     d = Desc()
     nx, ny = int(shape[0]), int(shape[1])
     nz = int(shape[2]) if len(shape) > 2 else 1
     lib().lbm_desc_init(C.byref(d), lattice, collision, storage, nx, ny, nz)
     d.arithmetic = arithmetic
+    d.rounding = rounding
     d.omega = omega
     if mrt_s is not None:
         for i, v in enumerate(mrt_s):
