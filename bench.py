@@ -334,10 +334,14 @@ def timed_steps(torch, lat, steps, dev):
 def build_workload(lb, args, storage):
     fn = WORKLOADS[args.workload][0]
     if args.dims and (args.workload.startswith("d3q27") or args.workload == "d2q9_shanchen_1024"):
-        return fn(lb, storage, tuple(int(v) for v in args.dims.lower().split("x")))
-    if args.size and (args.workload.startswith("d3q27") or args.workload == "d2q9_lid_8192"):
-        return fn(lb, storage, args.size)
-    return fn(lb, storage)
+        d, m = fn(lb, storage, tuple(int(v) for v in args.dims.lower().split("x")))
+    elif args.size and (args.workload.startswith("d3q27") or args.workload == "d2q9_lid_8192"):
+        d, m = fn(lb, storage, args.size)
+    else:
+        d, m = fn(lb, storage)
+    if getattr(args, "rounding", "stochastic") == "nearest":
+        d.rounding = lb.ROUND_NEAREST
+    return d, m
 
 
 def apply_kernel_choice(lb, lat, args):
@@ -595,13 +599,15 @@ def acc_mrt256(lb, steps=5000, shape=(256, 256, 256)):
 
 def acc_ensemble(lb, steps=1000):
     """Config 5: the F16S batch (one launch per step over every member) against each member's FP64 run
-    (stepped alone), after `steps` steps: per-member rel. L2 of u; max, median and the pooled value."""
+    (stepped alone), after `steps` steps: per-member rel. L2 of u; max, median and the pooled value over
+    the members whose FP64 run stays finite (a member that blows up in FP64 too is under-resolved, not a
+    storage error, and is listed instead)."""
     members = ensemble_members(lb, lb.F16S)
     batch = lb.Batch([d for d, _, _ in members], [m for _, m, _ in members])
     batch.step(steps)
     batch.sync()
     members64 = ensemble_members(lb, lb.F64)
-    errs, num, den = [], 0.0, 0.0
+    errs, num, den, diverged, worst = [], 0.0, 0.0, [], (0.0, "")
     for k, (d, m, name) in enumerate(members):
         _, u16 = batch.macros(k)
         dd, mm, _ = members64[k]
@@ -609,13 +615,18 @@ def acc_ensemble(lb, steps=1000):
             lat.step(steps)
             _, u64 = lat.macros()
         keep = np.tile(~solid_cells(lb, dd, mm), d.dim)
-        errs.append(rel_l2(u16[keep], u64[keep]))
+        if not np.all(np.isfinite(u64[keep])):
+            diverged.append(f"{name} (member {k}, tau {1.0 / d.omega:.4f}, FP64 {'and F16S ' if not np.all(np.isfinite(u16[keep])) else ''}non-finite)")
+            continue
+        e = rel_l2(u16[keep], u64[keep])
+        errs.append(e)
+        worst = max(worst, (e, name))
         num += float(np.sum((u16[keep] - u64[keep]) ** 2))
         den += float(np.sum(u64[keep] ** 2))
     batch.close()
     return {"rel_l2_u_f16s_vs_f64_max": max(errs), "rel_l2_u_f16s_vs_f64_median": float(np.median(errs)),
-            "rel_l2_u_f16s_vs_f64_pooled": float(np.sqrt(num / den)), "members": len(members), "steps": steps,
-            "worst_member": members[int(np.argmax(errs))][2]}
+            "rel_l2_u_f16s_vs_f64_pooled": float(np.sqrt(num / den)), "members": len(members),
+            "members_compared": len(errs), "diverged_in_fp64": diverged, "steps": steps, "worst_member": worst[1]}
 
 
 ACCURACY = {
@@ -656,15 +667,17 @@ def reduce_max(torch, value, dev, world):
 # ---------------------------------------------------------------------------------------------
 def ensemble_members(lb, storage, seed=3):
     """48 D2Q9 BGK lid cavities (L uniform in {64, 128, ..., 1024}, Re uniform in [100, 1000], lid 0.1,
-    C++ viscosity rule nu = u L / Re) and 16 D3Q27 BGK channels (4L, L, L), L uniform in
-    {64, 96, 128, 160, 192}, sphere of diameter L/4 centred in the channel, equilibrium inlet 0.04,
-    zero-gradient outlet, nu from Re = 100 on the sphere diameter.  numpy PCG64 seeded with `seed`."""
+    the Rust examples' viscosity rule nu = u 2 L / Re, rust/examples/d2q9_bgk_lid.rs:52) and 16 D3Q27 BGK
+    channels (4L, L, L), L uniform in {64, 96, 128, 160, 192}, sphere of diameter L/4 centred in the
+    channel, equilibrium inlet 0.04, zero-gradient outlet, nu from Re = 100 on the sphere diameter.  numpy
+    PCG64 seeded with `seed`.  (With the C++ rule nu = u L / Re four of the lids -- L = 64 and 128 at
+    Re 450-840, tau 0.52-0.55 -- are under-resolved and blow up in FP64 too; with the Rust rule one is.)"""
     rng = np.random.default_rng(seed)
     members = []
     for _ in range(48):
         L = int(rng.integers(1, 17)) * 64
         re = float(rng.uniform(100.0, 1000.0))
-        d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (L, L), omega=lb.omega_from_re(0.1, L, re, 0))
+        d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (L, L), omega=lb.omega_from_re(0.1, L, re, 1))
         members.append((d, lb.setup_cavity2d(d, 0.1), f"d2q9_lid_{L}"))
     for _ in range(16):
         L = int(rng.choice([64, 96, 128, 160, 192]))
@@ -927,6 +940,8 @@ def main():
                     help="cube side for D3Q27 workloads, square side for d2q9_lid_8192 (default: the config's)")
     ap.add_argument("--dims", default="", help="NXxNYxNZ for D3Q27 workloads, NXxNY for the Shan-Chen one")
     ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "rows"], help="step-kernel family")
+    ap.add_argument("--rounding", default="stochastic", choices=["stochastic", "nearest"],
+                    help="rounding of 16-bit storage in the timed runs")
     ap.add_argument("--block", type=int, default=0, help="fixed block width (default: autotune)")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:

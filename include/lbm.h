@@ -179,6 +179,11 @@ int   lbm_get_desc(const lbm_ctx* c, lbm_desc* out);
  * memory = LBM_DEVICE: asynchronous on the context stream; LBM_HOST: returns when the copy is done. */
 int   lbm_face_get(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, void* dst, int memory);
 int   lbm_face_set(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, const void* src, int memory);
+/* Index of this lattice's first cell within a larger lattice it is a part of (a slab of a decomposed
+ * lattice; any integer, taken modulo 2^32; default 0).  Stochastic rounding hashes that global index
+ * with the step number, so the slabs of a decomposed lattice round exactly like the undivided lattice.
+ * No counterpart in the reference (one lattice on one device).                                     */
+int   lbm_set_cell_offset(lbm_ctx* c, int64_t offset);
 /* Block width (threads along x) used by the step kernel; 0 = autotune on first step. */
 int   lbm_set_block(lbm_ctx* c, int threads_x);
 int   lbm_get_block(const lbm_ctx* c);

@@ -34,6 +34,7 @@ struct BatchLattice {
     R omega, one_m_omega;
     R scale, inv_scale;
     int sr;                         // 16-bit storage: stochastic rounding (1) or to nearest (0)
+    uint32_t cell_base;             // 0: a member's cells are hashed by their own index
     alignas(16) ClassTable<R> cls;  // 16-byte aligned: the row pipeline bulk-copies it into shared memory
 };
 

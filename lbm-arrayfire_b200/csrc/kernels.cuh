@@ -47,6 +47,7 @@ struct StepParams {
     unsigned* tick;       // the step counter pair of the rounding (see step_rounding)
     int parity;           // the input buffer of this launch: it reads tick[parity], writes tick[parity ^ 1]
     int sr;               // 16-bit storage: 1 stochastic rounding, 0 round to nearest
+    uint32_t cell_base;   // index of cell 0 in the lattice this one is part of (the rounding's hash input)
     ClassTable<R> cls;
     MrtCoef<R> mrt;
     Mrt2Coef<R> mrt2;
@@ -321,7 +322,10 @@ __device__ __forceinline__ void store16(S* __restrict__ fo, long long N, const R
             return 0.0f;
     };
     if (rnd.sr) {
-        const uint32_t h = mix32(cell ^ rnd.seed);
+        // one multiply round of the cell index against the step's (fully hashed) seed: over the steps a
+        // cell's words are uniform (the seed is), and the multiply spreads neighbouring cells' bits
+        uint32_t h = (cell ^ rnd.seed) * 0x9e3779b1u;
+        h ^= h >> 16;
         static_for<NP>([&](auto K) {
             constexpr uint32_t salt = 0x9e3779b9u * (uint32_t)(decltype(K)::value + 1);
             put(K, Pair16<S>::rs(out[2 * K], second(K), h ^ salt));
@@ -335,7 +339,7 @@ template <class L, class S, bool ABS, class P, class R>
 __device__ __forceinline__ void store_cell(S* __restrict__ fout, const P& p, long long c, const R (&out)[L::Q],
                                            const Rounding& rnd) {
     if constexpr (!ABS && Codec<S>::kScaled) {
-        store16<L, S>(fout + c, p.N, out, rnd, (uint32_t)c);
+        store16<L, S>(fout + c, p.N, out, rnd, (uint32_t)c + p.cell_base);
     } else {
         static_for<L::Q>([&](auto I) {
             constexpr int i = I;

@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         const S* st0 = in + (long long)s * Q * SB;
         const uint8_t* ms0 = has_mask ? mask_st + s * SB : nullptr;
         S* out0 = static_cast<S*>(p.fout) + ((long long)z * ny + y0) * nx;
-        const uint32_t cell0 = (uint32_t)(((long long)z * ny + y0) * nx);
+        const uint32_t cell0 = (uint32_t)(((long long)z * ny + y0) * nx) + p.cell_base;
 #pragma unroll 1
         while (b < nb) {
             row_cell_wrap<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, x, nx, sc, isc,
@@ -547,7 +547,7 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
         const S* st = in + (long long)s * Q * SB + H;  // staged index of x0 is 0
         const uint8_t* mrow = has_mask ? mask_st + s * SB : nullptr;
         S* orow = static_cast<S*>(p.fout) + (long long)row * nx + x0;
-        const uint32_t cell0 = (uint32_t)((long long)row * nx + x0);
+        const uint32_t cell0 = (uint32_t)((long long)row * nx + x0) + p.cell_base;
 #pragma unroll 1
         for (int xl = tid; xl < w; xl += Sh::CONSUMERS)
             row_cell<L, S, SB, COLL>(p, st, mrow, xl, xl - 1, xl + 1, xl, xl, sc, isc, orow, rnd,

@@ -138,6 +138,7 @@ struct lbm_ctx {
     long long steps = 0;
     double scale = 1.0;
     bool mrt2 = false;             // two-rate Gram-Schmidt MRT (mrt2_collide) in use
+    long long cell_offset = 0;     // lbm_set_cell_offset
     StepParams<float> pf{};
     StepParams<double> pd{};
 };
@@ -161,6 +162,7 @@ static StepParams<R> make_params(const lbm_ctx* c) {
     p.psi = static_cast<R*>(c->psi);
     p.tick = c->tick;
     p.sr = d.rounding == LBM_ROUND_STOCHASTIC ? 1 : 0;
+    p.cell_base = (uint32_t)c->cell_offset;
     for (int k = 0; k < kMaxClasses; ++k) {
         const bool used = k < d.n_classes;
         p.cls.flags[k] = used ? d.classes[k].flags : 0u;
@@ -1060,6 +1062,17 @@ int lbm_set_kernel(lbm_ctx* c, int kind) {
 }
 
 int lbm_get_kernel(const lbm_ctx* c) { return c ? c->kernel_used : 0; }
+
+int lbm_set_cell_offset(lbm_ctx* c, int64_t offset) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    LBM_CK(cudaSetDevice(c->d.device));
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);  // the graphs captured the old offset in their launch parameters
+    c->cell_offset = offset;
+    c->pf = make_params<float>(c);
+    c->pd = make_params<double>(c);
+    return LBM_OK;
+}
 
 int lbm_test_stall_next_step(lbm_ctx* c, int64_t item, int64_t wait_clocks) {
     if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");

@@ -117,6 +117,7 @@ _SIGS = {
     "lbm_set_kernel": (C.c_int, [_P, C.c_int]),
     "lbm_get_kernel": (C.c_int, [_P]),
     "lbm_test_stall_next_step": (C.c_int, [_P, C.c_int64, C.c_int64]),
+    "lbm_set_cell_offset": (C.c_int, [_P, C.c_int64]),
     "lbm_sums_fp64_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_double, _P, _P]),
     "lbm_batch_create": (C.c_int, [_DP, C.c_int, C.POINTER(_P)]),
     "lbm_batch_destroy": (None, [_P]),
@@ -355,6 +356,10 @@ class Lattice:
 
     def kernel(self) -> int:
         return lib().lbm_get_kernel(self._h)
+
+    def set_cell_offset(self, offset: int):
+        """Index of this lattice's cell 0 in the lattice it is a slab of (stochastic rounding's hash)."""
+        _check(lib().lbm_set_cell_offset(self._h, offset))
 
     def test_stall_next_step(self, item: int = 0, wait_clocks: int = 1 << 21):
         """Test hook: the next step's row pipeline leaves work item `item` unfilled and gives its waits

@@ -114,6 +114,10 @@ class Slab:
         self.n = self.p1 - self.p0
         self.desc, self.mask = local_problem(desc, mask, self.p0, self.p1)
         self.lat = (lattice_factory or Lattice)(self.desc, self.mask)
+        if hasattr(self.lat, "set_cell_offset"):
+            # local plane 0 is global plane p0 - 1: the slab's cells hash (stochastic rounding) like the
+            # undivided lattice's
+            self.lat.set_cell_offset((self.p0 - 1) * (desc.cells // _planes(desc)))
         self.up_dirs, self.down_dirs = axis_dirs(desc.lattice)
         self.device = torch.device(device) if device is not None else torch.device("cpu")
         if self.device.type == "cuda":
@@ -205,6 +209,8 @@ class SlabSet:
         for p0, p1 in self.ranges:
             d, m = local_problem(desc, mask, p0, p1)
             lat = (lattice_factory or Lattice)(d, m)
+            if hasattr(lat, "set_cell_offset"):
+                lat.set_cell_offset((p0 - 1) * (desc.cells // _planes(desc)))
             lat.set_populations(scatter_populations(desc, F0, p0, p1))
             self.lats.append(lat)
             self.ns.append(p1 - p0)

@@ -218,7 +218,7 @@ def config_bgk_lid3d(shape=(256, 256, 256)):
 
 def ensemble_spec(seed: int = 3):
     """Config 5: 48 D2Q9 BGK lid cavities (L uniform in {64, 128, ..., 1024}, Re uniform in [100, 1000],
-    lid 0.1, C++ viscosity rule) and 16 D3Q27 BGK channels (4L, L, L), L uniform in
+    lid 0.1, the Rust examples' viscosity rule nu = u 2 L / Re) and 16 D3Q27 BGK channels (4L, L, L), L uniform in
     {64, 96, 128, 160, 192}, sphere of diameter L/4 at (2L, L/2, L/2), equilibrium inlet 0.04,
     zero-gradient outlet, nu from Re 100 on the sphere diameter.  numpy PCG64 seeded with `seed`.
     Returns (name, shape, omega) per member, in order."""
@@ -227,7 +227,7 @@ def ensemble_spec(seed: int = 3):
     for _ in range(48):
         L = int(rng.integers(1, 17)) * 64
         re = float(rng.uniform(100.0, 1000.0))
-        out.append((f"d2q9_lid_{L}", (L, L), omega_from_re(0.1, L, re, 0)))
+        out.append((f"d2q9_lid_{L}", (L, L), omega_from_re(0.1, L, re, 1)))
     for _ in range(16):
         L = int(rng.choice([64, 96, 128, 160, 192]))
         nu = 0.04 * (L / 4.0) / 100.0
