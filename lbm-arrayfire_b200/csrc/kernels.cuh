@@ -303,8 +303,29 @@ __device__ __forceinline__ Rounding step_rounding(unsigned* tick, int parity, in
     }
 }
 
-// The 16-bit store of a cell's outputs (raw, storage units) at fo[i * N]: directions in pairs through
-// one paired conversion; stochastic rounding draws one 32-bit word per pair from the cell's hash.
+// Random bits of the stochastic rounding.  Every stored value (cell c, direction i) has its own 16-bit
+// word g(c, i) = h(c) ^ salt(i), with h(c) a hash of the cell index and the step's seed; a paired
+// conversion takes the upper value's word in bits 31..16 of its random operand and the lower value's in
+// bits 15..0 (the layout cvt.rs uses, measured on B200).  A value therefore rounds with the same bits
+// whichever value it is paired with: two directions of one cell (store16) or one direction of two
+// adjacent cells (row_pair) -- the kernel families stay bit-identical.
+__host__ __device__ constexpr uint32_t rs_salt(int i) { return ((0x9e3779b9u * (uint32_t)(i + 1)) >> 16) & 0xffffu; }
+__device__ __forceinline__ uint32_t cell_hash16(uint32_t cell, uint32_t seed) {
+    uint32_t h = (cell ^ seed) * 0x9e3779b1u;
+    return (h ^ (h >> 16)) & 0xffffu;
+}
+// The random operands of one thread's paired conversions: base = (upper value's cell hash << 16) | lower's.
+struct PairBits {
+    uint32_t base;
+    // directions i (upper) and j (lower)
+    template <int I, int J>
+    __device__ __forceinline__ uint32_t word() const {
+        return base ^ ((rs_salt(I) << 16) | rs_salt(J));
+    }
+};
+
+// The 16-bit store of a cell's outputs (raw, storage units) at fo[i * N]: directions in pairs (i, i + 1,
+// i in the upper half) through one paired conversion each.
 template <class L, class S, class R>
 __device__ __forceinline__ void store16(S* __restrict__ fo, long long N, const R (&out)[L::Q], const Rounding& rnd,
                                         uint32_t cell) {
@@ -322,13 +343,11 @@ __device__ __forceinline__ void store16(S* __restrict__ fo, long long N, const R
             return 0.0f;
     };
     if (rnd.sr) {
-        // one multiply round of the cell index against the step's (fully hashed) seed: over the steps a
-        // cell's words are uniform (the seed is), and the multiply spreads neighbouring cells' bits
-        uint32_t h = (cell ^ rnd.seed) * 0x9e3779b1u;
-        h ^= h >> 16;
+        const uint32_t h = cell_hash16(cell, rnd.seed);
+        const PairBits pb{(h << 16) | h};
         static_for<NP>([&](auto K) {
-            constexpr uint32_t salt = 0x9e3779b9u * (uint32_t)(decltype(K)::value + 1);
-            put(K, Pair16<S>::rs(out[2 * K], second(K), h ^ salt));
+            constexpr int i = 2 * decltype(K)::value;
+            put(K, Pair16<S>::rs(out[i], second(K), pb.template word<i, i + 1>()));
         });
     } else {
         static_for<NP>([&](auto K) { put(K, Pair16<S>::rn(out[2 * K], second(K))); });

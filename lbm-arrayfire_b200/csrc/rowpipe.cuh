@@ -168,7 +168,18 @@ constexpr unsigned long long pack_c(bool z) {
 //   SEG       rows wider than PITCH: a work item is one row segment of up to SEGW = PITCH - 16 cells
 //             (SEGW_RUN by default) staged with HALO = 8 cells on either side, one segment per stage;
 //             CR only sets the consumer count, and every stage the CTA's shared memory holds is used
-template <class L, class S, int PITCH, bool SEG = false>
+#ifndef LBM_ROWPIPE_PAIR
+#define LBM_ROWPIPE_PAIR 1  // 16-bit storage, BGK / two-rate MRT: consumers take two adjacent cells (row_pair)
+#endif
+#ifndef LBM_ROWPIPE_PAIR_WARPS3
+#define LBM_ROWPIPE_PAIR_WARPS3 15  // D3Q27 consumer warps with pairs: 16 warps in all, 4 per sub-partition
+#endif
+
+// The row kernel's consumers take pairs of adjacent cells (row_pair) for this lattice, storage and collision.
+template <class L, class S, int COLL>
+constexpr bool kRowPair = LBM_ROWPIPE_PAIR && Codec<S>::kScaled && (COLL == 0 || COLL == 3);
+
+template <class L, class S, int PITCH, bool SEG = false, bool PAIR = false>
 struct RowPipeShape {
     static constexpr int HALO = 8;
     static constexpr int SEGW = PITCH - 2 * HALO;
@@ -198,7 +209,10 @@ struct RowPipeShape {
     static constexpr int CR = CR0 < 1 ? 1 : CR0;
     // D3Q27 consumer warps (0: CR row sets of THREADS): the register file holds 5 warps of 96
     // registers per SM sub-partition, i.e. up to 19 consumer warps beside the producer
-    static constexpr int CONSUMERS = k3 && LBM_ROWPIPE_CWARPS3 > 0    ? LBM_ROWPIPE_CWARPS3 * 32
+    // with pairs a D3Q27 thread holds two cells' outputs: 15 consumer warps + the producer keep every
+    // sub-partition at 4 warps, i.e. up to 128 registers a thread (17 warps put 5 on one: 96 at most)
+    static constexpr int CONSUMERS = PAIR && k3                       ? LBM_ROWPIPE_PAIR_WARPS3 * 32
+                                     : k3 && LBM_ROWPIPE_CWARPS3 > 0    ? LBM_ROWPIPE_CWARPS3 * 32
                                      : !k3 && LBM_ROWPIPE_CWARPS2 > 0 ? LBM_ROWPIPE_CWARPS2 * 32
                                                                        : CR * THREADS;
     // CTAs per SM: D3Q27 collisions need ~90-120 registers per thread, D2Q9 far fewer; fewer CTAs
@@ -308,6 +322,84 @@ __device__ __forceinline__ void row_cell_wrap(const P& p, const S* st, const uin
     row_cell<L, S, SB, COLL>(p, st, mrow, x, xm, xp, x, x, sc, isc, orow, rnd, row0 + (uint32_t)x);
 }
 
+// Two adjacent cells (x even and x + 1) of a whole staged row of width nx (periodic in x), for 16-bit
+// storage and a collision that applies its own bounce-back (BGK, two-rate MRT).  Both cells collide as
+// row_cell's would; then every direction's two outputs go through one paired conversion and one 32-bit
+// store (cell x in the low half, x + 1 in the high half: both cells are adjacent in every plane), which
+// halves the stores and their address arithmetic of one-cell threads, and the populations with c_x = 0
+// of both cells come in one 32-bit shared load.  Stochastic rounding gives each value the same random
+// bits as the one-cell path (pair_rbits), so the kernel families stay bit-identical.
+template <class L, class S, int SB, int COLL, class P>
+__device__ __forceinline__ void row_pair(const P& p, const S* st, const uint8_t* mrow, int x, int nx,
+                                         typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow,
+                                         const Rounding& rnd, uint32_t cell) {
+    using R = typename Codec<S>::Real;
+    constexpr int Q = L::Q;
+    static_assert(Codec<S>::kScaled && (COLL == 0 || COLL == 3), "pairs: 16-bit storage, BGK or two-rate MRT");
+    const int xl = x == 0 ? nx - 1 : x - 1;   // left of the pair
+    const int xr = x + 2 == nx ? 0 : x + 2;   // right of the pair
+    int clsA = 0, clsB = 0;
+    if (mrow) {
+        const uint32_t m2 = *reinterpret_cast<const unsigned short*>(mrow + x);
+        clsA = (int)(m2 & 0xffu);
+        clsB = (int)(m2 >> 8);
+    }
+    const uint32_t flA = p.cls.flags[clsA], flB = p.cls.flags[clsB];
+    R outA[Q];
+    {
+        R v[Q];
+        static_for<Q>([&](auto I) {
+            constexpr int i = I;
+            constexpr int cx = L::cx(i);
+            const int xs = cx == 1 ? xl : (cx == -1 ? x + 1 : x);
+            v[i] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
+        });
+        if (flA & kZeroGradXp) {
+            static_for<Q>([&](auto I) {
+                constexpr int i = I;
+                if constexpr (L::cx(i) == -1) v[i] = Codec<S>::raw(st[i * SB + x], R(L::w(i)));
+            });
+        }
+        if constexpr (COLL == 0)
+            bgk_collide<L, false, false>(p, clsA, flA, v, sc, isc, outA);
+        else
+            mrt2_collide(p, clsA, flA, v, sc, isc, outA);
+    }
+    R outB[Q];
+    {
+        R v[Q];
+        static_for<Q>([&](auto I) {
+            constexpr int i = I;
+            constexpr int cx = L::cx(i);
+            const int xs = cx == 1 ? x : (cx == -1 ? xr : x + 1);
+            v[i] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
+        });
+        if (flB & kZeroGradXp) {
+            static_for<Q>([&](auto I) {
+                constexpr int i = I;
+                if constexpr (L::cx(i) == -1) v[i] = Codec<S>::raw(st[i * SB + x + 1], R(L::w(i)));
+            });
+        }
+        if constexpr (COLL == 0)
+            bgk_collide<L, false, false>(p, clsB, flB, v, sc, isc, outB);
+        else
+            mrt2_collide(p, clsB, flB, v, sc, isc, outB);
+    }
+    S* __restrict__ fo = orow + x;
+    if (rnd.sr) {
+        const PairBits pb{(cell_hash16(cell + 1u, rnd.seed) << 16) | cell_hash16(cell, rnd.seed)};
+        static_for<Q>([&](auto I) {
+            constexpr int i = I;
+            *reinterpret_cast<uint32_t*>(fo + (long long)i * p.N) = Pair16<S>::rs(outB[i], outA[i], pb.template word<i, i>());
+        });
+    } else {
+        static_for<Q>([&](auto I) {
+            constexpr int i = I;
+            *reinterpret_cast<uint32_t*>(fo + (long long)i * p.N) = Pair16<S>::rn(outB[i], outA[i]);
+        });
+    }
+}
+
 // COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt), 3 = two-rate MRT (Gram-Schmidt,
 // mrt2_collide).  Deviation arithmetic.
 // Requires nx <= PITCH with nx * sizeof(S) a multiple of 16 bytes; `rows` = rows per group
@@ -316,11 +408,14 @@ __device__ __forceinline__ void row_cell_wrap(const P& p, const S* st, const uin
 //   empty[s]  every consumer warp has finished reading stage s
 // Stage s holds, for direction i, the group's source rows at in[(s * Q + i) * SB + b * nx].
 template <class L, class S, int PITCH, int COLL>
-__global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, RowPipeShape<L, S, PITCH>::CTAS)
+using RowShape = RowPipeShape<L, S, PITCH, false, kRowPair<L, S, COLL>>;
+
+template <class L, class S, int PITCH, int COLL>
+__global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, RowShape<L, S, PITCH, COLL>::CTAS)
     k_step_rows(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int rows, int* __restrict__ err,
                   const WaitLimits wl) {
     using R = typename Codec<S>::Real;
-    using Sh = RowPipeShape<L, S, PITCH>;
+    using Sh = RowShape<L, S, PITCH, COLL>;
     constexpr int Q = L::Q;
     constexpr int NS = Sh::NS;
     constexpr int SB = Sh::SB;
@@ -397,8 +492,11 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
     const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, (blockIdx.x | tid) == 0);
     // cells of a group flattened (row b, column x; staged index b * nx + x), CONSUMERS apart and
     // continued across stages: the cells one stage leaves over go to other threads in the next
-    const int cq = Sh::CONSUMERS / nx, cr = Sh::CONSUMERS - cq * nx;
-    int b = tid / nx, x = tid - b * nx;
+    // 16-bit BGK / two-rate MRT: threads take pairs of adjacent cells (row_pair), nx / 2 per row
+    constexpr bool kPair = kRowPair<L, S, COLL>;
+    const int cw = kPair ? nx >> 1 : nx;  // work units per row
+    const int cq = Sh::CONSUMERS / cw, cr = Sh::CONSUMERS - cq * cw;
+    int b = tid / cw, x = tid - b * cw;
     for (unsigned k = 0; first + k * stride < groups; ++k) {
         const unsigned g = first + k * stride;
         const int s = (int)(k % NS);
@@ -419,12 +517,16 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         const uint32_t cell0 = (uint32_t)(((long long)z * ny + y0) * nx) + p.cell_base;
 #pragma unroll 1
         while (b < nb) {
-            row_cell_wrap<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, x, nx, sc, isc,
-                                          out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
+            if constexpr (kPair)
+                row_pair<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, 2 * x, nx, sc, isc,
+                                         out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx + 2 * x));
+            else
+                row_cell_wrap<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, x, nx, sc, isc,
+                                              out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
             x += cr;
             b += cq;
-            if (x >= nx) {
-                x -= nx;
+            if (x >= cw) {
+                x -= cw;
                 ++b;
             }
         }

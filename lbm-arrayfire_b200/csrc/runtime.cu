@@ -256,7 +256,7 @@ static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>&
                                                                                               c->waits);
         return;
     }
-    using Sh = RowPipeShape<L, S, PITCH>;
+    using Sh = RowShape<L, S, PITCH, COLL>;
     auto kern = k_step_rows<L, S, PITCH, COLL>;
     kern<<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err, c->waits);  // + producer warp
 }
@@ -284,7 +284,7 @@ static int prepare_rows_t(lbm_ctx* c) {
         c->rows_grid = grid;
         return LBM_OK;
     } else {
-        using Sh = RowPipeShape<L, S, PITCH>;
+        using Sh = RowShape<L, S, PITCH, COLL>;
         auto kern = k_step_rows<L, S, PITCH, COLL>;
         LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
         LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
