@@ -24,6 +24,11 @@
 
 namespace lbm {
 
+template <class T>
+struct BTag {
+    using type = T;
+};
+
 // One ensemble member as the kernels see it (lives in device memory).
 template <class R>
 struct BatchLattice {
@@ -82,21 +87,25 @@ struct RowItem {
     int lat, y0, z, nb, fam;
 };
 
+// The row pipeline's shape in the ensemble kernels (BGK: pairs of cells for 16-bit storage).
+template <class L, class S, int PITCH>
+using BatchShape = RowPipeShape<L, S, PITCH, false, kRowPair<L, S, 0>>;
+
 // Shared memory of k_batch_rows: the row pipeline's stages plus one class table per stage.
 template <class L, class S, int PITCH>
 constexpr size_t batch_rows_smem() {
-    using Sh = RowPipeShape<L, S, PITCH>;
+    using Sh = BatchShape<L, S, PITCH>;
     return Sh::smem_bytes() + (size_t)Sh::NS * sizeof(ClassTable<typename Codec<S>::Real>);
 }
 
 // The row pipeline of rowpipe.cuh over a work table of row groups of several lattices (BGK).
 template <class L, class S, int PITCH>
-__global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, RowPipeShape<L, S, PITCH>::CTAS)
+__global__ void __launch_bounds__(BatchShape<L, S, PITCH>::CONSUMERS + 32, BatchShape<L, S, PITCH>::CTAS)
     k_batch_rows(const BatchLattice<typename Codec<S>::Real>* __restrict__ lats, const RowItem* __restrict__ items,
                  long long n_items, int parity, int* __restrict__ err, const WaitLimits wl, unsigned* tick,
                  int advance) {
     using R = typename Codec<S>::Real;
-    using Sh = RowPipeShape<L, S, PITCH>;
+    using Sh = BatchShape<L, S, PITCH>;
     constexpr int Q = L::Q;
     constexpr int NS = Sh::NS;
     constexpr int SB = Sh::SB;
@@ -193,18 +202,25 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
         // cells of the group, flattened (row b, column x), CONS apart.  tid / nx and CONS / nx by a
         // float reciprocal: exact here (numerators below 2^11, nx <= 1024: the quotient's distance to
         // the next integer, at least 1/(2 nx), is far above the rounding error)
-        const float inv_nx = __frcp_rn((float)nx);
-        int b = (int)(((float)tid + 0.5f) * inv_nx), x = tid - b * nx;
-        const int cq = (int)(((float)CONS + 0.5f) * inv_nx), cr = CONS - cq * nx;
+        // 16-bit storage: pairs of adjacent cells (row_pair), nx / 2 per row
+        constexpr bool kPair = kRowPair<L, S, 0>;
+        const int cw = kPair ? nx >> 1 : nx;
+        const float inv_nx = __frcp_rn((float)cw);
+        int b = (int)(((float)tid + 0.5f) * inv_nx), x = tid - b * cw;
+        const int cq = (int)(((float)CONS + 0.5f) * inv_nx), cr = CONS - cq * cw;
         const int nb = it.nb;
 #pragma unroll 1
         while (b < nb) {
-            row_cell_wrap<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
-                                       out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
+            if constexpr (kPair)
+                row_pair_wrap<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, 2 * x, nx, sc, isc,
+                                           out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
+            else
+                row_cell_wrap<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
+                                           out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
             x += cr;
             b += cq;
-            if (x >= nx) {
-                x -= nx;
+            if (x >= cw) {
+                x -= cw;
                 ++b;
             }
         }
@@ -214,19 +230,19 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, PITCH>::CONSUMERS + 32, Row
 }
 
 // The whole ensemble in one persistent launch: one work table holds the row groups of both lattice
-// families, and every CTA has the D3Q27 shape (RowPipeShape<D3Q27, S, PITCH>: consumer count, stage
+// families, and every CTA has the D3Q27 shape (BatchShape<D3Q27, S, PITCH>: consumer count, stage
 // size, stages).  A stage keeps 27 direction slots of SB elements; a D2Q9 group fills the first 9 (its
 // rows sized by the host so that nb * nx <= SB), a D3Q27 group all of them; the mask rows and the
 // member's class table follow as in k_batch_rows.  Lanes 0 .. Q-1 of the producer copy the directions,
 // lane 27 the mask rows, lane 28 the class table.  Each consumer runs the collision of the item's family
 // (both are compiled into the kernel; the register budget is D3Q27's).
 template <class S, int PITCH>
-__global__ void __launch_bounds__(RowPipeShape<D3Q27, S, PITCH>::CONSUMERS + 32, RowPipeShape<D3Q27, S, PITCH>::CTAS)
+__global__ void __launch_bounds__(BatchShape<D3Q27, S, PITCH>::CONSUMERS + 32, BatchShape<D3Q27, S, PITCH>::CTAS)
     k_batch_rows_mix(const BatchLattice<typename Codec<S>::Real>* __restrict__ lats,
                      const RowItem* __restrict__ items, long long n_items, int parity, int* __restrict__ err,
                      const WaitLimits wl, unsigned* tick, int advance) {
     using R = typename Codec<S>::Real;
-    using Sh = RowPipeShape<D3Q27, S, PITCH>;
+    using Sh = BatchShape<D3Q27, S, PITCH>;
     constexpr int NS = Sh::NS;
     constexpr int SB = Sh::SB;
     constexpr int CONS = Sh::CONSUMERS;
@@ -321,44 +337,40 @@ __global__ void __launch_bounds__(RowPipeShape<D3Q27, S, PITCH>::CONSUMERS + 32,
         const uint32_t cell0 = (uint32_t)(((long long)it.z * m.ny + it.y0) * nx);
         const Rounding rnd{seed, m.sr != 0};
         // cells of the group, flattened (row b, column x), CONS apart (as k_batch_rows)
-        const float inv_nx = __frcp_rn((float)nx);
-        int b = (int)(((float)tid + 0.5f) * inv_nx), x = tid - b * nx;
-        const int cq = (int)(((float)CONS + 0.5f) * inv_nx), cr = CONS - cq * nx;
+        // 16-bit storage: pairs of adjacent cells (row_pair), nx / 2 per row
+        constexpr bool kPair = kRowPair<D3Q27, S, 0>;
+        const int cw = kPair ? nx >> 1 : nx;
+        const float inv_nx = __frcp_rn((float)cw);
+        int b = (int)(((float)tid + 0.5f) * inv_nx), x = tid - b * cw;
+        const int cq = (int)(((float)CONS + 0.5f) * inv_nx), cr = CONS - cq * cw;
         const int nb = it.nb;
-        if (it.fam) {
+        auto walk = [&](auto lt) {
+            using L = typename decltype(lt)::type;
 #pragma unroll 1
             while (b < nb) {
-                row_cell_wrap<D3Q27, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
+                if constexpr (kPair)
+                    row_pair_wrap<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, 2 * x, nx, sc, isc,
+                                               out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
+                else
+                    row_cell_wrap<L, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
                                                out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
                 x += cr;
                 b += cq;
-                if (x >= nx) {
-                    x -= nx;
+                if (x >= cw) {
+                    x -= cw;
                     ++b;
                 }
             }
-        } else {
-#pragma unroll 1
-            while (b < nb) {
-                row_cell_wrap<D2Q9, S, SB, 0>(mc, st + b * nx, ms ? ms + b * nx : nullptr, x, nx, sc, isc,
-                                              out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
-                x += cr;
-                b += cq;
-                if (x >= nx) {
-                    x -= nx;
-                    ++b;
-                }
-            }
-        }
+        };
+        if (it.fam)
+            walk(BTag<D3Q27>{});
+        else
+            walk(BTag<D2Q9>{});
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
     }
 }
 
-template <class T>
-struct BTag {
-    using type = T;
-};
 template <class F>
 static void batch_dispatch(int storage, F&& f) {
     switch (storage) {
@@ -485,7 +497,7 @@ static int batch_build_rows(lbm_batch* b) {
             using L = typename decltype(lt)::type;
             using S = typename decltype(st)::type;
             constexpr int PITCH = decltype(pi)::value;
-            using Sh = RowPipeShape<L, S, PITCH>;
+            using Sh = BatchShape<L, S, PITCH>;
             for (int k = 0; k < (int)b->descs.size(); ++k) {
                 const lbm_desc& d = b->descs[k];
                 if ((d.lattice == LBM_D2Q9) != (fam == 0) || !batch_row_member(b, k)) continue;
@@ -540,7 +552,7 @@ static int batch_build_mixed(lbm_batch* b, double scale) {
     auto build = [&](auto st, auto pi) {
         using S = typename decltype(st)::type;
         constexpr int PITCH = decltype(pi)::value;
-        using Sh = RowPipeShape<D3Q27, S, PITCH>;
+        using Sh = BatchShape<D3Q27, S, PITCH>;
         const int target[2] = {(int)(RowPipeShape<D2Q9, S, PITCH>::kGroupBytes * scale), (int)(Sh::kGroupBytes * scale)};
         b->group_bytes[0] = target[0];
         b->group_bytes[1] = target[1];
@@ -631,7 +643,7 @@ static void batch_launch(lbm_batch* b, int parity, cudaStream_t s) {
             using S = typename decltype(st)::type;
             using R = typename Codec<S>::Real;
             constexpr int PITCH = decltype(pi)::value;
-            using Sh = RowPipeShape<D3Q27, S, PITCH>;
+            using Sh = BatchShape<D3Q27, S, PITCH>;
             k_batch_rows_mix<S, PITCH><<<b->mix_grid, Sh::CONSUMERS + 32, batch_rows_smem<D3Q27, S, PITCH>(), s>>>(
                 static_cast<const BatchLattice<R>*>(b->lats_d), b->mix_items_d, b->mix_n, parity, b->err, b->waits,
                 b->tick, advance);
@@ -644,7 +656,7 @@ static void batch_launch(lbm_batch* b, int parity, cudaStream_t s) {
             using L = typename decltype(lt)::type;
             using S = typename decltype(st)::type;
             using R = typename Codec<S>::Real;
-            using Sh = RowPipeShape<L, S, decltype(pi)::value>;
+            using Sh = BatchShape<L, S, decltype(pi)::value>;
             k_batch_rows<L, S, decltype(pi)::value><<<b->rows_grid[fam], Sh::CONSUMERS + 32,
                                                       batch_rows_smem<L, S, decltype(pi)::value>(), s>>>(
                 static_cast<const BatchLattice<R>*>(b->lats_d), b->items_d[fam], b->n_items[fam], parity, b->err,

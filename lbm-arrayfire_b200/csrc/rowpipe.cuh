@@ -322,22 +322,22 @@ __device__ __forceinline__ void row_cell_wrap(const P& p, const S* st, const uin
     row_cell<L, S, SB, COLL>(p, st, mrow, x, xm, xp, x, x, sc, isc, orow, rnd, row0 + (uint32_t)x);
 }
 
-// Two adjacent cells (x even and x + 1) of a whole staged row of width nx (periodic in x), for 16-bit
+// Two adjacent cells (x even and x + 1) of a staged row, for 16-bit
 // storage and a collision that applies its own bounce-back (BGK, two-rate MRT).  Both cells collide as
 // row_cell's would; then every direction's two outputs go through one paired conversion and one 32-bit
 // store (cell x in the low half, x + 1 in the high half: both cells are adjacent in every plane), which
 // halves the stores and their address arithmetic of one-cell threads, and the populations with c_x = 0
 // of both cells come in one 32-bit shared load.  Stochastic rounding gives each value the same random
 // bits as the one-cell path (pair_rbits), so the kernel families stay bit-identical.
+// x: staged index of the first cell (even); xl, xr: staged indices of the pair's left and right neighbours
+// (periodic wrap or halo already applied).
 template <class L, class S, int SB, int COLL, class P>
-__device__ __forceinline__ void row_pair(const P& p, const S* st, const uint8_t* mrow, int x, int nx,
+__device__ __forceinline__ void row_pair(const P& p, const S* st, const uint8_t* mrow, int x, int xl, int xr,
                                          typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow,
                                          const Rounding& rnd, uint32_t cell) {
     using R = typename Codec<S>::Real;
     constexpr int Q = L::Q;
     static_assert(Codec<S>::kScaled && (COLL == 0 || COLL == 3), "pairs: 16-bit storage, BGK or two-rate MRT");
-    const int xl = x == 0 ? nx - 1 : x - 1;   // left of the pair
-    const int xr = x + 2 == nx ? 0 : x + 2;   // right of the pair
     int clsA = 0, clsB = 0;
     if (mrow) {
         const uint32_t m2 = *reinterpret_cast<const unsigned short*>(mrow + x);
@@ -398,6 +398,15 @@ __device__ __forceinline__ void row_pair(const P& p, const S* st, const uint8_t*
             *reinterpret_cast<uint32_t*>(fo + (long long)i * p.N) = Pair16<S>::rn(outB[i], outA[i]);
         });
     }
+}
+
+// A pair of a whole staged row of width nx (periodic in x); row0: the cell index of the row's x = 0.
+template <class L, class S, int SB, int COLL, class P>
+__device__ __forceinline__ void row_pair_wrap(const P& p, const S* st, const uint8_t* mrow, int x, int nx,
+                                              typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow,
+                                              const Rounding& rnd, uint32_t row0) {
+    row_pair<L, S, SB, COLL>(p, st, mrow, x, x == 0 ? nx - 1 : x - 1, x + 2 == nx ? 0 : x + 2, sc, isc, orow, rnd,
+                             row0 + (uint32_t)x);
 }
 
 // COLL: 0 = BGK, 1 = MRT (reference basis), 2 = MRT (Gram-Schmidt), 3 = two-rate MRT (Gram-Schmidt,
@@ -518,8 +527,8 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
 #pragma unroll 1
         while (b < nb) {
             if constexpr (kPair)
-                row_pair<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, 2 * x, nx, sc, isc,
-                                         out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx + 2 * x));
+                row_pair_wrap<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, 2 * x, nx, sc, isc,
+                                              out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
             else
                 row_cell_wrap<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, x, nx, sc, isc,
                                               out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
@@ -545,11 +554,14 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
 // 16 bytes: population rows at x0 - 8, mask rows at x0 for w bytes.  Stage s, direction i, staged
 // index j holds x = x0 - HALO + j.
 template <class L, class S, int COLL>
-__global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS + 32, RowPipeShape<L, S, kSegPitch, true>::CTAS)
+using SegShape = RowPipeShape<L, S, kSegPitch, true, kRowPair<L, S, COLL>>;
+
+template <class L, class S, int COLL>
+__global__ void __launch_bounds__(SegShape<L, S, COLL>::CONSUMERS + 32, SegShape<L, S, COLL>::CTAS)
     k_step_rows_seg(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int segw, int* __restrict__ err,
                   const WaitLimits wl) {
     using R = typename Codec<S>::Real;
-    using Sh = RowPipeShape<L, S, kSegPitch, true>;
+    using Sh = SegShape<L, S, COLL>;
     constexpr int Q = L::Q;
     constexpr int NS = Sh::NS;
     constexpr int SB = Sh::SB;
@@ -650,10 +662,17 @@ __global__ void __launch_bounds__(RowPipeShape<L, S, kSegPitch, true>::CONSUMERS
         const uint8_t* mrow = has_mask ? mask_st + s * SB : nullptr;
         S* orow = static_cast<S*>(p.fout) + (long long)row * nx + x0;
         const uint32_t cell0 = (uint32_t)((long long)row * nx + x0) + p.cell_base;
+        if constexpr (kRowPair<L, S, COLL>) {
+            // pairs (xl, xl + 1): w is even, the halos hold both neighbours
 #pragma unroll 1
-        for (int xl = tid; xl < w; xl += Sh::CONSUMERS)
-            row_cell<L, S, SB, COLL>(p, st, mrow, xl, xl - 1, xl + 1, xl, xl, sc, isc, orow, rnd,
-                                     cell0 + (uint32_t)xl);
+            for (int xl = 2 * tid; xl < w; xl += 2 * Sh::CONSUMERS)
+                row_pair<L, S, SB, COLL>(p, st, mrow, xl, xl - 1, xl + 2, sc, isc, orow, rnd, cell0 + (uint32_t)xl);
+        } else {
+#pragma unroll 1
+            for (int xl = tid; xl < w; xl += Sh::CONSUMERS)
+                row_cell<L, S, SB, COLL>(p, st, mrow, xl, xl - 1, xl + 1, xl, xl, sc, isc, orow, rnd,
+                                         cell0 + (uint32_t)xl);
+        }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
     }

@@ -251,7 +251,7 @@ static int seg_width(int w) { return LBM_ROWPIPE_SEGW > 0 ? std::min(LBM_ROWPIPE
 template <class L, class S, int PITCH, int COLL>
 static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s) {
     if (rows_segmented(c)) {
-        using Sh = RowPipeShape<L, S, kSegPitch, true>;
+        using Sh = SegShape<L, S, COLL>;
         k_step_rows_seg<L, S, COLL><<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err,
                                                                                               c->waits);
         return;
@@ -268,7 +268,7 @@ static int prepare_rows_t(lbm_ctx* c) {
     long long groups = 0;
     int gy = 1;
     if (rows_segmented(c)) {
-        using Sh = RowPipeShape<L, S, kSegPitch, true>;
+        using Sh = SegShape<L, S, COLL>;
         auto kern = k_step_rows_seg<L, S, COLL>;
         LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
         LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
