@@ -733,8 +733,9 @@ def run_ensemble(args, rank, world, local_rank):
     barrier(torch, world)
     el_max = reduce_max(torch, el, dev, world)
     tile = batch.tile_info()
-    mode = {lb.BATCH_TILES: "tiles", lb.BATCH_ROWS: "rows+tiles"}.get(batch.mode(), "auto")
-    families = len({d.lattice for d, _, _ in mine})
+    mode = {lb.BATCH_TILES: "tiles", lb.BATCH_ROWS: "rows, one launch for both families",
+            lb.BATCH_ROWS_PER_FAMILY: "rows, one launch per family"}.get(batch.mode(), "auto")
+    launches, group2, group3 = batch.plan()
     batch.close()
     del batch
 
@@ -772,15 +773,17 @@ def run_ensemble(args, rank, world, local_rank):
                    "l2": f"inputs larger than L2: {total_bytes / 2 / 1e9:.2f} GB of populations per buffer set",
                    "parallelism": f"LPT shards x{world}" if world > 1 else "single GPU",
                    "members_per_rank": [len(p) for p in parts], "cells_this_rank": my_cells,
-                   "batch_mode": mode, "tile_width": tile[0], "tiles": tile[1]},
+                   "batch_mode": mode, "launches_per_step": launches,
+                   "row_group_bytes": {"d2q9": group2, "d3q27": group3}, "tile_width": tile[0], "tiles": tile[1]},
         "roofline": {"bound": "hbm", "achieved": achieved / world, "peak": peak, "unit": "GB/s",
                      "frac": achieved / world / peak, "traffic": None,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s",
-                     "kernel": "k_batch_rows<D2Q9/D3Q27> (+ k_batch_bgk tiles)" if mode == "rows+tiles"
-                     else "k_batch_bgk<D2Q9> + k_batch_bgk<D3Q27>",
+                     "kernel": {"tiles": "k_batch_bgk<D2Q9> + k_batch_bgk<D3Q27>",
+                                "rows, one launch for both families": "k_batch_rows_mix",
+                                "rows, one launch per family": "k_batch_rows<D2Q9> + k_batch_rows<D3Q27>"}.get(mode, mode),
                      "note": "achieved per GPU: algorithmic bytes of all members / max-over-ranks time / ranks"},
-        "gpu_launches": args.steps * families,
+        "gpu_launches": args.steps * launches,
         "clocks": clocks,
     }
     if el32 > 0:
@@ -837,7 +840,8 @@ def config_lines(torch, lb, args, dev, world):
     keep = ("value", "unit", "ms_per_step", "roofline", "fp32_batched", "speedup_f16s_vs_f32", "sequential_plain",
             "speedup_batched_vs_sequential", "clocks", "gpu_launches", "steps")
     out["ensemble_config5"] = {k: e[k] for k in keep if k in e}
-    out["ensemble_config5"]["config"] = {k: e["config"][k] for k in ("members", "cells", "storage", "l2", "batch_mode")}
+    out["ensemble_config5"]["config"] = {k: e["config"][k] for k in ("members", "cells", "storage", "l2", "batch_mode",
+                                                                      "launches_per_step", "row_group_bytes")}
     return out
 
 

@@ -470,7 +470,7 @@ __device__ __forceinline__ void mrt_pre(R (&T)[27], R isc, R& rho, R& drho, R& u
 }
 
 // Relaxation towards the equilibrium moments of (rho, u), inverse transform, direction order.
-template <int BASIS, class R, class K>
+template <int BASIS, bool EXACT, class R, class K>
 __device__ __forceinline__ void mrt_post(R (&T)[27], R rho, R drho, R ux, R uy, R uz, const MrtCoef<K>& k,
                                          R (&out)[27]) {
     using L = D3Q27;
@@ -486,7 +486,7 @@ __device__ __forceinline__ void mrt_post(R (&T)[27], R rho, R drho, R ux, R uy, 
     q[8] = q[1] * uz;
     q[9] = q[2] * uz;
     q[10] = mad(uz, uz, mad(uy, uy, ux * ux));
-    mrt_relax<BASIS>(T, q, k);
+    mrt_relax<BASIS, EXACT>(T, q, k);
     mrt_inverse<BASIS>(T);
     static_for<27>([&](auto I) {
         constexpr int i = I;
@@ -501,7 +501,7 @@ __device__ __forceinline__ void mrt_collide(const P& p, int cls, uint32_t fl, R 
     R rho, drho, ux, uy, uz;
     mrt_pre<BASIS>(T, isc, rho, drho, ux, uy, uz);
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, 3);
-    mrt_post<BASIS>(T, rho, drho, ux, uy, uz, p.mrt, out);
+    mrt_post<BASIS, EXACTW>(T, rho, drho, ux, uy, uz, p.mrt, out);
     if (fl & kEquilibrium) equilibrium_dev<L, EXACTW, R>(rho, drho, ux, uy, uz, sc, out);
 }
 

@@ -161,10 +161,15 @@ LBM_HD void mrt_inverse(R (&T)[27]) {
 
 // Relaxation coefficients of one lattice: T'[t] = alpha[t] T[t] + beta[t] meq[t] for unmixed
 // slots, and a 3x3 pair (A, B) for the mixed slots (2, 6, 18).  Scales of the inverse included.
+// The conserved slots (rho and j: tensor slots 0, 1, 3, 9) also carry their rate s and slot scale d
+// (the inverse's per-axis scales, e.g. 1/27 and 1/18 for the Gram-Schmidt basis) as d = dhi + dlo in
+// two floats: see mrt_relax.
 template <class R>
 struct MrtCoef {
     R alpha[27], beta[27], A[9], B[9];
+    R cs[4], chi[4], clo[4];
 };
+LBM_HD constexpr int mrt_conserved_index(int t) { return t == 0 ? 0 : t == 1 ? 1 : t == 3 ? 2 : t == 9 ? 3 : -1; }
 
 // Coefficients of the two-rate Gram-Schmidt collision (mrt2_collide in kernels.cuh): every row relaxes
 // at s_o except the five shear rows (4-6: cx cy, cx cz, cy cz; 8, 9: the traceless second-order
@@ -219,13 +224,25 @@ LBM_HD R mrt_meq(const R (&q)[11]) {
 
 // m* = relaxed, scaled moments.  q: cell quantities for the equilibrium.  K: coefficient type (the
 // scalar of R).
-template <int BASIS, class R, class K>
+// EXACT (FP32 storage): the conserved slots relax as d * (T + s (meq - T)) with d applied as two floats.
+// alpha + beta of a single-float pair differs from the slot scale d by ~1e-8 whenever d is not a power
+// of two (every Gram-Schmidt slot: 1/27, 1/18, ...), and a conserved moment has no restoring force, so
+// that scale error compounds step after step: the FP32 MRT cavity's velocity drifted 1.2e-4 from FP64
+// over 5,000 steps (256^3, config rates).  The other slots relax towards their equilibria, where a scale
+// error of 1e-8 only shifts the relaxation rate by as much.
+template <int BASIS, bool EXACT = false, class R, class K>
 LBM_HD void mrt_relax(R (&T)[27], const R (&q)[11], const MrtCoef<K>& k) {
     static_for<27>([&](auto TI) {
         constexpr int t = TI;
         if constexpr (mrt_slot_row(t) >= 0) {
             const R e = mrt_meq<BASIS, t>(q);
-            T[t] = mad(R(k.alpha[t]), T[t], R(k.beta[t]) * e);
+            constexpr int ci = mrt_conserved_index(t);
+            if constexpr (EXACT && ci >= 0) {
+                const R x = mad(R(k.cs[ci]), e - T[t], T[t]);
+                T[t] = mad(R(k.chi[ci]), x, R(k.clo[ci]) * x);
+            } else {
+                T[t] = mad(R(k.alpha[t]), T[t], R(k.beta[t]) * e);
+            }
         }
     });
     const R a = T[2], b = T[6], c = T[18];

@@ -185,6 +185,13 @@ static StepParams<R> make_params(const lbm_ctx* c) {
             p.mrt.A[t] = R(k.A[t]);
             p.mrt.B[t] = R(k.B[t] * es);
         }
+        const int cslot[4] = {0, 1, 3, 9};
+        for (int j = 0; j < 4; ++j) {
+            const double dsc = mrt_slot_scale(d.mrt_basis, cslot[j]);
+            p.mrt.cs[j] = R(d.mrt_s[mrt_slot_row(cslot[j])]);
+            p.mrt.chi[j] = R(dsc);
+            p.mrt.clo[j] = R(dsc - (double)R(dsc));
+        }
         if (c->mrt2) {
             const double so = d.mrt_s[0], sv = d.mrt_s[4], dv = sv - so;
             p.mrt2.om1 = R(1.0 - so);
