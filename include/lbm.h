@@ -179,6 +179,16 @@ int   lbm_get_desc(const lbm_ctx* c, lbm_desc* out);
  * memory = LBM_DEVICE: asynchronous on the context stream; LBM_HOST: returns when the copy is done. */
 int   lbm_face_get(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, void* dst, int memory);
 int   lbm_face_set(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, const void* src, int memory);
+/* One time step over planes [first, first + count) of the slowest axis only (z planes of D3Q27, y rows of
+ * D2Q9), from the current buffer into the other one, asynchronously on the context stream.  Calls for
+ * disjoint ranges that together cover every plane make one step; the last of them passes finish = 1,
+ * which makes the written buffer current.  This lets a slab of a decomposed lattice update its two
+ * boundary planes first, exchange their faces while its interior planes are updated, and finish the
+ * step (no counterpart in the reference).  BGK and MRT; not Shan-Chen.  Planes outside the ranges
+ * keep whatever the other buffer held.                                                             */
+int   lbm_step_planes(lbm_ctx* c, int64_t first, int64_t count, int finish);
+/* Both population buffers: the current one and the one the next step writes (device pointers). */
+int   lbm_device_buffers(lbm_ctx* c, void** current, void** next, size_t* bytes);
 /* Index of this lattice's first cell within a larger lattice it is a part of (a slab of a decomposed
  * lattice; any integer, taken modulo 2^32; default 0).  Stochastic rounding hashes that global index
  * with the step number, so the slabs of a decomposed lattice round exactly like the undivided lattice.

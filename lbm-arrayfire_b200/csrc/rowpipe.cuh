@@ -442,10 +442,13 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
     const int lane = tid & 31;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int B = rows;
-    const int gy = (ny + B - 1) / B;  // row groups per z plane; the last one may be short
+    // the launch updates planes [plo, plo + pcnt) of the slowest axis (z for D3Q27, y for D2Q9)
+    const int ybeg = L::DIM == 2 ? p.plo : 0, yend = L::DIM == 2 ? p.plo + p.pcnt : ny;
+    const int zbeg = L::DIM == 3 ? p.plo : 0, zcnt = L::DIM == 3 ? p.pcnt : nz;
+    const int gy = (yend - ybeg + B - 1) / B;  // row groups per z plane; the last one may be short
     // item indices in 32 bits (the host keeps the item count below 2^31): a 64-bit division by a
     // runtime divisor is a long software sequence, paid once per stage by every consumer thread
-    const unsigned groups = (unsigned)gy * (unsigned)nz, ugy = (unsigned)gy;
+    const unsigned groups = (unsigned)gy * (unsigned)zcnt, ugy = (unsigned)gy;
     const uint32_t row_bytes = (uint32_t)(nx * sizeof(S));
     const unsigned first = blockIdx.x, stride = gridDim.x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
@@ -453,8 +456,8 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
     // Issue the bulk loads of group g into stage s (one warp; lanes 0..Q-1 one direction each).
     auto issue = [&](unsigned g, int s) {
         if (g == wl.skip) return;  // test hook: this item's stage is never filled
-        const int y0 = (int)(g % ugy) * B, z = (int)(g / ugy);
-        const int nb = ny - y0 < B ? ny - y0 : B;
+        const int y0 = ybeg + (int)(g % ugy) * B, z = zbeg + (int)(g / ugy);
+        const int nb = yend - y0 < B ? yend - y0 : B;
         if (lane == 0)
             mbar_arrive_expect_tx(&full[s], (uint32_t)(Q * nb) * row_bytes + (has_mask ? (uint32_t)(nb * nx) : 0u));
         __syncwarp();
@@ -518,8 +521,8 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
                     break;
             return;
         }
-        const int y0 = (int)(g % ugy) * B, z = (int)(g / ugy);
-        const int nb = ny - y0 < B ? ny - y0 : B;
+        const int y0 = ybeg + (int)(g % ugy) * B, z = zbeg + (int)(g / ugy);
+        const int nb = yend - y0 < B ? yend - y0 : B;
         const S* st0 = in + (long long)s * Q * SB;
         const uint8_t* ms0 = has_mask ? mask_st + s * SB : nullptr;
         S* out0 = static_cast<S*>(p.fout) + ((long long)z * ny + y0) * nx;
@@ -582,15 +585,20 @@ __global__ void __launch_bounds__(SegShape<L, S, COLL>::CONSUMERS + 32, SegShape
     const int lane = tid & 31;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int nseg = (nx + SW - 1) / SW;
-    const unsigned groups = (unsigned)nseg * (unsigned)ny * (unsigned)nz;  // < 2^31 (host-checked)
+    // the launch updates rows [row0, row0 + nrows) (global row index y + ny z): the planes [plo, plo + pcnt)
+    // of the slowest axis
+    const unsigned row0 = L::DIM == 3 ? (unsigned)p.plo * (unsigned)ny : (unsigned)p.plo;
+    const unsigned nrows = L::DIM == 3 ? (unsigned)p.pcnt * (unsigned)ny : (unsigned)p.pcnt;
+    const unsigned groups = (unsigned)nseg * nrows;  // < 2^31 (host-checked)
     const unsigned useg = (unsigned)nseg, uny = (unsigned)ny;
     const unsigned first = blockIdx.x, stride = gridDim.x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
 
     auto issue = [&](unsigned g, int s) {
         if (g == wl.skip) return;  // test hook: this item's stage is never filled
-        const unsigned row = g / useg;
-        const int seg = (int)(g - row * useg);
+        const unsigned gq = g / useg;
+        const unsigned row = row0 + gq;
+        const int seg = (int)(g - gq * useg);
         const int z = (int)(row / uny), y = (int)(row - (unsigned)z * uny);
         const int x0 = seg * SW;
         const int w = nx - x0 < SW ? nx - x0 : SW;
@@ -654,8 +662,9 @@ __global__ void __launch_bounds__(SegShape<L, S, COLL>::CONSUMERS + 32, SegShape
                     break;
             return;
         }
-        const unsigned row = g / useg;
-        const int seg = (int)(g - row * useg);
+        const unsigned gq = g / useg;
+        const unsigned row = row0 + gq;
+        const int seg = (int)(g - gq * useg);
         const int x0 = seg * SW;
         const int w = nx - x0 < SW ? nx - x0 : SW;
         const S* st = in + (long long)s * Q * SB + H;  // staged index of x0 is 0

@@ -163,6 +163,8 @@ static StepParams<R> make_params(const lbm_ctx* c) {
     p.tick = c->tick;
     p.sr = d.rounding == LBM_ROUND_STOCHASTIC ? 1 : 0;
     p.cell_base = (uint32_t)c->cell_offset;
+    p.plo = 0;
+    p.pcnt = (int)(d.lattice == LBM_D3Q27 ? d.nz : d.ny);
     for (int k = 0; k < kMaxClasses; ++k) {
         const bool used = k < d.n_classes;
         p.cls.flags[k] = used ? d.classes[k].flags : 0u;
@@ -385,7 +387,14 @@ static int prepare_rows(lbm_ctx* c) {
 }
 
 // Launch one time step reading buffer `from` and writing the other one.
-static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
+// Launch one time step reading buffer `from` and writing the other one, over planes [plo, plo + pcnt)
+// of the slowest axis (pcnt < 0: all of them; Shan-Chen always steps every plane).
+static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo = 0, int pcnt = -1) {
+    const int planes = (int)(c->d.lattice == LBM_D3Q27 ? c->d.nz : c->d.ny);
+    if (pcnt < 0) {
+        plo = 0;
+        pcnt = planes;
+    }
     if (c->kernel_used == LBM_KERNEL_ROWS && c->d.collision == LBM_SHANCHEN) {
         const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
         dispatch_storage(c->d.storage, [&](auto tag) {
@@ -413,11 +422,15 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
             p.fin = c->f[from];
             p.fout = c->f[from ^ 1];
             p.parity = from;
+            p.plo = plo;
+            p.pcnt = pcnt;
             launch_rows_t<L, S, decltype(pi)::value, decltype(co)::value>(c, p, s);
         });
         return;
     }
-    const dim3 blk(block), grid((unsigned)((c->d.nx + block - 1) / block), (unsigned)c->d.ny, (unsigned)c->d.nz);
+    const bool d3 = c->d.lattice == LBM_D3Q27;
+    const dim3 blk(block), grid((unsigned)((c->d.nx + block - 1) / block), (unsigned)(d3 ? c->d.ny : pcnt),
+                                (unsigned)(d3 ? pcnt : c->d.nz));
     dispatch_storage(c->d.storage, [&](auto tag) {
         using S = typename decltype(tag)::type;
         using R = typename Codec<S>::Real;
@@ -425,6 +438,8 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block) {
         p.fin = c->f[from];
         p.fout = c->f[from ^ 1];
         p.parity = from;
+        p.plo = plo;
+        p.pcnt = pcnt;
         const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
         switch (c->d.collision) {
             case LBM_BGK:
@@ -1069,6 +1084,36 @@ int lbm_set_kernel(lbm_ctx* c, int kind) {
 }
 
 int lbm_get_kernel(const lbm_ctx* c) { return c ? c->kernel_used : 0; }
+
+int lbm_step_planes(lbm_ctx* c, int64_t first, int64_t count, int finish) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    const long long planes = c->d.lattice == LBM_D3Q27 ? c->d.nz : c->d.ny;
+    if (first < 0 || count < 1 || first + count > planes)
+        return set_error(LBM_ERR_INVALID, "plane range outside the lattice's slowest axis");
+    if (c->d.collision == LBM_SHANCHEN)
+        return set_error(LBM_ERR_UNSUPPORTED, "Shan-Chen steps every plane at once (its force reads psi of the neighbours)");
+    LBM_CK(cudaSetDevice(c->d.device));
+    if (!c->kernel_used) {
+        int rc = autotune(c);
+        if (rc) return rc;
+    }
+    launch_step(c, c->cur, c->stream, c->block, (int)first, (int)count);
+    LBM_CK(cudaGetLastError());
+    if (finish) {
+        c->cur ^= 1;
+        c->has_prev = true;
+        c->steps += 1;
+    }
+    return LBM_OK;
+}
+
+int lbm_device_buffers(lbm_ctx* c, void** current, void** next, size_t* bytes) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    if (current) *current = c->f[c->cur];
+    if (next) *next = c->f[c->cur ^ 1];
+    if (bytes) *bytes = (size_t)c->N * c->q * c->sbytes;
+    return LBM_OK;
+}
 
 int lbm_set_cell_offset(lbm_ctx* c, int64_t offset) {
     if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");

@@ -118,6 +118,8 @@ _SIGS = {
     "lbm_get_kernel": (C.c_int, [_P]),
     "lbm_test_stall_next_step": (C.c_int, [_P, C.c_int64, C.c_int64]),
     "lbm_set_cell_offset": (C.c_int, [_P, C.c_int64]),
+    "lbm_step_planes": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int]),
+    "lbm_device_buffers": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(C.c_size_t)]),
     "lbm_sums_fp64_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_double, _P, _P]),
     "lbm_batch_create": (C.c_int, [_DP, C.c_int, C.POINTER(_P)]),
     "lbm_batch_destroy": (None, [_P]),
@@ -356,6 +358,16 @@ class Lattice:
 
     def kernel(self) -> int:
         return lib().lbm_get_kernel(self._h)
+
+    def step_planes(self, first: int, count: int, finish: bool):
+        """One step over planes [first, first + count) of the slowest axis (lbm_step_planes)."""
+        _check(lib().lbm_step_planes(self._h, first, count, 1 if finish else 0))
+
+    def device_buffers(self):
+        """(current, next, bytes): device pointers of both population buffers."""
+        cur, nxt, nb = _P(), _P(), C.c_size_t()
+        _check(lib().lbm_device_buffers(self._h, C.byref(cur), C.byref(nxt), C.byref(nb)))
+        return cur.value, nxt.value, nb.value
 
     def set_cell_offset(self, offset: int):
         """Index of this lattice's cell 0 in the lattice it is a slab of (stochastic rounding's hash)."""

@@ -17,6 +17,13 @@ are never read, and bounce-back keeps them finite.  The exchange is point-to-poi
 and it is the only data-path communication.  Shan-Chen is not decomposed (its force needs psi of the
 neighbour planes as a second exchange per step).
 
+On a GPU the exchange overlaps the interior update (`lbm_step_planes`): a step first updates the two
+boundary planes (local planes 1 and n), then a second CUDA stream packs their outgoing faces straight
+from the buffer being written, exchanges them (NCCL, or copies within one process) and unpacks the
+incoming ones into that buffer's ghost planes, while the main stream updates planes 2 .. n-1 and
+finishes the step; the next step waits for both.  Slabs of fewer than three planes, and steppers
+without plane ranges (the oracle in the CPU tests), step whole and exchange afterwards.
+
 `Slab` is one rank's part (one process per GPU).  `SlabSet` holds every rank's part in one process and
 exchanges by plain copies, for tests and for several slabs on one device.
 """
@@ -90,6 +97,22 @@ def scatter_populations(desc: Desc, F, p0: int, p1: int) -> np.ndarray:
     return np.ascontiguousarray(G[:, idx, :]).ravel()
 
 
+def _device_bytes(ptr: int, nbytes: int, device):
+    """A torch uint8 tensor viewing `nbytes` of device memory at `ptr` (no copy; the memory stays the
+    lattice's)."""
+    import torch
+
+    class _View:
+        __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_View(), device=device)
+
+
+def _plane_bytes(F, N: int, pc: int, s: int, dirs, plane: int):
+    """Byte views of plane `plane` of each direction in `dirs` (each one contiguous run in the layout)."""
+    return [F[(i * N + plane * pc) * s:(i * N + plane * pc + pc) * s] for i in dirs]
+
+
 def _interior(lat, n: int, dtype=np.float64) -> np.ndarray:
     F = lat.get_populations(dtype)
     return F.reshape(lat.q, n + 2, -1)[:, 1:n + 1, :]
@@ -99,10 +122,12 @@ class Slab:
     """One rank's slab of a lattice, stepped with halo exchanges over a torch.distributed group.
 
     lattice_factory(desc, mask) builds the local stepper (default: a GPU `Lattice`); it must offer
-    step, face_get, face_set, get_populations, set_populations, set_stream and face_cells."""
+    step, face_get, face_set, get_populations, set_populations, set_stream and face_cells.  A GPU
+    stepper that also offers step_planes and device_buffers gets the overlapped step unless
+    `overlap=False` (then: step, then exchange)."""
 
     def __init__(self, desc: Desc, mask, F0, rank: int, world: int, group=None, device=None,
-                 lattice_factory=None):
+                 lattice_factory=None, overlap: bool = True):
         import torch
         import torch.distributed as dist
 
@@ -121,7 +146,8 @@ class Slab:
         self.up_dirs, self.down_dirs = axis_dirs(desc.lattice)
         self.device = torch.device(device) if device is not None else torch.device("cpu")
         if self.device.type == "cuda":
-            # one stream for the steps, the face copies and the NCCL transfers: ordered without events
+            # the steps run on torch's current stream; so does the exchange of a sequential step, while
+            # an overlapped step exchanges on a side stream ordered by events
             self.lat.set_stream(torch.cuda.current_stream(self.device).cuda_stream)
         # faces travel as raw bytes of the stored words (NCCL has no 16-bit integer type; a
         # point-to-point transfer never touches the values); an injected stepper uses FP64 words
@@ -130,6 +156,10 @@ class Slab:
         self._buf = {name: torch.empty(k, dtype=word, device=self.device)
                      for name in ("send_up", "send_down", "recv_down", "recv_up")}
         self.lat.set_populations(scatter_populations(desc, F0, self.p0, self.p1))
+        # the overlapped step (see the module docstring): GPU steppers with plane ranges, >= 3 planes
+        self.overlap = (overlap and self.device.type == "cuda" and hasattr(self.lat, "step_planes")
+                        and self.n >= 3)
+        self._comm = torch.cuda.Stream(device=self.device) if self.overlap else None
 
     def _pack(self):
         self.lat.face_get(self.n, self.up_dirs, self._buf["send_up"])
@@ -158,8 +188,50 @@ class Slab:
 
     def step(self, n: int = 1):
         for _ in range(n):
-            self.lat.step(1)
-            self.exchange()
+            if self.overlap:
+                self._step_overlapped()
+            else:
+                self.lat.step(1)
+                self.exchange()
+
+    def _step_overlapped(self):
+        """One step: boundary planes, then the face exchange on the side stream while the interior
+        planes are updated on the main stream."""
+        import torch
+
+        dist, lat, n, b = self.dist, self.lat, self.n, self._buf
+        main = torch.cuda.current_stream(self.device)
+        lat.step_planes(1, 1, False)
+        lat.step_planes(n, 1, False)
+        ready = torch.cuda.Event()
+        ready.record(main)
+        _, nxt, nbytes = lat.device_buffers()
+        F = _device_bytes(nxt, nbytes, self.device)
+        N, pc, sb = self.desc.cells, lat.face_cells(), STORAGE_BYTES[self.desc.storage]
+        with torch.cuda.stream(self._comm):
+            self._comm.wait_event(ready)
+            torch.cat(_plane_bytes(F, N, pc, sb, self.up_dirs, n), out=b["send_up"])
+            torch.cat(_plane_bytes(F, N, pc, sb, self.down_dirs, 1), out=b["send_down"])
+            if self.world == 1:
+                from_down, from_up = b["send_up"], b["send_down"]
+            else:
+                up, down = (self.rank + 1) % self.world, (self.rank - 1) % self.world
+                ops = [dist.P2POp(dist.isend, b["send_up"], up, self.group, tag=1),
+                       dist.P2POp(dist.irecv, b["recv_down"], down, self.group, tag=1),
+                       dist.P2POp(dist.isend, b["send_down"], down, self.group, tag=2),
+                       dist.P2POp(dist.irecv, b["recv_up"], up, self.group, tag=2)]
+                for req in dist.batch_isend_irecv(ops):
+                    req.wait()
+                from_down, from_up = b["recv_down"], b["recv_up"]
+            w = pc * sb
+            for k, dst in enumerate(_plane_bytes(F, N, pc, sb, self.up_dirs, 0)):
+                dst.copy_(from_down[k * w:(k + 1) * w])
+            for k, dst in enumerate(_plane_bytes(F, N, pc, sb, self.down_dirs, n + 1)):
+                dst.copy_(from_up[k * w:(k + 1) * w])
+            done = torch.cuda.Event()
+            done.record(self._comm)
+        lat.step_planes(2, n - 2, True)
+        main.wait_event(done)
 
     def interior_populations(self, dtype=np.float64) -> np.ndarray:
         """This rank's planes, [Q, n, plane cells]."""
@@ -201,7 +273,7 @@ class SlabSet:
     The same planes, ghost classes and exchange order as `Slab`, for parity tests on one device and
     for decompositions whose slabs share a GPU."""
 
-    def __init__(self, desc: Desc, mask, F0, parts: int, lattice_factory=None):
+    def __init__(self, desc: Desc, mask, F0, parts: int, lattice_factory=None, overlap: bool = False):
         self.global_desc = desc
         self.ranges = split_planes(_planes(desc), parts)
         self.up_dirs, self.down_dirs = axis_dirs(desc.lattice)
@@ -219,6 +291,15 @@ class SlabSet:
             if lattice_factory is None else np.float64
         self._up = [np.empty(k, dtype=word) for _ in self.lats]
         self._down = [np.empty(k, dtype=word) for _ in self.lats]
+        # overlapped steps (GPU lattices on torch's current stream, a side stream for the face copies)
+        self.overlap = overlap and lattice_factory is None and min(self.ns) >= 3
+        if self.overlap:
+            import torch
+
+            self._dev = torch.device("cuda", desc.device)
+            for lat in self.lats:
+                lat.set_stream(torch.cuda.current_stream(self._dev).cuda_stream)
+            self._comm = torch.cuda.Stream(device=self._dev)
 
     def exchange(self):
         R = len(self.lats)
@@ -231,9 +312,47 @@ class SlabSet:
 
     def step(self, n: int = 1):
         for _ in range(n):
+            if self.overlap:
+                self._step_overlapped()
+                continue
             for lat in self.lats:
                 lat.step(1)
             self.exchange()
+
+    def _step_overlapped(self):
+        """The overlapped step of `Slab`, for every slab of one device: boundary planes, face copies
+        between the slabs' next buffers on the side stream, interior planes on the main stream."""
+        import torch
+
+        main = torch.cuda.current_stream(self._dev)
+        for lat, n in zip(self.lats, self.ns):
+            lat.step_planes(1, 1, False)
+            lat.step_planes(n, 1, False)
+        ready = torch.cuda.Event()
+        ready.record(main)
+        sb = STORAGE_BYTES[self.global_desc.storage]
+        views = []
+        for lat in self.lats:
+            _, nxt, nbytes = lat.device_buffers()
+            views.append(_device_bytes(nxt, nbytes, self._dev))
+        R = len(self.lats)
+        with torch.cuda.stream(self._comm):
+            self._comm.wait_event(ready)
+            pc = self.lats[0].face_cells()
+            cells = [lat.desc.cells for lat in self.lats]
+            for r, n in enumerate(self.ns):
+                lo, hi = (r - 1) % R, (r + 1) % R
+                up = _plane_bytes(views[lo], cells[lo], pc, sb, self.up_dirs, self.ns[lo])
+                down = _plane_bytes(views[hi], cells[hi], pc, sb, self.down_dirs, 1)
+                for dst, src in zip(_plane_bytes(views[r], cells[r], pc, sb, self.up_dirs, 0), up):
+                    dst.copy_(src)
+                for dst, src in zip(_plane_bytes(views[r], cells[r], pc, sb, self.down_dirs, n + 1), down):
+                    dst.copy_(src)
+            done = torch.cuda.Event()
+            done.record(self._comm)
+        for lat, n in zip(self.lats, self.ns):
+            lat.step_planes(2, n - 2, True)
+        main.wait_event(done)
 
     def gather_populations(self, dtype=np.float64) -> np.ndarray:
         return np.concatenate([_interior(lat, n, dtype) for lat, n in zip(self.lats, self.ns)], axis=1).ravel()

@@ -180,9 +180,11 @@ def test_slab_gloo_ranks_equal_undivided_oracle(tmp_path, case, world):
 @pytest.mark.parametrize("storage", [lb.F32, lb.F16S])
 @pytest.mark.parametrize("case", ["mrt_cavity3d", "channel2d", "periodic3d", "mrt_rows"])
 @pytest.mark.parametrize("parts", [2, 3])
-def test_slabset_of_engine_lattices_equals_one_lattice(storage, case, parts):
+@pytest.mark.parametrize("overlap", [False, True])
+def test_slabset_of_engine_lattices_equals_one_lattice(storage, case, parts, overlap):
     """Slabs stepped by the engine (its kernel choice per slab: plain or row pipeline) and exchanged
-    by face_get/face_set: bit-identical to one lattice of the full size."""
+    by face_get/face_set, or overlapped (boundary planes, face copies between the slabs' buffers on a
+    side stream, interior planes): bit-identical to one lattice of the full size."""
     if case == "mrt_rows":
         d, m, F0 = mrt_cavity3d(storage, n=(128, 16, 24))  # row-pipeline eligible slabs
     else:
@@ -191,7 +193,8 @@ def test_slabset_of_engine_lattices_equals_one_lattice(storage, case, parts):
         lat.set_populations(np.asarray(F0, dtype=np.float64))
         lat.step(15)
         ref = lat.get_populations(np.float32)
-    s = SlabSet(d, m, F0, parts)
+    s = SlabSet(d, m, F0, parts, overlap=overlap)
+    assert s.overlap == (overlap and min(s.ns) >= 3)
     try:
         s.step(15)
         got = s.gather_populations(np.float32)
@@ -200,11 +203,68 @@ def test_slabset_of_engine_lattices_equals_one_lattice(storage, case, parts):
     assert np.isfinite(got).all() and np.array_equal(got, ref)
 
 
+def _plane_case(name, storage):
+    if name == "mrt3d":
+        return mrt_cavity3d(storage, n=(128, 16, 12))
+    if name == "mrt3d_seg":  # rows wider than 1024 cells: the segmented row kernel
+        return mrt_cavity3d(storage, n=(1040, 4, 6))
+    if name == "channel":
+        return channel(storage, nx=256, ny=40)
+    if name == "channel_seg":
+        return channel(storage, nx=1088, ny=12)
+    return periodic3d(storage, n=(64, 6, 7))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S])
+@pytest.mark.parametrize("kernel", [lb.KERNEL_PLAIN, lb.KERNEL_ROWS])
+@pytest.mark.parametrize("case", ["mrt3d", "mrt3d_seg", "channel", "channel_seg", "bgk3d"])
+def test_step_planes_in_pieces_equals_whole_steps(storage, kernel, case):
+    """lbm_step_planes: a step cut into plane ranges (in any order; the last one finishes it) is
+    bit-identical to lbm_step, for the plain kernels, the row pipeline and its segmented form, with
+    stochastic rounding on for the 16-bit storage."""
+    d, m, F0 = _plane_case(case, storage)
+    planes = d.nz if d.dim == 3 else d.ny
+    F0 = np.asarray(F0, dtype=np.float64)
+    with lb.Lattice(d, m) as a, lb.Lattice(d, m) as b:
+        for lat in (a, b):
+            lat.set_kernel(kernel)
+            lat.set_populations(F0)
+        a.step(6)
+        cuts = [[(0, 1), (planes - 1, 1), (1, planes - 2)],  # the slab order: boundary planes first
+                [(3, planes - 3), (0, 3)],
+                [(k, 1) for k in range(planes - 1, -1, -1)]]
+        for t in range(6):
+            pieces = cuts[t % len(cuts)]
+            for k, (first, count) in enumerate(pieces):
+                b.step_planes(first, count, k == len(pieces) - 1)
+        assert b.steps_done == a.steps_done == 6
+        ref, got = a.get_populations(np.float32), b.get_populations(np.float32)
+    assert np.isfinite(got).all() and np.array_equal(got, ref)
+
+
+@pytest.mark.gpu
+def test_step_planes_rejects_bad_ranges_and_shanchen():
+    d, m, _ = mrt_cavity3d(lb.F32, n=(32, 4, 5))
+    with lb.Lattice(d, m) as lat:
+        for first, count in ((-1, 1), (0, 0), (4, 2), (5, 1)):
+            with pytest.raises(lb.LbmError):
+                lat.step_planes(first, count, True)
+        assert lat.steps_done == 0
+    d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, lb.F32, (32, 16), omega=1.0, sc_G=-5.0)
+    with lb.Lattice(d, None) as lat:
+        with pytest.raises(lb.LbmError):
+            lat.step_planes(0, 16, True)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("storage", [lb.F32, lb.BF16S])
-def test_one_rank_slab_on_the_gpu_equals_one_lattice(storage):
+@pytest.mark.parametrize("overlap", [False, True])
+def test_one_rank_slab_on_the_gpu_equals_one_lattice(storage, overlap):
     """The rank-side Slab with CUDA byte buffers on torch's stream: with one rank its ghost planes are
-    filled from its own far planes (the periodic wrap), so it equals the undivided lattice."""
+    filled from its own far planes (the periodic wrap), so it equals the undivided lattice.  Both the
+    sequential step and the overlapped one (faces packed from the buffer being written, on a side
+    stream, while the interior planes are updated)."""
     import torch
 
     d, m, F0 = mrt_cavity3d(storage, n=(128, 16, 12))
@@ -213,7 +273,8 @@ def test_one_rank_slab_on_the_gpu_equals_one_lattice(storage):
         lat.step(10)
         ref = lat.get_populations(np.float32)
         ref_sums = lat.sums()
-    slab = Slab(d, m, F0, 0, 1, device="cuda:0")
+    slab = Slab(d, m, F0, 0, 1, device="cuda:0", overlap=overlap)
+    assert slab.overlap == overlap
     assert slab._buf["send_up"].dtype == torch.uint8 and slab._buf["send_up"].is_cuda
     slab.step(10)
     torch.cuda.synchronize()
