@@ -922,6 +922,65 @@ def run_ours(args, rank, world, local_rank):
     return out
 
 
+def run_slab(args, rank, world, local_rank):
+    """The workload's lattice split into `world` slabs along its slowest axis (lbm_b200.slab.Slab, one
+    rank per GPU, faces over NCCL; with one rank the faces wrap onto the rank itself).  Times the
+    overlapped step (interior planes beside the boundary planes and the face exchange) and the
+    sequential one (step, then exchange) with CUDA events on the slab's stream, max over ranks, and
+    the undivided lattice at one rank.  Strong scaling: the global lattice is fixed."""
+    import torch
+
+    import lbm_b200 as lb
+    from lbm_b200.slab import Slab
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    storage = STORAGES[args.storage]
+    d, m = build_workload(lb, args, storage)
+    d.device = local_rank
+    _, _, _, w, _ = lb.velocities(d.lattice)
+    F0 = np.repeat(np.asarray(w, dtype=np.float32), d.cells)  # rest state
+
+    def timed(slab):
+        slab.step(max(args.warmup, 1))
+        torch.cuda.synchronize(dev)
+        barrier(torch, world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(slab.stream)
+        slab.step(args.steps)
+        e1.record(slab.stream)
+        e1.synchronize()
+        el = reduce_max(torch, e0.elapsed_time(e1) / 1e3, dev, world)
+        barrier(torch, world)
+        return el
+
+    out = {}
+    for overlap in (True, False):
+        slab = Slab(d, m, F0, rank, world, device=dev, overlap=overlap)
+        out[overlap] = (timed(slab), slab.overlap)
+        slab.close()
+    whole = None
+    if world == 1:
+        with lb.Lattice(d, m) as lat:
+            lat.set_populations(F0)
+            lat.step(max(args.warmup, 1))
+            lat.sync()
+            whole = timed_steps(torch, lat, args.steps, dev)
+    el, used = out[True]
+    return {
+        "metric": METRIC, "value": d.cells * args.steps / el / 1e6, "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (rest state)",
+        "config": {"workload": args.workload, "storage": args.storage, "shape": list(d.shape),
+                   "parallelism": f"slab x{world}", "overlap": used, "reserved_sms": 8,
+                   "exchange": "nccl p2p" if world > 1 else "faces wrap onto the one rank",
+                   "l2": "inputs larger than L2"},
+        "sequential_ms_per_step": out[False][0] / args.steps * 1e3,
+        "undivided_ms_per_step": whole / args.steps * 1e3 if whole else None,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -947,6 +1006,8 @@ def main():
     ap.add_argument("--rounding", default="stochastic", choices=["stochastic", "nearest"],
                     help="rounding of 16-bit storage in the timed runs")
     ap.add_argument("--block", type=int, default=0, help="fixed block width (default: autotune)")
+    ap.add_argument("--slab", action="store_true",
+                    help="slab decomposition of the workload over the ranks (overlapped and sequential exchange)")
     args = ap.parse_args()
     if args.warmup < 0 or args.steps < 1:
         raise SystemExit("steps must be >= 1 and warmup >= 0")
@@ -975,7 +1036,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device(f"cuda:{local_rank}"))
     try:
-        out = (run_ensemble if args.workload == "ensemble_config5" else run_ours)(args, rank, world, local_rank)
+        if args.slab:
+            out = run_slab(args, rank, world, local_rank)
+        else:
+            out = (run_ensemble if args.workload == "ensemble_config5" else run_ours)(args, rank, world, local_rank)
         if rank == 0:
             print(json.dumps(out), flush=True)
     finally:

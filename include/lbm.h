@@ -168,7 +168,8 @@ int  lbm_last_step_ms(lbm_ctx* c, float* ms);
 int64_t lbm_steps_done(const lbm_ctx* c);
 /* The context's CUDA stream (cudaStream_t) and device buffers, for callers that interoperate. */
 void* lbm_stream(lbm_ctx* c);
-int   lbm_set_stream(lbm_ctx* c, void* stream);          /* NULL restores the context's own */
+/* NULL restores the context's own (non-blocking) stream; the legacy default stream is cudaStreamLegacy. */
+int   lbm_set_stream(lbm_ctx* c, void* stream);
 /* Current population buffer on the device (storage type of the descriptor) and its byte size. */
 void* lbm_device_populations(lbm_ctx* c, size_t* bytes);
 int   lbm_get_desc(const lbm_ctx* c, lbm_desc* out);
@@ -179,14 +180,22 @@ int   lbm_get_desc(const lbm_ctx* c, lbm_desc* out);
  * memory = LBM_DEVICE: asynchronous on the context stream; LBM_HOST: returns when the copy is done. */
 int   lbm_face_get(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, void* dst, int memory);
 int   lbm_face_set(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs, const void* src, int memory);
-/* One time step over planes [first, first + count) of the slowest axis only (z planes of D3Q27, y rows of
- * D2Q9), from the current buffer into the other one, asynchronously on the context stream.  Calls for
- * disjoint ranges that together cover every plane make one step; the last of them passes finish = 1,
- * which makes the written buffer current.  This lets a slab of a decomposed lattice update its two
- * boundary planes first, exchange their faces while its interior planes are updated, and finish the
- * step (no counterpart in the reference).  BGK and MRT; not Shan-Chen.  Planes outside the ranges
- * keep whatever the other buffer held.                                                             */
-int   lbm_step_planes(lbm_ctx* c, int64_t first, int64_t count, int finish);
+/* One time step over planes first + k * stride, k < count, of the slowest axis only (z planes of D3Q27,
+ * y rows of D2Q9), from the current buffer into the other one, in one launch, asynchronously on
+ * `stream` (a cudaStream_t; NULL: the context stream).  Calls for disjoint plane sets that together
+ * cover every plane make one step; the last of them passes finish = 1, which makes the written buffer
+ * current.  Calls on different streams may run at the same time (they read one buffer and write
+ * disjoint planes of the other); the caller orders every one of them before the next step's first
+ * launch.  This lets a slab of a decomposed lattice update its two boundary planes (first 1, count 2,
+ * stride n - 1) and exchange their faces on a side stream while its interior planes are updated (no
+ * counterpart in the reference).  BGK and MRT; not Shan-Chen.  Planes outside the sets keep whatever
+ * the other buffer held.                                                                           */
+int   lbm_step_planes(lbm_ctx* c, int64_t first, int64_t count, int64_t stride, int finish, void* stream);
+/* Splits the SMs between the context stream and side streams for the row pipeline's persistent grid
+ * (0..64; default 0): its launches on the context stream leave `sms` SMs free, so that kernels on
+ * another stream (a face exchange, a collective) run beside a step instead of after it, and its
+ * lbm_step_planes launches on another stream use at most those `sms` SMs (with sms > 0).            */
+int   lbm_set_reserved_sms(lbm_ctx* c, int sms);
 /* Both population buffers: the current one and the one the next step writes (device pointers). */
 int   lbm_device_buffers(lbm_ctx* c, void** current, void** next, size_t* bytes);
 /* Index of this lattice's first cell within a larger lattice it is a part of (a slab of a decomposed

@@ -136,7 +136,9 @@ extern "C" {
     pub fn lbm_get_desc(c: *const lbm_ctx, out: *mut lbm_desc) -> c_int;
     pub fn lbm_face_get(c: *mut lbm_ctx, plane: i64, dirs: *const i32, ndirs: i32, dst: *mut c_void, memory: c_int) -> c_int;
     pub fn lbm_face_set(c: *mut lbm_ctx, plane: i64, dirs: *const i32, ndirs: i32, src: *const c_void, memory: c_int) -> c_int;
-    pub fn lbm_step_planes(c: *mut lbm_ctx, first: i64, count: i64, finish: c_int) -> c_int;
+    pub fn lbm_step_planes(c: *mut lbm_ctx, first: i64, count: i64, stride: i64, finish: c_int,
+                           stream: *mut c_void) -> c_int;
+    pub fn lbm_set_reserved_sms(c: *mut lbm_ctx, sms: c_int) -> c_int;
     pub fn lbm_device_buffers(c: *mut lbm_ctx, current: *mut *mut c_void, next: *mut *mut c_void,
                               bytes: *mut usize) -> c_int;
     pub fn lbm_set_cell_offset(c: *mut lbm_ctx, offset: i64) -> c_int;

@@ -48,8 +48,9 @@ struct StepParams {
     int parity;           // the input buffer of this launch: it reads tick[parity], writes tick[parity ^ 1]
     int sr;               // 16-bit storage: 1 stochastic rounding, 0 round to nearest
     uint32_t cell_base;   // index of cell 0 in the lattice this one is part of (the rounding's hash input)
-    int plo, pcnt;        // the step kernels update planes [plo, plo + pcnt) of the slowest axis (z for D3Q27,
-                          // y for D2Q9; lbm_step_planes); 0 and every plane for a whole step
+    int plo, pcnt, pstride;  // the step kernels update planes plo + k pstride, k < pcnt, of the slowest axis
+                             // (z for D3Q27, y for D2Q9; lbm_step_planes); 0, every plane and 1 for a
+                             // whole step
     ClassTable<R> cls;
     MrtCoef<R> mrt;
     Mrt2Coef<R> mrt2;
@@ -447,7 +448,8 @@ __global__ void __launch_bounds__(512) k_step_bgk(const __grid_constant__ StepPa
     if (x >= p.nx) return;
     const bool designated = (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0;
     const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, designated);
-    const int y = blockIdx.y + (L::DIM == 2 ? p.plo : 0), z = blockIdx.z + (L::DIM == 3 ? p.plo : 0);
+    const int y = L::DIM == 2 ? p.plo + (int)blockIdx.y * p.pstride : (int)blockIdx.y;
+    const int z = L::DIM == 3 ? p.plo + (int)blockIdx.z * p.pstride : (int)blockIdx.z;
     bgk_cell<L, S, ABS>(p, static_cast<const S*>(p.fin), static_cast<S*>(p.fout), x, y, z, rnd);
 }
 
@@ -637,7 +639,7 @@ __global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepPa
     using R = typename Codec<S>::Real;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
-    const int y = blockIdx.y, z = blockIdx.z + p.plo;
+    const int y = blockIdx.y, z = p.plo + (int)blockIdx.z * p.pstride;
     const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
     const long long c = rows.base[1][1] + x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
@@ -680,7 +682,7 @@ __global__ void __launch_bounds__(256) k_step_mrt2(const __grid_constant__ StepP
     using R = typename Codec<S>::Real;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
-    const Rows<L> rows(blockIdx.y, blockIdx.z + p.plo, p.nx, p.ny, p.nz);
+    const Rows<L> rows(blockIdx.y, p.plo + (int)blockIdx.z * p.pstride, p.nx, p.ny, p.nz);
     const long long c = rows.base[1][1] + x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
     R v[27];

@@ -441,11 +441,15 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
-    const int B = rows;
-    // the launch updates planes [plo, plo + pcnt) of the slowest axis (z for D3Q27, y for D2Q9)
-    const int ybeg = L::DIM == 2 ? p.plo : 0, yend = L::DIM == 2 ? p.plo + p.pcnt : ny;
+    // the launch updates planes plo + k pstride, k < pcnt, of the slowest axis (z for D3Q27, y for
+    // D2Q9); a strided D2Q9 launch takes one row per group
+    const int ps = p.pstride;
+    const int B = L::DIM == 2 && ps > 1 ? 1 : rows;
+    const int ystep = L::DIM == 2 && ps > 1 ? ps : B, zstep = L::DIM == 3 ? ps : 1;
+    const int ybeg = L::DIM == 2 ? p.plo : 0, yend = L::DIM == 2 ? p.plo + (p.pcnt - 1) * ps + 1 : ny;
     const int zbeg = L::DIM == 3 ? p.plo : 0, zcnt = L::DIM == 3 ? p.pcnt : nz;
-    const int gy = (yend - ybeg + B - 1) / B;  // row groups per z plane; the last one may be short
+    // row groups per z plane (the last one may be short)
+    const int gy = L::DIM == 2 ? (p.pcnt + B - 1) / B : (ny + B - 1) / B;
     // item indices in 32 bits (the host keeps the item count below 2^31): a 64-bit division by a
     // runtime divisor is a long software sequence, paid once per stage by every consumer thread
     const unsigned groups = (unsigned)gy * (unsigned)zcnt, ugy = (unsigned)gy;
@@ -456,7 +460,7 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
     // Issue the bulk loads of group g into stage s (one warp; lanes 0..Q-1 one direction each).
     auto issue = [&](unsigned g, int s) {
         if (g == wl.skip) return;  // test hook: this item's stage is never filled
-        const int y0 = ybeg + (int)(g % ugy) * B, z = zbeg + (int)(g / ugy);
+        const int y0 = ybeg + (int)(g % ugy) * ystep, z = zbeg + (int)(g / ugy) * zstep;
         const int nb = yend - y0 < B ? yend - y0 : B;
         if (lane == 0)
             mbar_arrive_expect_tx(&full[s], (uint32_t)(Q * nb) * row_bytes + (has_mask ? (uint32_t)(nb * nx) : 0u));
@@ -521,7 +525,7 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
                     break;
             return;
         }
-        const int y0 = ybeg + (int)(g % ugy) * B, z = zbeg + (int)(g / ugy);
+        const int y0 = ybeg + (int)(g % ugy) * ystep, z = zbeg + (int)(g / ugy) * zstep;
         const int nb = yend - y0 < B ? yend - y0 : B;
         const S* st0 = in + (long long)s * Q * SB;
         const uint8_t* ms0 = has_mask ? mask_st + s * SB : nullptr;
@@ -585,19 +589,26 @@ __global__ void __launch_bounds__(SegShape<L, S, COLL>::CONSUMERS + 32, SegShape
     const int lane = tid & 31;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int nseg = (nx + SW - 1) / SW;
-    // the launch updates rows [row0, row0 + nrows) (global row index y + ny z): the planes [plo, plo + pcnt)
-    // of the slowest axis
+    // the launch updates nrows rows (global row index y + ny z): those of the planes plo + k pstride,
+    // k < pcnt, of the slowest axis
     const unsigned row0 = L::DIM == 3 ? (unsigned)p.plo * (unsigned)ny : (unsigned)p.plo;
     const unsigned nrows = L::DIM == 3 ? (unsigned)p.pcnt * (unsigned)ny : (unsigned)p.pcnt;
     const unsigned groups = (unsigned)nseg * nrows;  // < 2^31 (host-checked)
-    const unsigned useg = (unsigned)nseg, uny = (unsigned)ny;
+    const unsigned useg = (unsigned)nseg, uny = (unsigned)ny, ups = (unsigned)p.pstride;
+    // the q-th row of the launch
+    auto row_of = [&](unsigned q) -> unsigned {
+        if (ups == 1) return row0 + q;
+        if (L::DIM == 2) return row0 + q * ups;
+        const unsigned k = q / uny;
+        return row0 + (k * ups) * uny + (q - k * uny);
+    };
     const unsigned first = blockIdx.x, stride = gridDim.x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
 
     auto issue = [&](unsigned g, int s) {
         if (g == wl.skip) return;  // test hook: this item's stage is never filled
         const unsigned gq = g / useg;
-        const unsigned row = row0 + gq;
+        const unsigned row = row_of(gq);
         const int seg = (int)(g - gq * useg);
         const int z = (int)(row / uny), y = (int)(row - (unsigned)z * uny);
         const int x0 = seg * SW;
@@ -663,7 +674,7 @@ __global__ void __launch_bounds__(SegShape<L, S, COLL>::CONSUMERS + 32, SegShape
             return;
         }
         const unsigned gq = g / useg;
-        const unsigned row = row0 + gq;
+        const unsigned row = row_of(gq);
         const int seg = (int)(g - gq * useg);
         const int x0 = seg * SW;
         const int w = nx - x0 < SW ? nx - x0 : SW;

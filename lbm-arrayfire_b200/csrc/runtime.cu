@@ -125,7 +125,9 @@ struct lbm_ctx {
     int block = 0;
     int kernel = LBM_KERNEL_AUTO;  // requested family
     int kernel_used = 0;           // family chosen (PLAIN or ROWS); 0 before the first step
-    int rows_grid = 0;             // persistent grid of the row pipeline
+    int rows_grid = 0;             // persistent grid of the row pipeline (a whole step)
+    int rows_per_sm = 0, sms = 0;  // its CTAs per SM and the device's SMs
+    int reserved_sms = 0;          // lbm_set_reserved_sms: SMs the persistent grids leave free
     int rows_rpg = 1;              // its rows per group (segmented rows: the segment width)
     int* err = nullptr;            // device error word of the row pipeline
     unsigned* tick = nullptr;      // the rounding's step counter pair (step_rounding)
@@ -165,6 +167,7 @@ static StepParams<R> make_params(const lbm_ctx* c) {
     p.cell_base = (uint32_t)c->cell_offset;
     p.plo = 0;
     p.pcnt = (int)(d.lattice == LBM_D3Q27 ? d.nz : d.ny);
+    p.pstride = 1;
     for (int k = 0; k < kMaxClasses; ++k) {
         const bool used = k < d.n_classes;
         p.cls.flags[k] = used ? d.classes[k].flags : 0u;
@@ -257,56 +260,71 @@ static bool rows_segmented(const lbm_ctx* c) { return c->d.nx > 1024; }
 #endif
 static int seg_width(int w) { return LBM_ROWPIPE_SEGW > 0 ? std::min(LBM_ROWPIPE_SEGW / 16 * 16, 1008) : w; }
 
+// Persistent grid of the row pipeline for pcnt planes (pstride apart): one CTA per work item up to
+// rows_per_sm x (SMs - reserved_sms), or, for a launch on a side stream (`side`), up to rows_per_sm x
+// reserved_sms, the SMs left to it.  CTA b takes items b, b + grid, ...; where every plane (or
+// row) ends in a short item, grid and the items per plane are kept coprime, so the short items do not
+// all land on the same CTAs (148 = 4 x 37 CTAs and 4 segments per row would do that).
+static int rows_grid_for(const lbm_ctx* c, int pcnt, int pstride, bool side = false) {
+    const bool d3 = c->d.lattice == LBM_D3Q27;
+    long long groups = 0, per_plane = 0;
+    bool ragged = false;
+    if (rows_segmented(c)) {
+        per_plane = (c->d.nx + c->rows_rpg - 1) / c->rows_rpg;  // segments per row
+        groups = per_plane * (d3 ? (long long)pcnt * c->d.ny : pcnt);
+        ragged = true;
+    } else if (d3) {
+        per_plane = (c->d.ny + c->rows_rpg - 1) / c->rows_rpg;  // row groups per plane
+        groups = per_plane * pcnt;
+        ragged = c->d.ny % c->rows_rpg != 0;
+    } else {
+        // D2Q9: a plane is one row; a strided launch takes one row per group
+        per_plane = groups = pstride > 1 ? pcnt : (pcnt + c->rows_rpg - 1) / c->rows_rpg;
+        ragged = pstride == 1 && pcnt % c->rows_rpg != 0;
+    }
+    const int sms = side ? c->reserved_sms : c->sms - c->reserved_sms;
+    const long long cap = (long long)c->rows_per_sm * std::max(1, sms);
+    int grid = (int)std::max<long long>(1, std::min(groups, cap));
+    if (ragged)
+        while (grid > 1 && std::gcd((long long)grid, per_plane) != 1) --grid;
+    return grid;
+}
+
 template <class L, class S, int PITCH, int COLL>
-static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s) {
+static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s, bool side) {
+    const int grid = rows_grid_for(c, p.pcnt, p.pstride, side);
     if (rows_segmented(c)) {
         using Sh = SegShape<L, S, COLL>;
-        k_step_rows_seg<L, S, COLL><<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err,
-                                                                                              c->waits);
+        k_step_rows_seg<L, S, COLL><<<grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err,
+                                                                                       c->waits);
         return;
     }
     using Sh = RowShape<L, S, PITCH, COLL>;
     auto kern = k_step_rows<L, S, PITCH, COLL>;
-    kern<<<c->rows_grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err, c->waits);  // + producer warp
+    kern<<<grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err, c->waits);  // + producer warp
 }
 
 template <class L, class S, int PITCH, int COLL>
 static int prepare_rows_t(lbm_ctx* c) {
     int per_sm = 0, sms = 0;
     LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->d.device));
-    long long groups = 0;
-    int gy = 1;
     if (rows_segmented(c)) {
         using Sh = SegShape<L, S, COLL>;
         auto kern = k_step_rows_seg<L, S, COLL>;
         LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
         LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
         c->rows_rpg = seg_width(Sh::SEGW_RUN);
-        const int nseg = (int)((c->d.nx + c->rows_rpg - 1) / c->rows_rpg);
-        groups = (long long)nseg * c->d.ny * c->d.nz;
-        if (per_sm < 1) return set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
-        // CTA b takes items b, b + grid, ...; with grid and nseg coprime it cycles through every
-        // segment of a row, so no CTA is left with only the short last segments (148 = 4 x 37 CTAs
-        // and 4 segments per row would be)
-        int grid = (int)std::min<long long>(groups, (long long)per_sm * sms);
-        while (grid > 1 && std::gcd(grid, nseg) != 1) --grid;
-        c->rows_grid = grid;
-        return LBM_OK;
     } else {
         using Sh = RowShape<L, S, PITCH, COLL>;
         auto kern = k_step_rows<L, S, PITCH, COLL>;
         LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
         LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
         c->rows_rpg = Sh::rows_per_group((int)c->d.nx);
-        gy = (int)((c->d.ny + c->rows_rpg - 1) / c->rows_rpg);
-        groups = (long long)gy * c->d.nz;
     }
     if (per_sm < 1) return set_error(LBM_ERR_UNSUPPORTED, "row pipeline does not fit on an SM");
-    int grid = (int)std::min<long long>(groups, (long long)per_sm * sms);
-    // a short last group in every plane: as for segments, keep it from landing on the same CTAs
-    if (c->d.ny % c->rows_rpg != 0)
-        while (grid > 1 && std::gcd(grid, gy) != 1) --grid;
-    c->rows_grid = grid;
+    c->rows_per_sm = per_sm;
+    c->sms = sms;
+    c->rows_grid = rows_grid_for(c, (int)(c->d.lattice == LBM_D3Q27 ? c->d.nz : c->d.ny), 1);
     return LBM_OK;
 }
 
@@ -388,12 +406,15 @@ static int prepare_rows(lbm_ctx* c) {
 
 // Launch one time step reading buffer `from` and writing the other one.
 // Launch one time step reading buffer `from` and writing the other one, over planes [plo, plo + pcnt)
-// of the slowest axis (pcnt < 0: all of them; Shan-Chen always steps every plane).
-static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo = 0, int pcnt = -1) {
+// of the slowest axis, plo + k pstride for k < pcnt (pcnt < 0: all of them; Shan-Chen always steps
+// every plane).
+static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo = 0, int pcnt = -1,
+                        int pstride = 1, bool side = false) {
     const int planes = (int)(c->d.lattice == LBM_D3Q27 ? c->d.nz : c->d.ny);
     if (pcnt < 0) {
         plo = 0;
         pcnt = planes;
+        pstride = 1;
     }
     if (c->kernel_used == LBM_KERNEL_ROWS && c->d.collision == LBM_SHANCHEN) {
         const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
@@ -424,7 +445,8 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
             p.parity = from;
             p.plo = plo;
             p.pcnt = pcnt;
-            launch_rows_t<L, S, decltype(pi)::value, decltype(co)::value>(c, p, s);
+            p.pstride = pstride;
+            launch_rows_t<L, S, decltype(pi)::value, decltype(co)::value>(c, p, s, side);
         });
         return;
     }
@@ -440,6 +462,7 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
         p.parity = from;
         p.plo = plo;
         p.pcnt = pcnt;
+        p.pstride = pstride;
         const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
         switch (c->d.collision) {
             case LBM_BGK:
@@ -1085,11 +1108,11 @@ int lbm_set_kernel(lbm_ctx* c, int kind) {
 
 int lbm_get_kernel(const lbm_ctx* c) { return c ? c->kernel_used : 0; }
 
-int lbm_step_planes(lbm_ctx* c, int64_t first, int64_t count, int finish) {
+int lbm_step_planes(lbm_ctx* c, int64_t first, int64_t count, int64_t stride, int finish, void* stream) {
     if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
     const long long planes = c->d.lattice == LBM_D3Q27 ? c->d.nz : c->d.ny;
-    if (first < 0 || count < 1 || first + count > planes)
-        return set_error(LBM_ERR_INVALID, "plane range outside the lattice's slowest axis");
+    if (first < 0 || count < 1 || stride < 1 || first >= planes || (count - 1) > (planes - 1 - first) / stride)
+        return set_error(LBM_ERR_INVALID, "planes outside the lattice's slowest axis");
     if (c->d.collision == LBM_SHANCHEN)
         return set_error(LBM_ERR_UNSUPPORTED, "Shan-Chen steps every plane at once (its force reads psi of the neighbours)");
     LBM_CK(cudaSetDevice(c->d.device));
@@ -1097,13 +1120,25 @@ int lbm_step_planes(lbm_ctx* c, int64_t first, int64_t count, int finish) {
         int rc = autotune(c);
         if (rc) return rc;
     }
-    launch_step(c, c->cur, c->stream, c->block, (int)first, (int)count);
+    // a launch on a side stream runs in the SMs that lbm_set_reserved_sms keeps from the context stream
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    launch_step(c, c->cur, s, c->block, (int)first, (int)count, (int)stride, s != c->stream && c->reserved_sms > 0);
     LBM_CK(cudaGetLastError());
     if (finish) {
         c->cur ^= 1;
         c->has_prev = true;
         c->steps += 1;
     }
+    return LBM_OK;
+}
+
+int lbm_set_reserved_sms(lbm_ctx* c, int sms) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    if (sms < 0 || sms > 64) return set_error(LBM_ERR_INVALID, "reserved SMs must be in [0, 64]");
+    LBM_CK(cudaSetDevice(c->d.device));
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);  // the graphs captured the persistent grid
+    c->reserved_sms = sms;
     return LBM_OK;
 }
 

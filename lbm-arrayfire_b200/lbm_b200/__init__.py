@@ -46,6 +46,14 @@ ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory"
           -5: "unsupported", -6: "no device", -7: "invalid state", -8: "device wait timed out"}
 
 
+def _stream_handle(stream):
+    """cudaStream_t handle of a torch.cuda.Stream or a raw handle; None stays None.  Torch's default
+    stream (handle 0) becomes CUDA's legacy default stream (handle 1, cudaStreamLegacy), since the C
+    calls read NULL as "the lattice's own stream"."""
+    h = getattr(stream, "cuda_stream", stream)
+    return 1 if stream is not None and h == 0 else h
+
+
 class LbmError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)} ({code}): {msg}")
@@ -118,7 +126,8 @@ _SIGS = {
     "lbm_get_kernel": (C.c_int, [_P]),
     "lbm_test_stall_next_step": (C.c_int, [_P, C.c_int64, C.c_int64]),
     "lbm_set_cell_offset": (C.c_int, [_P, C.c_int64]),
-    "lbm_step_planes": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int]),
+    "lbm_step_planes": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int, _P]),
+    "lbm_set_reserved_sms": (C.c_int, [_P, C.c_int]),
     "lbm_device_buffers": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(C.c_size_t)]),
     "lbm_sums_fp64_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_double, _P, _P]),
     "lbm_batch_create": (C.c_int, [_DP, C.c_int, C.POINTER(_P)]),
@@ -343,8 +352,11 @@ class Lattice:
     def stream(self) -> int:
         return lib().lbm_stream(self._h) or 0
 
-    def set_stream(self, stream: int | None):
-        _check(lib().lbm_set_stream(self._h, C.c_void_p(stream or 0)))
+    def set_stream(self, stream):
+        """Run the lattice's work on `stream`: a torch.cuda.Stream, a cudaStream_t handle, or None for
+        the lattice's own stream.  Torch's default stream (handle 0) is passed as CUDA's legacy
+        default stream (handle 1, cudaStreamLegacy), since lbm_set_stream reads NULL as "own stream"."""
+        _check(lib().lbm_set_stream(self._h, C.c_void_p(_stream_handle(stream) or 0)))
 
     def set_block(self, threads_x: int):
         _check(lib().lbm_set_block(self._h, threads_x))
@@ -359,9 +371,15 @@ class Lattice:
     def kernel(self) -> int:
         return lib().lbm_get_kernel(self._h)
 
-    def step_planes(self, first: int, count: int, finish: bool):
-        """One step over planes [first, first + count) of the slowest axis (lbm_step_planes)."""
-        _check(lib().lbm_step_planes(self._h, first, count, 1 if finish else 0))
+    def step_planes(self, first: int, count: int, finish: bool, stream=None, stride: int = 1):
+        """One step over planes first + k * stride, k < count, of the slowest axis (lbm_step_planes),
+        on `stream` (a torch.cuda.Stream or cudaStream_t handle; None: the lattice's stream)."""
+        h = _stream_handle(stream)
+        _check(lib().lbm_step_planes(self._h, first, count, stride, 1 if finish else 0, C.c_void_p(h or 0)))
+
+    def set_reserved_sms(self, sms: int):
+        """SMs the row pipeline's persistent grid leaves free for kernels on other streams."""
+        _check(lib().lbm_set_reserved_sms(self._h, sms))
 
     def device_buffers(self):
         """(current, next, bytes): device pointers of both population buffers."""

@@ -13,16 +13,21 @@ of its plane n up and the c = -1 populations of its plane 1 down, as stored word
 `face_set` on the C ABI: one copy per direction, no conversion), so the decomposed run is
 bit-identical to the undivided lattice.  Ghost cells take a bounce-back solid class: their own updates
 are never read, and bounce-back keeps them finite.  The exchange is point-to-point
-(`torch.distributed` isend/irecv; NCCL over NVLink on GPUs, gloo on CPUs) on the lattice's own stream,
+(`torch.distributed` isend/irecv; NCCL over NVLink on GPUs, gloo on CPUs) on the slab's stream,
 and it is the only data-path communication.  Shan-Chen is not decomposed (its force needs psi of the
 neighbour planes as a second exchange per step).
 
-On a GPU the exchange overlaps the interior update (`lbm_step_planes`): a step first updates the two
-boundary planes (local planes 1 and n), then a second CUDA stream packs their outgoing faces straight
-from the buffer being written, exchanges them (NCCL, or copies within one process) and unpacks the
-incoming ones into that buffer's ghost planes, while the main stream updates planes 2 .. n-1 and
-finishes the step; the next step waits for both.  Slabs of fewer than three planes, and steppers
-without plane ranges (the oracle in the CPU tests), step whole and exchange afterwards.
+On a GPU the exchange overlaps the interior update (`lbm_step_planes`).  Within a step the slab's
+stream updates planes 2 .. n-1 in all but a few SMs, while a second (high-priority) CUDA stream, in
+those few SMs (`lbm_set_reserved_sms`: the row pipeline's persistent grid would otherwise hold every
+SM until it ends), updates the two boundary planes (local planes 1 and n, one strided launch), packs
+their outgoing faces straight from the buffer being written, exchanges them (NCCL, or copies within
+one process) and unpacks the incoming ones into that buffer's ghost planes.  The next step waits for
+both streams.  D3Q27 MRT 256^3 F16S on one B200: 351 us per step with 8 SMs for the side stream
+(one rank, faces copied to itself), against 470 us for step-then-exchange and 341 us for the
+undivided lattice.  Slabs of
+fewer than three planes, and steppers without plane ranges (the oracle in the CPU tests), step whole
+and exchange afterwards.
 
 `Slab` is one rank's part (one process per GPU).  `SlabSet` holds every rank's part in one process and
 exchanges by plain copies, for tests and for several slabs on one device.
@@ -108,9 +113,11 @@ def _device_bytes(ptr: int, nbytes: int, device):
     return torch.as_tensor(_View(), device=device)
 
 
-def _plane_bytes(F, N: int, pc: int, s: int, dirs, plane: int):
-    """Byte views of plane `plane` of each direction in `dirs` (each one contiguous run in the layout)."""
-    return [F[(i * N + plane * pc) * s:(i * N + plane * pc + pc) * s] for i in dirs]
+def _plane_views(lat, planes: int, device) -> dict:
+    """{device pointer: [Q, planes, plane bytes] uint8 view} for both population buffers of `lat`
+    (the layout is [i][plane][cell], so a plane of one direction is one contiguous run)."""
+    cur, nxt, nbytes = lat.device_buffers()
+    return {ptr: _device_bytes(ptr, nbytes, device).view(lat.q, planes, -1) for ptr in (cur, nxt)}
 
 
 def _interior(lat, n: int, dtype=np.float64) -> np.ndarray:
@@ -124,10 +131,11 @@ class Slab:
     lattice_factory(desc, mask) builds the local stepper (default: a GPU `Lattice`); it must offer
     step, face_get, face_set, get_populations, set_populations, set_stream and face_cells.  A GPU
     stepper that also offers step_planes and device_buffers gets the overlapped step unless
-    `overlap=False` (then: step, then exchange)."""
+    `overlap=False` (then: step, then exchange); its row pipeline then leaves `reserved_sms` SMs to
+    the exchange stream (NCCL's point-to-point kernels included: limit its channels to fit them)."""
 
     def __init__(self, desc: Desc, mask, F0, rank: int, world: int, group=None, device=None,
-                 lattice_factory=None, overlap: bool = True):
+                 lattice_factory=None, overlap: bool = True, reserved_sms: int = 8):
         import torch
         import torch.distributed as dist
 
@@ -145,10 +153,12 @@ class Slab:
             self.lat.set_cell_offset((self.p0 - 1) * (desc.cells // _planes(desc)))
         self.up_dirs, self.down_dirs = axis_dirs(desc.lattice)
         self.device = torch.device(device) if device is not None else torch.device("cpu")
-        if self.device.type == "cuda":
-            # the steps run on torch's current stream; so does the exchange of a sequential step, while
-            # an overlapped step exchanges on a side stream ordered by events
-            self.lat.set_stream(torch.cuda.current_stream(self.device).cuda_stream)
+        # a stream of the slab's own orders the steps, the face copies and the NCCL transfers (torch's
+        # default stream has handle 0, which the engine would read as "the lattice's own stream");
+        # an overlapped step exchanges on a second stream ordered by events
+        self.stream = torch.cuda.Stream(device=self.device) if self.device.type == "cuda" else None
+        if self.stream is not None:
+            self.lat.set_stream(self.stream.cuda_stream)
         # faces travel as raw bytes of the stored words (NCCL has no 16-bit integer type; a
         # point-to-point transfer never touches the values); an injected stepper uses FP64 words
         k = len(self.up_dirs) * self.lat.face_cells()
@@ -159,7 +169,14 @@ class Slab:
         # the overlapped step (see the module docstring): GPU steppers with plane ranges, >= 3 planes
         self.overlap = (overlap and self.device.type == "cuda" and hasattr(self.lat, "step_planes")
                         and self.n >= 3)
-        self._comm = torch.cuda.Stream(device=self.device) if self.overlap else None
+        if self.overlap:
+            # the exchange stream runs first wherever SMs free up; the row pipeline leaves it some
+            self._comm = torch.cuda.Stream(device=self.device, priority=-1)
+            self.lat.set_reserved_sms(reserved_sms)
+            self._views = _plane_views(self.lat, self.n + 2, self.device)
+            self._up_idx = torch.tensor(self.up_dirs, device=self.device)
+            self._down_idx = torch.tensor(self.down_dirs, device=self.device)
+            self._ready, self._done = torch.cuda.Event(), torch.cuda.Event()
 
     def _pack(self):
         self.lat.face_get(self.n, self.up_dirs, self._buf["send_up"])
@@ -171,6 +188,12 @@ class Slab:
 
     def exchange(self):
         """Fill both ghost planes from the neighbours' boundary planes (the same steps on every rank)."""
+        import torch
+
+        with torch.cuda.stream(self.stream):  # no-op without a CUDA stream
+            self._exchange()
+
+    def _exchange(self):
         b = self._buf
         self._pack()
         if self.world == 1:
@@ -187,31 +210,31 @@ class Slab:
         self._unpack(b["recv_down"], b["recv_up"])
 
     def step(self, n: int = 1):
-        for _ in range(n):
-            if self.overlap:
-                self._step_overlapped()
-            else:
-                self.lat.step(1)
-                self.exchange()
+        import torch
+
+        with torch.cuda.stream(self.stream):
+            for _ in range(n):
+                if self.overlap:
+                    self._step_overlapped()
+                else:
+                    self.lat.step(1)
+                    self._exchange()
 
     def _step_overlapped(self):
-        """One step: boundary planes, then the face exchange on the side stream while the interior
-        planes are updated on the main stream."""
+        """One step: the interior planes on the slab's stream, and beside them, on the side stream in
+        the SMs the row pipeline leaves free, the boundary planes and the face exchange."""
         import torch
 
         dist, lat, n, b = self.dist, self.lat, self.n, self._buf
-        main = torch.cuda.current_stream(self.device)
-        lat.step_planes(1, 1, False)
-        lat.step_planes(n, 1, False)
-        ready = torch.cuda.Event()
-        ready.record(main)
-        _, nxt, nbytes = lat.device_buffers()
-        F = _device_bytes(nxt, nbytes, self.device)
-        N, pc, sb = self.desc.cells, lat.face_cells(), STORAGE_BYTES[self.desc.storage]
-        with torch.cuda.stream(self._comm):
-            self._comm.wait_event(ready)
-            torch.cat(_plane_bytes(F, N, pc, sb, self.up_dirs, n), out=b["send_up"])
-            torch.cat(_plane_bytes(F, N, pc, sb, self.down_dirs, 1), out=b["send_down"])
+        main, comm, up_idx, down_idx = self.stream, self._comm, self._up_idx, self._down_idx
+        self._ready.record(main)  # the previous step (and its exchange) is complete on `main`
+        F = self._views[lat.device_buffers()[1]]  # the buffer this step writes
+        lat.step_planes(2, n - 2, False, main)  # the interior first: it takes its SMs before the side
+        with torch.cuda.stream(comm):
+            comm.wait_event(self._ready)
+            lat.step_planes(1, 2, True, comm, stride=n - 1)  # planes 1 and n in one launch; ends the step
+            torch.index_select(F[:, n], 0, up_idx, out=b["send_up"].view(len(self.up_dirs), -1))
+            torch.index_select(F[:, 1], 0, down_idx, out=b["send_down"].view(len(self.down_dirs), -1))
             if self.world == 1:
                 from_down, from_up = b["send_up"], b["send_down"]
             else:
@@ -223,15 +246,10 @@ class Slab:
                 for req in dist.batch_isend_irecv(ops):
                     req.wait()
                 from_down, from_up = b["recv_down"], b["recv_up"]
-            w = pc * sb
-            for k, dst in enumerate(_plane_bytes(F, N, pc, sb, self.up_dirs, 0)):
-                dst.copy_(from_down[k * w:(k + 1) * w])
-            for k, dst in enumerate(_plane_bytes(F, N, pc, sb, self.down_dirs, n + 1)):
-                dst.copy_(from_up[k * w:(k + 1) * w])
-            done = torch.cuda.Event()
-            done.record(self._comm)
-        lat.step_planes(2, n - 2, True)
-        main.wait_event(done)
+            F[:, 0].index_copy_(0, up_idx, from_down.view(len(self.up_dirs), -1))
+            F[:, n + 1].index_copy_(0, down_idx, from_up.view(len(self.down_dirs), -1))
+            self._done.record(comm)
+        main.wait_event(self._done)
 
     def interior_populations(self, dtype=np.float64) -> np.ndarray:
         """This rank's planes, [Q, n, plane cells]."""
@@ -273,7 +291,8 @@ class SlabSet:
     The same planes, ghost classes and exchange order as `Slab`, for parity tests on one device and
     for decompositions whose slabs share a GPU."""
 
-    def __init__(self, desc: Desc, mask, F0, parts: int, lattice_factory=None, overlap: bool = False):
+    def __init__(self, desc: Desc, mask, F0, parts: int, lattice_factory=None, overlap: bool = False,
+                 reserved_sms: int = 8):
         self.global_desc = desc
         self.ranges = split_planes(_planes(desc), parts)
         self.up_dirs, self.down_dirs = axis_dirs(desc.lattice)
@@ -291,15 +310,21 @@ class SlabSet:
             if lattice_factory is None else np.float64
         self._up = [np.empty(k, dtype=word) for _ in self.lats]
         self._down = [np.empty(k, dtype=word) for _ in self.lats]
-        # overlapped steps (GPU lattices on torch's current stream, a side stream for the face copies)
+        # overlapped steps: every lattice on one stream of the set's own, the face copies on a second
         self.overlap = overlap and lattice_factory is None and min(self.ns) >= 3
         if self.overlap:
             import torch
 
             self._dev = torch.device("cuda", desc.device)
+            self.stream = torch.cuda.Stream(device=self._dev)
             for lat in self.lats:
-                lat.set_stream(torch.cuda.current_stream(self._dev).cuda_stream)
-            self._comm = torch.cuda.Stream(device=self._dev)
+                lat.set_stream(self.stream.cuda_stream)
+                lat.set_reserved_sms(reserved_sms)
+            self._comm = torch.cuda.Stream(device=self._dev, priority=-1)
+            self._views = [_plane_views(lat, n + 2, self._dev) for lat, n in zip(self.lats, self.ns)]
+            self._up_idx = torch.tensor(self.up_dirs, device=self._dev)
+            self._down_idx = torch.tensor(self.down_dirs, device=self._dev)
+            self._ready, self._done = torch.cuda.Event(), torch.cuda.Event()
 
     def exchange(self):
         R = len(self.lats)
@@ -324,35 +349,22 @@ class SlabSet:
         between the slabs' next buffers on the side stream, interior planes on the main stream."""
         import torch
 
-        main = torch.cuda.current_stream(self._dev)
-        for lat, n in zip(self.lats, self.ns):
-            lat.step_planes(1, 1, False)
-            lat.step_planes(n, 1, False)
-        ready = torch.cuda.Event()
-        ready.record(main)
-        sb = STORAGE_BYTES[self.global_desc.storage]
-        views = []
-        for lat in self.lats:
-            _, nxt, nbytes = lat.device_buffers()
-            views.append(_device_bytes(nxt, nbytes, self._dev))
+        main, comm, up_idx, down_idx = self.stream, self._comm, self._up_idx, self._down_idx
+        self._ready.record(main)
+        F = [v[lat.device_buffers()[1]] for lat, v in zip(self.lats, self._views)]
         R = len(self.lats)
-        with torch.cuda.stream(self._comm):
-            self._comm.wait_event(ready)
-            pc = self.lats[0].face_cells()
-            cells = [lat.desc.cells for lat in self.lats]
+        for lat, n in zip(self.lats, self.ns):
+            lat.step_planes(2, n - 2, False, main)
+        with torch.cuda.stream(comm):
+            comm.wait_event(self._ready)
+            for lat, n in zip(self.lats, self.ns):
+                lat.step_planes(1, 2, True, comm, stride=n - 1)
             for r, n in enumerate(self.ns):
                 lo, hi = (r - 1) % R, (r + 1) % R
-                up = _plane_bytes(views[lo], cells[lo], pc, sb, self.up_dirs, self.ns[lo])
-                down = _plane_bytes(views[hi], cells[hi], pc, sb, self.down_dirs, 1)
-                for dst, src in zip(_plane_bytes(views[r], cells[r], pc, sb, self.up_dirs, 0), up):
-                    dst.copy_(src)
-                for dst, src in zip(_plane_bytes(views[r], cells[r], pc, sb, self.down_dirs, n + 1), down):
-                    dst.copy_(src)
-            done = torch.cuda.Event()
-            done.record(self._comm)
-        for lat, n in zip(self.lats, self.ns):
-            lat.step_planes(2, n - 2, True)
-        main.wait_event(done)
+                F[r][:, 0].index_copy_(0, up_idx, F[lo][:, self.ns[lo]].index_select(0, up_idx))
+                F[r][:, n + 1].index_copy_(0, down_idx, F[hi][:, 1].index_select(0, down_idx))
+            self._done.record(comm)
+        main.wait_event(self._done)
 
     def gather_populations(self, dtype=np.float64) -> np.ndarray:
         return np.concatenate([_interior(lat, n, dtype) for lat, n in zip(self.lats, self.ns)], axis=1).ravel()

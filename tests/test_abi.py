@@ -181,7 +181,8 @@ def test_null_handles_are_rejected():
     assert L.lbm_sums_fp64(None, None) == -1
     assert L.lbm_batch_step(None, 1) == -1
     assert L.lbm_steps_done(None) == -1
-    assert L.lbm_step_planes(None, 0, 1, 1) == -1
+    assert L.lbm_step_planes(None, 0, 1, 1, 1, None) == -1
+    assert L.lbm_set_reserved_sms(None, 2) == -1
     assert L.lbm_device_buffers(None, None, None, None) == -1
     assert L.lbm_set_cell_offset(None, 0) == -1
     L.lbm_destroy(None)

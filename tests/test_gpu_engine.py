@@ -160,6 +160,25 @@ def test_external_stream():
         lat2.set_populations(F0)
         lat2.step(10)
         assert np.array_equal(lat2.get_populations(np.float32), a)
+    # torch's default stream (handle 0) becomes CUDA's legacy default stream, not the lattice's own:
+    # torch work queued after the steps on that stream sees their result
+    with lb.Lattice(d, m) as lat3:
+        lat3.set_populations(F0)
+        lat3.set_stream(torch.cuda.default_stream())
+        assert lat3.stream() == 1
+        ptr, nbytes = lat3.device_populations()
+        lat3.step(10)
+        view = torch.as_tensor(_ByteView(ptr, nbytes), device="cuda")
+        snap = view.clone()  # queued on torch's default stream right behind the steps
+        lat3.sync()
+        assert torch.equal(snap, view)
+        assert np.array_equal(lat3.get_populations(np.float32), a)
+        lat3.set_stream(None)
+
+
+class _ByteView:
+    def __init__(self, ptr, nbytes):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False), "version": 3}
 
 
 @pytest.mark.parametrize("mode", [lb.BATCH_TILES, lb.BATCH_ROWS, lb.BATCH_ROWS_PER_FAMILY])

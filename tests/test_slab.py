@@ -222,24 +222,43 @@ def _plane_case(name, storage):
 def test_step_planes_in_pieces_equals_whole_steps(storage, kernel, case):
     """lbm_step_planes: a step cut into plane ranges (in any order; the last one finishes it) is
     bit-identical to lbm_step, for the plain kernels, the row pipeline and its segmented form, with
-    stochastic rounding on for the 16-bit storage."""
+    stochastic rounding on for the 16-bit storage.  The ranges before the last run on a side stream,
+    beside the last one (the overlapped slab's pattern), with SMs reserved from the row pipeline."""
+    import torch
+
     d, m, F0 = _plane_case(case, storage)
     planes = d.nz if d.dim == 3 else d.ny
     F0 = np.asarray(F0, dtype=np.float64)
+    main, side = torch.cuda.Stream(), torch.cuda.Stream(priority=-1)
+    ready, done = torch.cuda.Event(), torch.cuda.Event()
     with lb.Lattice(d, m) as a, lb.Lattice(d, m) as b:
         for lat in (a, b):
             lat.set_kernel(kernel)
             lat.set_populations(F0)
-        a.step(6)
-        cuts = [[(0, 1), (planes - 1, 1), (1, planes - 2)],  # the slab order: boundary planes first
-                [(3, planes - 3), (0, 3)],
-                [(k, 1) for k in range(planes - 1, -1, -1)]]
-        for t in range(6):
+        a.step(8)
+        b.set_stream(main)
+        b.set_reserved_sms(3)
+        # (first, count, stride): the slab order (boundary planes in one strided launch, then the
+        # interior), contiguous ranges, single planes backwards, and the odd planes then the even ones
+        cuts = [[(0, 2, planes - 1), (1, planes - 2, 1)],
+                [(3, planes - 3, 1), (0, 3, 1)],
+                [(k, 1, 1) for k in range(planes - 1, -1, -1)],
+                [(1, planes // 2, 2), (0, (planes + 1) // 2, 2)]]
+        for t in range(8):
             pieces = cuts[t % len(cuts)]
-            for k, (first, count) in enumerate(pieces):
-                b.step_planes(first, count, k == len(pieces) - 1)
-        assert b.steps_done == a.steps_done == 6
+            ready.record(main)
+            side.wait_event(ready)
+            for k, (first, count, stride) in enumerate(pieces):
+                last = k == len(pieces) - 1
+                b.step_planes(first, count, last, main if last else side, stride=stride)
+            done.record(side)
+            main.wait_event(done)
+        assert b.steps_done == a.steps_done == 8
         ref, got = a.get_populations(np.float32), b.get_populations(np.float32)
+        b.set_stream(None)
+        b.step(2)  # whole steps with the reserved SMs
+        a.step(2)
+        assert np.array_equal(a.get_populations(np.float32), b.get_populations(np.float32))
     assert np.isfinite(got).all() and np.array_equal(got, ref)
 
 
@@ -247,9 +266,9 @@ def test_step_planes_in_pieces_equals_whole_steps(storage, kernel, case):
 def test_step_planes_rejects_bad_ranges_and_shanchen():
     d, m, _ = mrt_cavity3d(lb.F32, n=(32, 4, 5))
     with lb.Lattice(d, m) as lat:
-        for first, count in ((-1, 1), (0, 0), (4, 2), (5, 1)):
+        for first, count, stride in ((-1, 1, 1), (0, 0, 1), (4, 2, 1), (5, 1, 1), (0, 2, 0), (1, 2, 4), (1, 3, 2)):
             with pytest.raises(lb.LbmError):
-                lat.step_planes(first, count, True)
+                lat.step_planes(first, count, True, stride=stride)
         assert lat.steps_done == 0
     d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, lb.F32, (32, 16), omega=1.0, sc_G=-5.0)
     with lb.Lattice(d, None) as lat:
@@ -282,3 +301,18 @@ def test_one_rank_slab_on_the_gpu_equals_one_lattice(storage, overlap):
     # lbm_sums_fp64 decodes each population in FP32 before its FP64 sum; Slab.sums decodes in FP64
     assert np.allclose(slab.sums(), ref_sums, rtol=1e-6, atol=1e-6)
     slab.close()
+
+
+@pytest.mark.gpu
+def test_bench_slab_line():
+    """bench.py --slab: one JSON line with the overlapped, sequential and undivided step times."""
+    import subprocess
+    import sys
+
+    root = Path(__file__).resolve().parents[1]
+    cmd = [sys.executable, str(root / "bench.py"), "--slab", "--dims", "64x32x24", "--steps", "4", "--warmup", "1"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=str(root))
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["config"]["parallelism"] == "slab x1" and line["config"]["overlap"] is True
+    assert line["value"] > 0 and line["sequential_ms_per_step"] > 0 and line["undivided_ms_per_step"] > 0
