@@ -132,6 +132,13 @@ struct Pair16<__half> {
     }
     __device__ __forceinline__ static __half hi(uint32_t d) { return __ushort_as_half((unsigned short)(d >> 16)); }
     __device__ __forceinline__ static __half lo(uint32_t d) { return __ushort_as_half((unsigned short)(d & 0xffffu)); }
+    // the two halves of a packed pair as floats (low: the first cell)
+    __device__ __forceinline__ static float lo_f(uint32_t d) {
+        return __low2float(*reinterpret_cast<const __half2*>(&d));
+    }
+    __device__ __forceinline__ static float hi_f(uint32_t d) {
+        return __high2float(*reinterpret_cast<const __half2*>(&d));
+    }
 };
 
 template <>
@@ -152,6 +159,9 @@ struct Pair16<__nv_bfloat16> {
     __device__ __forceinline__ static __nv_bfloat16 lo(uint32_t d) {
         return __ushort_as_bfloat16((unsigned short)(d & 0xffffu));
     }
+    // the two halves of a packed pair as floats (a bfloat16 is the top half of its float)
+    __device__ __forceinline__ static float lo_f(uint32_t d) { return __uint_as_float(d << 16); }
+    __device__ __forceinline__ static float hi_f(uint32_t d) { return __uint_as_float(d & 0xffff0000u); }
 };
 
 // A 32-bit integer hash (xor-shift / multiply rounds): the random words of the stochastic rounding come

@@ -618,10 +618,10 @@ __device__ __forceinline__ void mrt2_collide(const P& p, int cls, uint32_t fl, c
                 const R t2 = cx * cz == 1 ? t1 + b : t1 - b;
                 corr = cy * cz == 1 ? t2 + c : t2 - c;
             }
+            // the odd part (+- w3 eu) enters by multiply-adds: two FMAs instead of a product and two adds
             const R sym = mad(w45[nz], eu * eu, wb[nz]) - corr;
-            const R anti = w3[nz] * eu;
-            out[i] = mad(om1, v[i], sym + anti);
-            out[o] = mad(om1, v[o], sym - anti);
+            out[i] = mad(om1, v[i], mad(w3[nz], eu, sym));
+            out[o] = mad(om1, v[o], mad(-w3[nz], eu, sym));
         }
     });
     if (fl & kEquilibrium) equilibrium_dev<L, false, R>(rho, drho, ux, uy, uz, sc, out);

@@ -345,14 +345,23 @@ __device__ __forceinline__ void row_pair(const P& p, const S* st, const uint8_t*
         clsB = (int)(m2 >> 8);
     }
     const uint32_t flA = p.cls.flags[clsA], flB = p.cls.flags[clsB];
+    // D3Q27: the c_x = 0 populations of both cells come in one 32-bit shared load per direction (x
+    // even, every staged row 4-byte aligned); cell x + 1's half waits in mid[] for its collision.
+    // (D2Q9 loads them one by one: its ensemble kernel has no registers to spare for mid[].)
+    constexpr bool kMid = Q == 27;
+    uint32_t mid[Q];
     R outA[Q];
     {
         R v[Q];
         static_for<Q>([&](auto I) {
             constexpr int i = I;
             constexpr int cx = L::cx(i);
-            const int xs = cx == 1 ? xl : (cx == -1 ? x + 1 : x);
-            v[i] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
+            if constexpr (kMid && cx == 0) {
+                mid[i] = *reinterpret_cast<const uint32_t*>(st + i * SB + x);
+                v[i] = Pair16<S>::lo_f(mid[i]);
+            } else {
+                v[i] = Codec<S>::raw(st[i * SB + (cx == 1 ? xl : (cx == -1 ? x + 1 : x))], R(L::w(i)));
+            }
         });
         if (flA & kZeroGradXp) {
             static_for<Q>([&](auto I) {
@@ -371,8 +380,10 @@ __device__ __forceinline__ void row_pair(const P& p, const S* st, const uint8_t*
         static_for<Q>([&](auto I) {
             constexpr int i = I;
             constexpr int cx = L::cx(i);
-            const int xs = cx == 1 ? x : (cx == -1 ? xr : x + 1);
-            v[i] = Codec<S>::raw(st[i * SB + xs], R(L::w(i)));
+            if constexpr (kMid && cx == 0)
+                v[i] = Pair16<S>::hi_f(mid[i]);
+            else
+                v[i] = Codec<S>::raw(st[i * SB + (cx == 1 ? x : (cx == -1 ? xr : x + 1))], R(L::w(i)));
         });
         if (flB & kZeroGradXp) {
             static_for<Q>([&](auto I) {
