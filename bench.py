@@ -346,12 +346,12 @@ def build_workload(lb, args, storage):
 
 def apply_kernel_choice(lb, lat, args):
     if args.kernel != "auto":
-        lat.set_kernel({"plain": lb.KERNEL_PLAIN, "rows": lb.KERNEL_ROWS}[args.kernel])
+        lat.set_kernel({"plain": lb.KERNEL_PLAIN, "rows": lb.KERNEL_ROWS, "cluster": lb.KERNEL_CLUSTER}[args.kernel])
     if args.block:
         lat.set_block(args.block)
 
 
-KERNEL_NAMES = {1: "plain", 2: "rows"}
+KERNEL_NAMES = {1: "plain", 2: "rows", 3: "cluster"}
 
 
 def measure(torch, lb, args, storage, dev, world, sample_clocks=False):
@@ -829,8 +829,11 @@ def config_lines(torch, lb, args, dev, world):
                         "kernel_family": fam,
                         "achieved_gbs": algorithmic_bytes_per_cell(d) * d.cells * steps / el / 1e9}
             rec["lattice"] = list(d.shape)
-            rec["l2"] = (f"L2-resident ({d.cells * d.q * storage_bytes(STORAGES[stn]) * 2 / 1e6:.1f} MB of "
-                         f"populations in both buffers at {stn}); no flush")
+            mb = d.cells * d.q * storage_bytes(STORAGES[stn]) * 2 / 1e6
+            rec["l2"] = (f"L2-resident ({mb:.1f} MB of populations in both buffers at {stn}); no flush"
+                         if fam != "cluster" else
+                         f"resident in one thread-block cluster's shared memory ({mb:.1f} MB at {stn}) for up "
+                         f"to 4096 steps per launch; HBM/L2 only at launch start and end")
         rec[f"speedup_{st16}_vs_f32"] = rec[st16]["value"] / rec["f32"]["value"]
         rec["steps"] = steps
         out[wl] = rec
@@ -1002,7 +1005,7 @@ def main():
     ap.add_argument("--size", type=int, default=0,
                     help="cube side for D3Q27 workloads, square side for d2q9_lid_8192 (default: the config's)")
     ap.add_argument("--dims", default="", help="NXxNYxNZ for D3Q27 workloads, NXxNY for the Shan-Chen one")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "rows"], help="step-kernel family")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "plain", "rows", "cluster"], help="step-kernel family")
     ap.add_argument("--rounding", default="stochastic", choices=["stochastic", "nearest"],
                     help="rounding of 16-bit storage in the timed runs")
     ap.add_argument("--block", type=int, default=0, help="fixed block width (default: autotune)")

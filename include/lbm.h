@@ -211,11 +211,15 @@ int   lbm_get_block(const lbm_ctx* c);
  * groups of whole rows (segments of rows wider than 1024 cells) staged in shared memory by bulk
  * copies (TMA) through an mbarrier ring; for D2Q9 Shan-Chen (any shape and storage) the one-pass
  * kernel (a window sliding down y: psi of the next row into a shared ring, the force from it) instead
- * of the two passes of PLAIN.  AUTO (default): the autotuner times the eligible ones.  Both give
+ * of the two passes of PLAIN.  CLUSTER (D2Q9 BGK, deviation arithmetic, both buffers within the
+ * shared memory of one thread-block cluster: 128^2 FP32, 256^2 FP16S): the lattice stays resident in
+ * the cluster's shared memory for up to 4096 steps of one launch, one cluster barrier per step, for
+ * lattices too small to fill the GPU (a step is then launch-bound); lbm_step_planes and lone steps
+ * inside CUDA graphs take PLAIN.  AUTO (default): the autotuner times the eligible ones.  All give
  * bit-identical results.                                                                            */
-enum lbm_kernel { LBM_KERNEL_AUTO = 0, LBM_KERNEL_PLAIN = 1, LBM_KERNEL_ROWS = 2 };
+enum lbm_kernel { LBM_KERNEL_AUTO = 0, LBM_KERNEL_PLAIN = 1, LBM_KERNEL_ROWS = 2, LBM_KERNEL_CLUSTER = 3 };
 int   lbm_set_kernel(lbm_ctx* c, int kind);
-int   lbm_get_kernel(const lbm_ctx* c);              /* the family in use (PLAIN or ROWS), or AUTO before the first step */
+int   lbm_get_kernel(const lbm_ctx* c);              /* the family in use (PLAIN, ROWS or CLUSTER), or AUTO before the first step */
 
 /* ---- test hook of the bounded device-side waits (no counterpart in the reference) --------
  * Arms a one-shot stall of the row pipeline so that tests can drive its bounded mbarrier waits to

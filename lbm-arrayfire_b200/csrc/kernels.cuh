@@ -290,11 +290,13 @@ struct Rounding {
     uint32_t seed;
     bool sr;
 };
+// The seed of step t.
+__device__ __forceinline__ uint32_t seed_of_step(unsigned t) { return mix32(t * 0x9e3779b9u + 0x7f4a7c15u); }
 // The step's seed for a launch reading buffer `parity` (advances the counter pair, see above).
 __device__ __forceinline__ uint32_t step_seed(unsigned* tick, int parity, bool designated) {
     const unsigned t = tick[parity];
     if (designated) tick[parity ^ 1] = t + 1u;
-    return mix32(t * 0x9e3779b9u + 0x7f4a7c15u);
+    return seed_of_step(t);
 }
 template <class S>
 __device__ __forceinline__ Rounding step_rounding(unsigned* tick, int parity, int sr, bool designated) {
@@ -327,16 +329,15 @@ struct PairBits {
     }
 };
 
-// The 16-bit store of a cell's outputs (raw, storage units) at fo[i * N]: directions in pairs (i, i + 1,
-// i in the upper half) through one paired conversion each.
-template <class L, class S, class R>
-__device__ __forceinline__ void store16(S* __restrict__ fo, long long N, const R (&out)[L::Q], const Rounding& rnd,
-                                        uint32_t cell) {
+// The 16-bit encoding of a cell's outputs (raw, storage units): directions in pairs (i, i + 1, i in the
+// upper half) through one paired conversion each; put(i, word) receives direction i's stored word.
+template <class L, class S, class R, class Put>
+__device__ __forceinline__ void encode16(const R (&out)[L::Q], const Rounding& rnd, uint32_t cell, Put&& put) {
     constexpr int NP = (L::Q + 1) / 2;
-    auto put = [&](auto K, uint32_t w) {
+    auto put2 = [&](auto K, uint32_t w) {
         constexpr int i = 2 * decltype(K)::value, j = i + 1;
-        fo[(long long)i * N] = Pair16<S>::hi(w);
-        if constexpr (j < L::Q) fo[(long long)j * N] = Pair16<S>::lo(w);
+        put(std::integral_constant<int, i>{}, Pair16<S>::hi(w));
+        if constexpr (j < L::Q) put(std::integral_constant<int, j>{}, Pair16<S>::lo(w));
     };
     auto second = [&](auto K) -> float {
         constexpr int j = 2 * decltype(K)::value + 1;
@@ -350,11 +351,18 @@ __device__ __forceinline__ void store16(S* __restrict__ fo, long long N, const R
         const PairBits pb{(h << 16) | h};
         static_for<NP>([&](auto K) {
             constexpr int i = 2 * decltype(K)::value;
-            put(K, Pair16<S>::rs(out[i], second(K), pb.template word<i, i + 1>()));
+            put2(K, Pair16<S>::rs(out[i], second(K), pb.template word<i, i + 1>()));
         });
     } else {
-        static_for<NP>([&](auto K) { put(K, Pair16<S>::rn(out[2 * K], second(K))); });
+        static_for<NP>([&](auto K) { put2(K, Pair16<S>::rn(out[2 * K], second(K))); });
     }
+}
+
+// The 16-bit store of a cell's outputs at fo[i * N].
+template <class L, class S, class R>
+__device__ __forceinline__ void store16(S* __restrict__ fo, long long N, const R (&out)[L::Q], const Rounding& rnd,
+                                        uint32_t cell) {
+    encode16<L, S>(out, rnd, cell, [&](auto I, S v) { fo[(long long)decltype(I)::value * N] = v; });
 }
 
 template <class L, class S, bool ABS, class P, class R>

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "cluster.cuh"
 #include "kernels.cuh"
 #include "rowpipe.cuh"
 
@@ -128,6 +129,7 @@ struct lbm_ctx {
     int rows_grid = 0;             // persistent grid of the row pipeline (a whole step)
     int rows_per_sm = 0, sms = 0;  // its CTAs per SM and the device's SMs
     int reserved_sms = 0;          // lbm_set_reserved_sms: SMs the persistent grids leave free
+    int cl_ctas = 0, cl_rows = 0;  // cluster-resident kernel: CTAs of the cluster, rows per CTA
     int rows_rpg = 1;              // its rows per group (segmented rows: the segment width)
     int* err = nullptr;            // device error word of the row pipeline
     unsigned* tick = nullptr;      // the rounding's step counter pair (step_rounding)
@@ -416,6 +418,9 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
         pcnt = planes;
         pstride = 1;
     }
+    // the cluster-resident family runs whole multi-step launches (launch_cluster); anything else it is
+    // asked for (plane sets, graph capture) takes the plain kernel, bit-identical to it
+    if (c->kernel_used == LBM_KERNEL_CLUSTER && block <= 0) block = 128;
     if (c->kernel_used == LBM_KERNEL_ROWS && c->d.collision == LBM_SHANCHEN) {
         const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
         dispatch_storage(c->d.storage, [&](auto tag) {
@@ -501,6 +506,92 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
 
 static int max_block(const lbm_ctx* c) { return c->d.collision == LBM_MRT ? 256 : 512; }
 
+// ---- cluster-resident kernel (cluster.cuh) --------------------------------------------------
+// D2Q9 BGK in deviation arithmetic whose two population buffers fit into the shared memory of one
+// cluster (16 CTAs where the device launches that size, else 8; at most 200 KB per CTA).
+static size_t cluster_smem(const lbm_ctx* c, int rows) {
+    return (size_t)2 * c->q * rows * c->d.nx * c->sbytes + (size_t)rows * c->d.nx;
+}
+
+template <class F>
+static void dispatch_cluster(const lbm_ctx* c, F&& f) {
+    switch (c->d.storage) {
+        case LBM_F32: f(k_step_cluster<float>); break;
+        case LBM_F16S: f(k_step_cluster<__half>); break;
+        case LBM_BF16S: f(k_step_cluster<__nv_bfloat16>); break;
+        default: f(k_step_cluster<double>); break;
+    }
+}
+
+// Sets cl_ctas / cl_rows and returns true when the lattice can run resident in one cluster.
+static bool cluster_eligible(lbm_ctx* c) {
+    const lbm_desc& d = c->d;
+    if (d.lattice != LBM_D2Q9 || d.collision != LBM_BGK || d.arithmetic != LBM_ARITH_DEVIATION) return false;
+    if ((long long)d.nx * d.ny > 16LL * kClusterThreads * 64) return false;
+    bool ok = false;
+    dispatch_cluster(c, [&](auto kern) {
+        for (int ctas : {16, 8}) {
+            const int rows = (int)((d.ny + ctas - 1) / ctas);
+            const size_t smem = cluster_smem(c, rows);
+            if (smem > 200 * 1024) continue;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+                (ctas > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
+                cudaGetLastError();
+                continue;
+            }
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = (unsigned)ctas;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3((unsigned)ctas);
+            cfg.blockDim = dim3(kClusterThreads);
+            cfg.dynamicSmemBytes = smem;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            if (clusters >= 1) {
+                c->cl_ctas = ctas;
+                c->cl_rows = rows;
+                ok = true;
+                return;
+            }
+        }
+    });
+    return ok;
+}
+
+// One launch of k (<= kClusterMaxSteps) steps from buffer `from` into the other one; write_prev: also
+// the state after k - 1 steps into buffer `from` (off for trial launches).
+static void launch_cluster(lbm_ctx* c, int from, cudaStream_t s, int k, bool write_prev = true) {
+    dispatch_storage(c->d.storage, [&](auto tag) {
+        using S = typename decltype(tag)::type;
+        using R = typename Codec<S>::Real;
+        StepParams<R> p = params_of<R>(c);
+        p.fin = c->f[from];
+        p.fout = c->f[from ^ 1];
+        p.parity = from;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)c->cl_ctas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3((unsigned)c->cl_ctas);
+        cfg.blockDim = dim3(kClusterThreads);
+        cfg.dynamicSmemBytes = cluster_smem(c, c->cl_rows);
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_step_cluster<S>, p, c->cl_rows, k, write_prev ? 1 : 0);
+    });
+}
+
 static std::mutex g_tune_mu;
 static std::map<std::string, int> g_tune_cache;
 
@@ -522,6 +613,11 @@ static int autotune(lbm_ctx* c) {
         c->kernel_used = LBM_KERNEL_ROWS;
         return prepare_rows(c);
     }
+    if (c->kernel == LBM_KERNEL_CLUSTER) {
+        if (!cluster_eligible(c)) return set_error(LBM_ERR_UNSUPPORTED, "the lattice does not fit one cluster");
+        c->kernel_used = LBM_KERNEL_CLUSTER;
+        return LBM_OK;
+    }
     if (c->kernel == LBM_KERNEL_PLAIN && c->block) {
         c->kernel_used = LBM_KERNEL_PLAIN;
         return LBM_OK;
@@ -531,11 +627,16 @@ static int autotune(lbm_ctx* c) {
         return LBM_OK;
     }
     const bool try_rows = c->kernel == LBM_KERNEL_AUTO && rows_eligible(c);
-    const std::string key = tune_key(c) + (try_rows ? "/rows" : "/plain");
+    const bool try_cluster = c->kernel == LBM_KERNEL_AUTO && cluster_eligible(c);
+    const std::string key = tune_key(c) + (try_rows ? "/rows" : "/plain") + (try_cluster ? "/cluster" : "");
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
+            if (it->second == -2) {
+                c->kernel_used = LBM_KERNEL_CLUSTER;
+                return LBM_OK;
+            }
             if (it->second < 0) {
                 c->kernel_used = LBM_KERNEL_ROWS;
                 return prepare_rows(c);
@@ -547,7 +648,7 @@ static int autotune(lbm_ctx* c) {
     }
     const int maxb = max_block(c);
     const long long nxr = ((c->d.nx + 31) / 32) * 32;
-    std::vector<int> cands;  // block widths of the plain kernel; -1 = row pipeline
+    std::vector<int> cands;  // block widths of the plain kernel; -1 = row pipeline, -2 = cluster-resident
     for (int b : {32, 64, 128, 256, 512})
         if (b <= maxb && (b <= nxr || b == 32)) cands.push_back(b);
     if (try_rows) {
@@ -555,6 +656,7 @@ static int autotune(lbm_ctx* c) {
         if (rc) return rc;
         cands.push_back(-1);
     }
+    if (try_cluster) cands.push_back(-2);
     int best_b = cands[0];
     if (cands.size() > 1) {
         cudaEvent_t a, b;
@@ -566,10 +668,19 @@ static int autotune(lbm_ctx* c) {
         // short launches to rank candidates a few percent apart), at least 2 and at most 50
         const int reps = (int)std::max(2LL, std::min(50LL, 10000000000LL / std::max(1LL, bytes)));
         for (int blk : cands) {
-            c->kernel_used = blk < 0 ? LBM_KERNEL_ROWS : LBM_KERNEL_PLAIN;
-            launch_step(c, c->cur, c->stream, blk);
-            LBM_CK(cudaEventRecord(a, c->stream));
-            for (int r = 0; r < reps; ++r) launch_step(c, c->cur, c->stream, blk);
+            if (blk == -2) {
+                // one launch of `reps` steps, per step as the others' single launches (its output goes
+                // to the other buffer, as every trial's does)
+                c->kernel_used = LBM_KERNEL_CLUSTER;
+                launch_cluster(c, c->cur, c->stream, 1, false);
+                LBM_CK(cudaEventRecord(a, c->stream));
+                launch_cluster(c, c->cur, c->stream, reps, false);
+            } else {
+                c->kernel_used = blk < 0 ? LBM_KERNEL_ROWS : LBM_KERNEL_PLAIN;
+                launch_step(c, c->cur, c->stream, blk);
+                LBM_CK(cudaEventRecord(a, c->stream));
+                for (int r = 0; r < reps; ++r) launch_step(c, c->cur, c->stream, blk);
+            }
             LBM_CK(cudaEventRecord(b, c->stream));
             LBM_CK(cudaEventSynchronize(b));
             float ms = 0;
@@ -583,7 +694,7 @@ static int autotune(lbm_ctx* c) {
         cudaEventDestroy(b);
         LBM_CK(cudaGetLastError());
     }
-    c->kernel_used = best_b < 0 ? LBM_KERNEL_ROWS : LBM_KERNEL_PLAIN;
+    c->kernel_used = best_b == -2 ? LBM_KERNEL_CLUSTER : best_b < 0 ? LBM_KERNEL_ROWS : LBM_KERNEL_PLAIN;
     c->block = best_b < 0 ? 0 : best_b;
     std::lock_guard<std::mutex> g(g_tune_mu);
     g_tune_cache[key] = best_b;
@@ -869,6 +980,14 @@ int lbm_step(lbm_ctx* c, int64_t nsteps) {
     }
     LBM_CK(cudaEventRecord(c->e0, c->stream));
     long long n = nsteps;
+    if (c->kernel_used == LBM_KERNEL_CLUSTER) {
+        while (n > 0) {
+            const int k = (int)std::min<long long>(n, kClusterMaxSteps);
+            launch_cluster(c, c->cur, c->stream, k);
+            c->cur ^= 1;
+            n -= k;
+        }
+    }
     if (c->stall_armed) {
         // the armed test stall: one direct launch with its wait limits, before any graph (which
         // captures the production limits)
@@ -1091,8 +1210,15 @@ int lbm_get_block(const lbm_ctx* c) { return c ? c->block : 0; }
 
 int lbm_set_kernel(lbm_ctx* c, int kind) {
     if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
-    if (kind != LBM_KERNEL_AUTO && kind != LBM_KERNEL_PLAIN && kind != LBM_KERNEL_ROWS)
+    if (kind != LBM_KERNEL_AUTO && kind != LBM_KERNEL_PLAIN && kind != LBM_KERNEL_ROWS && kind != LBM_KERNEL_CLUSTER)
         return set_error(LBM_ERR_INVALID, "unknown kernel family");
+    if (kind == LBM_KERNEL_CLUSTER) {
+        LBM_CK(cudaSetDevice(c->d.device));
+        if (!cluster_eligible(c))
+            return set_error(LBM_ERR_UNSUPPORTED,
+                             "the cluster-resident kernel needs D2Q9 BGK, deviation arithmetic and both population "
+                             "buffers within one cluster's shared memory");
+    }
     if (kind == LBM_KERNEL_ROWS && !rows_eligible(c))
         return set_error(LBM_ERR_UNSUPPORTED,
                          "the row pipeline needs D3Q27 BGK/MRT or D2Q9 BGK, deviation arithmetic, F32/F16S/BF16S "
@@ -1102,7 +1228,7 @@ int lbm_set_kernel(lbm_ctx* c, int kind) {
     drop_graphs(c);
     c->kernel = kind;
     c->kernel_used = 0;
-    if (kind == LBM_KERNEL_ROWS) c->block = 0;
+    if (kind == LBM_KERNEL_ROWS || kind == LBM_KERNEL_CLUSTER) c->block = 0;
     return LBM_OK;
 }
 

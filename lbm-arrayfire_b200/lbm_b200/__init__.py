@@ -35,7 +35,7 @@ STORAGE_BYTES = {F32: 4, F16S: 2, BF16S: 2, F64: 8}  # bytes of one stored popul
 MRT_REF, MRT_GRAM_SCHMIDT = 0, 1
 ARITH_DEVIATION, ARITH_ABSOLUTE = 0, 1
 ROUND_STOCHASTIC, ROUND_NEAREST = 0, 1
-KERNEL_AUTO, KERNEL_PLAIN, KERNEL_ROWS = 0, 1, 2
+KERNEL_AUTO, KERNEL_PLAIN, KERNEL_ROWS, KERNEL_CLUSTER = 0, 1, 2, 3
 BATCH_AUTO, BATCH_TILES, BATCH_ROWS, BATCH_ROWS_PER_FAMILY = 0, 1, 2, 3
 DTYPE_F32, DTYPE_F64 = 0, 1
 HOST, DEVICE = 0, 1
@@ -365,7 +365,8 @@ class Lattice:
         return lib().lbm_get_block(self._h)
 
     def set_kernel(self, kind: int):
-        """KERNEL_AUTO, KERNEL_PLAIN or KERNEL_ROWS (bulk-copy row pipeline)."""
+        """KERNEL_AUTO, KERNEL_PLAIN, KERNEL_ROWS (bulk-copy row pipeline) or KERNEL_CLUSTER (small D2Q9
+        BGK lattices resident in one thread-block cluster's shared memory)."""
         _check(lib().lbm_set_kernel(self._h, kind))
 
     def kernel(self) -> int:

@@ -530,3 +530,71 @@ def test_batch_members_match_the_oracle(storage, mode, tol):
         Fo, _, _ = O.run(p, F0, 120)
         assert rel_l2(b.get_populations(k, np.float64), Fo) < tol, (k, rel_l2(b.get_populations(k, np.float64), Fo))
     b.close()
+
+
+def _cluster_case(case, storage):
+    if case == "cavity128":
+        return cavity2d(n=128, storage=storage)
+    if case == "cavity_odd":  # rows not a multiple of the cluster size, a short and an empty CTA
+        d, m, F0 = cavity2d(n=100, storage=storage)
+        return d, m, F0
+    if case == "channel":  # equilibrium inlet, zero-gradient outlet, a solid circle
+        return channel2d(96, 40, 0.04, 100.0, 24, 20, 6, storage=storage, config_mode=True, seed=4, noise=1e-3)
+    # periodic, no mask, a thin lattice: rows 1 per CTA and a lattice one row high per CTA pair
+    d = lb.make_desc(lb.D2Q9, lb.BGK, storage, (48, 10), omega=1.7)
+    _, _, _, w, _ = lb.velocities(lb.D2Q9)
+    rng = np.random.default_rng(5)
+    return d, None, np.repeat(w, d.cells) * (1.0 + 0.02 * rng.standard_normal(9 * d.cells))
+
+
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.BF16S, lb.F64])
+@pytest.mark.parametrize("case", ["cavity128", "cavity_odd", "channel", "periodic_thin"])
+def test_cluster_resident_kernel_equals_plain(storage, case):
+    """LBM_KERNEL_CLUSTER (the lattice resident in one thread-block cluster's shared memory for many
+    steps per launch) is bit-identical to the plain kernel: runs of 1, 3, 10 and 4100 steps (two
+    launches), stochastic rounding for the 16-bit storage, and a step cut into plane sets (which take
+    the plain kernel) in between."""
+    d, m, F0 = _cluster_case(case, storage)
+    F0 = np.asarray(F0, dtype=np.float64)
+    with lb.Lattice(d, m) as a, lb.Lattice(d, m) as b:
+        a.set_kernel(lb.KERNEL_PLAIN)
+        b.set_kernel(lb.KERNEL_CLUSTER)
+        for lat in (a, b):
+            lat.set_populations(F0)
+        for n in (1, 3, 10):
+            a.step(n)
+            b.step(n)
+            assert b.kernel() == lb.KERNEL_CLUSTER
+            assert np.array_equal(a.get_populations(np.float64), b.get_populations(np.float64)), n
+            # the macros pull the previous step's populations: a multi-step launch leaves them too
+            (ra, ua), (rb, ub) = a.macros(np.float64), b.macros(np.float64)
+            assert np.array_equal(ra, rb) and np.array_equal(ua, ub), n
+        a.step(1)
+        b.step_planes(0, 1, False)
+        b.step_planes(1, d.ny - 1, True)
+        a.step(4100)
+        b.step(4100)
+        assert a.steps_done == b.steps_done == 4115
+        ref, got = a.get_populations(np.float64), b.get_populations(np.float64)
+        (ra, ua), (rb, ub) = a.macros(np.float64), b.macros(np.float64)
+        assert np.array_equal(ra, rb) and np.array_equal(ua, ub)
+    assert np.isfinite(got).all() and np.array_equal(got, ref)
+
+
+def test_cluster_kernel_is_refused_where_it_does_not_fit():
+    d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (1024, 256), omega=1.2)
+    with lb.Lattice(d, None) as lat:
+        with pytest.raises(lb.LbmError):
+            lat.set_kernel(lb.KERNEL_CLUSTER)
+    d = lb.make_desc(lb.D3Q27, lb.BGK, lb.F32, (16, 16, 16), omega=1.2)
+    with lb.Lattice(d, None) as lat:
+        with pytest.raises(lb.LbmError):
+            lat.set_kernel(lb.KERNEL_CLUSTER)
+
+
+def test_autotune_picks_the_cluster_kernel_for_the_128_cavity():
+    d, m, F0 = cavity2d(n=128)
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(F0)
+        lat.step(2)
+        assert lat.kernel() == lb.KERNEL_CLUSTER
