@@ -174,12 +174,20 @@ constexpr unsigned long long pack_c(bool z) {
 #ifndef LBM_ROWPIPE_PAIR_WARPS3
 #define LBM_ROWPIPE_PAIR_WARPS3 15  // D3Q27 consumer warps with pairs: 16 warps in all, 4 per sub-partition
 #endif
+// D3Q27 consumer warps with pairs in the single-lattice row-group kernel (k_step_rows): 11 + the producer
+// = 3 warps per sub-partition, up to 168 registers a thread.  A/B on B200 at 1965 MHz, 15 vs 11 warps,
+// MLUPS: MRT 256^3 F16S 50.2k vs 51.8k, D3Q27 BGK 256^3 F16S 52.6k vs 54.0k; 9 warps (uneven across
+// the sub-partitions) 44.0k, 7 warps 50.2k.  The segmented kernel (4096 x 64 x 64: 45.2k vs 45.1k) and
+// the ensemble kernel (54.6k vs 53.7k) keep 15.
+#ifndef LBM_ROWPIPE_PAIR_WARPS3_ROWS
+#define LBM_ROWPIPE_PAIR_WARPS3_ROWS 11
+#endif
 
 // The row kernel's consumers take pairs of adjacent cells (row_pair) for this lattice, storage and collision.
 template <class L, class S, int COLL>
 constexpr bool kRowPair = LBM_ROWPIPE_PAIR && Codec<S>::kScaled && (COLL == 0 || COLL == 3);
 
-template <class L, class S, int PITCH, bool SEG = false, bool PAIR = false>
+template <class L, class S, int PITCH, bool SEG = false, bool PAIR = false, int PAIRW = LBM_ROWPIPE_PAIR_WARPS3>
 struct RowPipeShape {
     static constexpr int HALO = 8;
     static constexpr int SEGW = PITCH - 2 * HALO;
@@ -209,9 +217,10 @@ struct RowPipeShape {
     static constexpr int CR = CR0 < 1 ? 1 : CR0;
     // D3Q27 consumer warps (0: CR row sets of THREADS): the register file holds 5 warps of 96
     // registers per SM sub-partition, i.e. up to 19 consumer warps beside the producer
-    // with pairs a D3Q27 thread holds two cells' outputs: 15 consumer warps + the producer keep every
-    // sub-partition at 4 warps, i.e. up to 128 registers a thread (17 warps put 5 on one: 96 at most)
-    static constexpr int CONSUMERS = PAIR && k3                       ? LBM_ROWPIPE_PAIR_WARPS3 * 32
+    // with pairs a D3Q27 thread holds two cells' outputs: PAIRW consumer warps + the producer, 15 (every
+    // sub-partition at 4 warps, up to 128 registers a thread; 17 warps put 5 on one: 96 at most) or 11
+    // (3 warps each, up to 168 registers: the single-lattice row-group kernel)
+    static constexpr int CONSUMERS = PAIR && k3                       ? PAIRW * 32
                                      : k3 && LBM_ROWPIPE_CWARPS3 > 0    ? LBM_ROWPIPE_CWARPS3 * 32
                                      : !k3 && LBM_ROWPIPE_CWARPS2 > 0 ? LBM_ROWPIPE_CWARPS2 * 32
                                                                        : CR * THREADS;
@@ -428,7 +437,7 @@ __device__ __forceinline__ void row_pair_wrap(const P& p, const S* st, const uin
 //   empty[s]  every consumer warp has finished reading stage s
 // Stage s holds, for direction i, the group's source rows at in[(s * Q + i) * SB + b * nx].
 template <class L, class S, int PITCH, int COLL>
-using RowShape = RowPipeShape<L, S, PITCH, false, kRowPair<L, S, COLL>>;
+using RowShape = RowPipeShape<L, S, PITCH, false, kRowPair<L, S, COLL>, LBM_ROWPIPE_PAIR_WARPS3_ROWS>;
 
 template <class L, class S, int PITCH, int COLL>
 __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, RowShape<L, S, PITCH, COLL>::CTAS)

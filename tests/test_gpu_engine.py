@@ -401,18 +401,24 @@ def test_row_pipeline_segmented_wide_rows_equal_plain(storage, case):
 @pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.F64])
 @pytest.mark.parametrize("arith", [lb.ARITH_ABSOLUTE, lb.ARITH_DEVIATION])
 @pytest.mark.parametrize("shape,solid", [((128, 128), False), ((100, 50), True), ((20, 10), False),
-                                         ((48, 36), True)])
+                                         ((48, 36), True), ((200, 24), "zerograd")])
 def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
     """The one-pass Shan-Chen kernel (KERNEL_ROWS: a window sliding down y, psi of the next row in a
     shared ring) against the two-pass kernels (KERNEL_PLAIN: psi through global memory): bit-identical
-    populations and fields, on full and partial column strips, a lattice narrower than a strip, and
-    with solid (bounce-back, set-density) cells."""
+    populations and fields, on full and partial column strips, a lattice narrower than a strip, with
+    solid (bounce-back, set-density) cells, and with zero-gradient outlet columns on both sides of the
+    first strip edge (x = 127 and 128: the window pulls them both as its own cells and as the
+    neighbouring strip's edge column)."""
     if arith == lb.ARITH_ABSOLUTE and storage == lb.F16S:
         pytest.skip("absolute arithmetic is F32/F64 only")
     d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, storage, shape, omega=1.0, sc_G=-4.5, arithmetic=arith)
     m = None
     n = d.cells
-    if solid:
+    if solid == "zerograd":
+        lb.set_classes(d, [(0, 1.0, 0.0, 0.0, 0.0), (lb.ZEROGRAD_XP, 1.0, 0.0, 0.0, 0.0)])
+        xx = np.repeat(np.arange(shape[0])[None, :], shape[1], axis=0).ravel()  # x of cell x + nx y
+        m = ((xx == 127) | (xx == 128) | (xx == shape[0] - 1)).astype(np.uint8)
+    elif solid:
         lb.set_classes(d, [(0, 1.0, 0.0, 0.0, 0.0), (lb.BOUNCE | lb.SET_RHO | lb.SET_UX | lb.SET_UY, 0.5, 0.0, 0.0, 0.0)])
         xx, yy = np.meshgrid(np.arange(shape[0]), np.arange(shape[1]), indexing="ij")
         m = ((xx - shape[0] // 3) ** 2 + (yy - shape[1] // 2) ** 2 <= (min(shape) // 5) ** 2).astype(np.uint8)
