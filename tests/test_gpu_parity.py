@@ -191,6 +191,37 @@ def test_shanchen_periodic(arith):
     check_fp32(d, m, F0, 500, arith, fields=False)
 
 
+@pytest.mark.parametrize("kind", [lb.KERNEL_PLAIN, lb.KERNEL_ROWS])
+def test_shanchen_config_size(kind):
+    """The Shan-Chen configuration at its own size (1024^2, G = -5.5, rho 0.693 + 0.01 noise, tau 1):
+    the FP64 engine against the FP64 oracle over 200 steps (both kernel families: the two passes and
+    the one-pass window), the FP32 engine against the FP32 oracle over 30 steps (the reference's
+    arithmetic; spinodal decomposition amplifies rounding differences beyond that), and the total
+    mass of FP32 and 16-bit (BF16S) runs against the start over 200 steps."""
+    d, m, F0 = shanchen(n=1024, G=-5.5, rho0=0.693, amp=0.01, seed=3)
+
+    def engine(storage, steps, arithmetic=DEV):
+        d.storage, d.arithmetic = storage, arithmetic
+        with lb.Lattice(d, m) as lat:
+            lat.set_kernel(kind)
+            lat.set_populations(F0)
+            s0 = lat.sums()
+            lat.step(steps)
+            assert lat.kernel() == kind
+            return lat.get_populations(np.float64), lat.sums()[0] / s0[0] - 1.0
+
+    F64, dm64 = engine(lb.F64, 200)
+    Fo64, _, _ = run_oracle(d, m, F0, 200)
+    assert rel_l2(F64, Fo64) < 1e-11
+    assert abs(dm64) < 1e-13
+    F32, _ = engine(lb.F32, 30, ABS)
+    Fo32, _, _ = run_oracle(d, m, F0, 30, np.float32)
+    assert rel_l2(F32, Fo32) < TOL_F32
+    _, dm32 = engine(lb.F32, 200)
+    _, dm16 = engine(lb.BF16S, 200)
+    assert abs(dm32) < 1e-5 and abs(dm16) < 1e-4, (dm32, dm16)
+
+
 @pytest.mark.parametrize("storage,tol", [(lb.F16S, 1e-3), (lb.BF16S, 5e-2)])
 def test_shifted_storage_accuracy_cavity(storage, tol):
     d, m, F0 = cavity2d(n=128, u_lid=0.1, re=100.0, storage=lb.F64)
