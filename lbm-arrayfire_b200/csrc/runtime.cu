@@ -582,6 +582,9 @@ static void launch_cluster(lbm_ctx* c, int from, cudaStream_t s, int k, bool wri
         attr[0].val.clusterDim.x = (unsigned)c->cl_ctas;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
+        // the attribute is per kernel, not per context: set it for this lattice before every launch
+        cudaFuncSetAttribute(k_step_cluster<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)cluster_smem(c, c->cl_rows));
         cfg.gridDim = dim3((unsigned)c->cl_ctas);
         cfg.blockDim = dim3(kClusterThreads);
         cfg.dynamicSmemBytes = cluster_smem(c, c->cl_rows);

@@ -598,6 +598,28 @@ def test_cluster_kernel_is_refused_where_it_does_not_fit():
             lat.set_kernel(lb.KERNEL_CLUSTER)
 
 
+def test_cluster_kernel_contexts_of_different_sizes_interleaved():
+    """The cluster kernel's shared-memory size is a per-kernel attribute: a context set up after a
+    larger one (which lowers it) must not break the larger one's next launch."""
+    big, small = cavity2d(n=128), cavity2d(n=64)
+    with lb.Lattice(big[0], big[1]) as a, lb.Lattice(big[0], big[1]) as ref:
+        ref.set_kernel(lb.KERNEL_PLAIN)
+        a.set_kernel(lb.KERNEL_CLUSTER)
+        for lat in (a, ref):
+            lat.set_populations(big[2])
+            lat.step(5)
+        with lb.Lattice(small[0], small[1]) as b:
+            b.set_kernel(lb.KERNEL_CLUSTER)
+            b.set_populations(small[2])
+            b.step(5)
+            a.step(7)
+            ref.step(7)
+            b.step(3)
+            b.sync()
+            a.sync()
+        assert np.array_equal(a.get_populations(np.float64), ref.get_populations(np.float64))
+
+
 def test_autotune_picks_the_cluster_kernel_for_the_128_cavity():
     d, m, F0 = cavity2d(n=128)
     with lb.Lattice(d, m) as lat:
