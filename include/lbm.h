@@ -99,6 +99,14 @@ enum lbm_memory    { LBM_HOST = 0, LBM_DEVICE = 1 };
 #define LBM_CELL_EQUILIBRIUM  0x20u /* write feq(rho,u) for every direction (Dirichlet equilibrium) */
 #define LBM_CELL_ZEROGRAD_XP  0x40u /* outlet on the x = nx-1 face: populations arriving from +x are
                                        copied from the streamed state of cell x-1 (zero gradient)  */
+/* Zou-He open boundaries (Zou & He 1997; no counterpart in the reference, whose only open boundaries
+ * are the density/velocity overwrites above).  D2Q9 BGK only.  Before the collision the populations
+ * that arrive from outside the lattice are rebuilt from the known ones so that the cell has the
+ * prescribed velocity or density; the collision then proceeds as for fluid.                       */
+#define LBM_CELL_ZOUHE_VEL_XM 0x80u /* velocity inlet on the x = 0 face: class (ux, uy) prescribed,
+                                       rho and the populations with c_x = +1 follow               */
+#define LBM_CELL_ZOUHE_RHO_XP 0x100u /* pressure outlet on the x = nx-1 face: class rho and uy
+                                       prescribed, ux and the populations with c_x = -1 follow     */
 
 typedef struct lbm_cell_class {
     uint32_t flags;
@@ -301,7 +309,8 @@ int lbm_setup_cavity3d(lbm_desc* d, uint8_t* mask, double u_lid);
 /* D2Q9 channel: solid circle (x-ox)^2+(y-oy)^2 <= r^2 and rows y=0, y=ny-1.  config_mode = 0 gives the
  * reference's equilibrium forcing (inlet u_x + rho=1 at x=0, rho=1 at x=nx-1, periodic in x;
  * cpp/d2q9_bgk_channel_packed.cpp:37-39,64-69).  config_mode = 1 gives an equilibrium inlet
- * (rho=1, u=(u_in,0)) and a zero-gradient outlet.                                               */
+ * (rho=1, u=(u_in,0)) and a zero-gradient outlet; config_mode = 2 a Zou-He velocity inlet
+ * (u=(u_in,0)) and a Zou-He pressure outlet (rho=1, uy=0).                                       */
 int lbm_setup_channel2d(lbm_desc* d, uint8_t* mask, double u_in, double ox, double oy, double r,
                         int config_mode);
 /* D3Q27 duct: walls y=0, y=ny-1, z=0, z=nz-1, solid sphere centre (ox,oy,oz) radius r,

@@ -22,7 +22,7 @@
 namespace lbm {
 
 constexpr uint32_t kBounce = 0x01u, kSetRho = 0x02u, kSetUx = 0x04u, kSetUy = 0x08u, kSetUz = 0x10u,
-                   kEquilibrium = 0x20u, kZeroGradXp = 0x40u;
+                   kEquilibrium = 0x20u, kZeroGradXp = 0x40u, kZouHeVelXm = 0x80u, kZouHeRhoXp = 0x100u;
 constexpr int kMaxClasses = 16;
 
 template <class R>
@@ -401,14 +401,50 @@ __device__ __forceinline__ void cell_class(const uint8_t* __restrict__ mask, con
     fl = ct.flags[cls];
 }
 
+// Zou-He open boundaries of D2Q9 (Zou & He 1997, the velocity condition on the x = 0 face and the
+// pressure condition on the x = nx-1 face): the streamed populations that arrive from outside the
+// lattice (c_x = +1 at the inlet, c_x = -1 at the outlet) are rebuilt from the known ones so that the
+// cell has the class's velocity (inlet) or density (outlet), with the non-equilibrium parts bounced
+// back.  Directions 1 E, 2 N, 3 W, 4 S, 5 NE, 6 NW, 7 SW, 8 SE.  v: populations (ABS) or deviations in
+// storage units (the weights of a rebuilt direction and its source agree, so deviations satisfy the
+// same relations with every rho u term in storage units); sc / isc the storage scale and its inverse.
+template <bool ABS, class T, class R>
+__device__ __forceinline__ void zouhe_d2q9(const ClassTable<T>& ct, int cls, uint32_t fl, R (&v)[9], R sc, R isc) {
+    const R k = ABS ? R(1) : sc;
+    const R uy = R(ct.uy[cls]);
+    const R half = R(0.5), sixth = R(1.0 / 6.0), two3 = R(2.0 / 3.0);
+    const R t24 = half * (v[2] - v[4]);
+    if (fl & kZouHeVelXm) {
+        const R ux = R(ct.ux[cls]);
+        const R s = v[0] + v[2] + v[4] + R(2) * (v[3] + v[6] + v[7]);
+        const R rho = (ABS ? s : mad(s, isc, R(1))) / (R(1) - ux);
+        const R ru = (rho * k) * ux, rv = (rho * k) * uy;
+        v[1] = mad(two3, ru, v[3]);
+        v[5] = mad(half, rv, mad(sixth, ru, v[7] - t24));
+        v[8] = mad(-half, rv, mad(sixth, ru, v[6] + t24));
+    } else {
+        const R rho = R(ct.rho[cls]);
+        const R s = v[0] + v[2] + v[4] + R(2) * (v[1] + v[5] + v[8]);
+        const R ux = (ABS ? s : mad(s, isc, R(1))) / rho - R(1);
+        const R ru = (rho * k) * ux, rv = (rho * k) * uy;
+        v[3] = mad(-two3, ru, v[1]);
+        v[7] = mad(-half, rv, mad(-sixth, ru, v[5] + t24));
+        v[6] = mad(half, rv, mad(-sixth, ru, v[8] - t24));
+    }
+}
+
 // ---- BGK ---------------------------------------------------------------------------------
 // Collision of one cell from its streamed populations v (ABS) or deviations v = f - w:
 // F = omega FEQ + (1 - omega) F_streamed (cpp/d2q9_bgk_lid.cpp:153), the class overwrites before it
 // and the full-way bounce-back after it (:155).  P supplies cls, omega, one_m_omega.  Deviations
-// are in storage units: sc / isc are the storage scale and its inverse (1 for ABS).
+// are in storage units: sc / isc are the storage scale and its inverse (1 for ABS).  A Zou-He cell
+// (D2Q9) first rebuilds its incoming populations in v.
 template <class L, bool ABS, bool EXACTW, class P, class R>
-__device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, const R (&v)[L::Q], R sc, R isc,
+__device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, R (&v)[L::Q], R sc, R isc,
                                             R (&out)[L::Q]) {
+    if constexpr (L::Q == 9) {
+        if (fl & (kZouHeVelXm | kZouHeRhoXp)) zouhe_d2q9<ABS>(p.cls, cls, fl, v, sc, isc);
+    }
     R rho, drho, ux, uy, uz;
     moments<L, ABS>(v, sc, isc, rho, drho, ux, uy, uz);
     if (fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);
@@ -944,6 +980,9 @@ __global__ void k_macros(const __grid_constant__ StepParams<typename Codec<S>::R
     }
     R sc, isc;
     storage_scale<S>(p, sc, isc);
+    if constexpr (L::Q == 9) {
+        if (pulled && (fl & (kZouHeVelXm | kZouHeRhoXp))) zouhe_d2q9<false>(p.cls, cls, fl, d, sc, isc);
+    }
     R rho, drho, ux, uy, uz;
     moments<L, false>(d, sc, isc, rho, drho, ux, uy, uz);
     if (pulled && fl) apply_class(p.cls, cls, fl, rho, drho, ux, uy, uz, L::DIM);

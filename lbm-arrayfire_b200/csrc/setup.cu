@@ -69,8 +69,19 @@ int validate_desc(const lbm_desc* d) {
         double m = std::frexp(d->storage_scale, &e);
         if (m != 0.5) return set_error(LBM_ERR_INVALID, "storage_scale must be a power of two");
     }
-    for (int k = 0; k < d->n_classes; ++k)
-        if (d->classes[k].flags & ~0x7fu) return set_error(LBM_ERR_INVALID, "unknown cell-class flag");
+    for (int k = 0; k < d->n_classes; ++k) {
+        const uint32_t fl = d->classes[k].flags;
+        if (fl & ~0x1ffu) return set_error(LBM_ERR_INVALID, "unknown cell-class flag");
+        if ((fl & (LBM_CELL_ZOUHE_VEL_XM | LBM_CELL_ZOUHE_RHO_XP)) &&
+            (d->lattice != LBM_D2Q9 || d->collision != LBM_BGK))
+            return set_error(LBM_ERR_UNSUPPORTED, "Zou-He boundaries are built for D2Q9 BGK only");
+        if ((fl & LBM_CELL_ZOUHE_VEL_XM) && (fl & LBM_CELL_ZOUHE_RHO_XP))
+            return set_error(LBM_ERR_INVALID, "a class is either a Zou-He inlet or a Zou-He outlet");
+        if ((fl & LBM_CELL_ZOUHE_VEL_XM) && !(d->classes[k].ux < 1.0))
+            return set_error(LBM_ERR_INVALID, "a Zou-He inlet needs ux < 1");
+        if ((fl & LBM_CELL_ZOUHE_RHO_XP) && !(d->classes[k].rho > 0.0))
+            return set_error(LBM_ERR_INVALID, "a Zou-He outlet needs rho > 0");
+    }
     return LBM_OK;
 }
 
@@ -257,6 +268,7 @@ int lbm_setup_channel2d(lbm_desc* d, uint8_t* mask, double u_in, double ox, doub
                         int config_mode) {
     if (!d || !mask || d->lattice != LBM_D2Q9 || d->nx < 3 || d->ny < 3)
         return set_error(LBM_ERR_INVALID, "channel2d needs a D2Q9 descriptor with nx, ny >= 3 and a mask");
+    if (config_mode < 0 || config_mode > 2) return set_error(LBM_ERR_INVALID, "config_mode must be 0, 1 or 2");
     const int64_t nx = d->nx, ny = d->ny;
     // classes: 0 fluid, 1 solid, 2 inlet, 3 outlet, 4 solid cell on the inlet/outlet column
     for (int64_t y = 0; y < ny; ++y)
@@ -284,6 +296,10 @@ int lbm_setup_channel2d(lbm_desc* d, uint8_t* mask, double u_in, double ox, doub
         set_class(d, 2, LBM_CELL_SET_UX | LBM_CELL_SET_RHO, 1, u_in, 0, 0);
         set_class(d, 3, LBM_CELL_SET_RHO, 1, 0, 0, 0);
         set_class(d, 4, kSolidFlags, 1, 0, 0, 0);
+    } else if (config_mode == 2) {
+        set_class(d, 2, LBM_CELL_ZOUHE_VEL_XM, 1, u_in, 0, 0);
+        set_class(d, 3, LBM_CELL_ZOUHE_RHO_XP, 1, 0, 0, 0);
+        set_class(d, 4, kSolidFlags, 0, 0, 0, 0);
     } else {
         set_class(d, 2, LBM_CELL_EQUILIBRIUM | LBM_CELL_SET_RHO | LBM_CELL_SET_UX | LBM_CELL_SET_UY | LBM_CELL_SET_UZ,
                   1, u_in, 0, 0);

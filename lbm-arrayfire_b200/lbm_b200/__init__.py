@@ -21,7 +21,8 @@ __all__ = [
     "LIB_PATH", "lib", "LbmError", "Desc", "CellClass", "Lattice", "Batch",
     "D2Q9", "D3Q27", "BGK", "MRT", "SHANCHEN", "F32", "F16S", "BF16S", "F64",
     "MRT_REF", "MRT_GRAM_SCHMIDT", "BOUNCE", "SET_RHO", "SET_UX", "SET_UY", "SET_UZ",
-    "EQUILIBRIUM", "ZEROGRAD_XP", "velocities", "omega_from_re", "mrt_reference_rates", "mrt_rates",
+    "EQUILIBRIUM", "ZEROGRAD_XP", "ZOUHE_VEL_XM", "ZOUHE_RHO_XP", "velocities", "omega_from_re",
+    "mrt_reference_rates", "mrt_rates",
     "mrt_collide_host", "setup_cavity2d", "setup_cavity3d", "setup_channel2d", "setup_duct3d",
     "mask_from_index_list", "EXPORTED_SYMBOLS", "ROUND_STOCHASTIC", "ROUND_NEAREST",
 ]
@@ -40,6 +41,7 @@ BATCH_AUTO, BATCH_TILES, BATCH_ROWS, BATCH_ROWS_PER_FAMILY = 0, 1, 2, 3
 DTYPE_F32, DTYPE_F64 = 0, 1
 HOST, DEVICE = 0, 1
 BOUNCE, SET_RHO, SET_UX, SET_UY, SET_UZ, EQUILIBRIUM, ZEROGRAD_XP = 1, 2, 4, 8, 16, 32, 64
+ZOUHE_VEL_XM, ZOUHE_RHO_XP = 128, 256  # Zou-He velocity inlet (x = 0), pressure outlet (x = nx-1); D2Q9 BGK
 MAX_CLASSES = 16
 
 ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "diverged",
@@ -264,7 +266,9 @@ def setup_cavity3d(d: Desc, u_lid: float) -> np.ndarray:
     return m
 
 
-def setup_channel2d(d: Desc, u_in: float, ox: float, oy: float, r: float, config_mode: bool) -> np.ndarray:
+def setup_channel2d(d: Desc, u_in: float, ox: float, oy: float, r: float, config_mode: int) -> np.ndarray:
+    """config_mode 0: the reference's boundaries; 1: equilibrium inlet, zero-gradient outlet; 2: Zou-He
+    velocity inlet and pressure outlet."""
     m = _mask_buf(d)
     _check(lib().lbm_setup_channel2d(C.byref(d), _ptr(m), u_in, ox, oy, r, int(config_mode)))
     return m

@@ -32,6 +32,8 @@
 #define ORC_SET_UZ      0x10u
 #define ORC_EQUILIBRIUM 0x20u
 #define ORC_ZEROGRAD_XP 0x40u
+#define ORC_ZOUHE_VEL_XM 0x80u
+#define ORC_ZOUHE_RHO_XP 0x100u
 
 typedef struct orc_desc {
     int32_t lattice;     /* 0 = D2Q9, 1 = D3Q27 */

@@ -22,6 +22,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liblbm_oracle.so"
 
 BOUNCE, SET_RHO, SET_UX, SET_UY, SET_UZ, EQUILIBRIUM, ZEROGRAD_XP = 1, 2, 4, 8, 16, 32, 64
+ZOUHE_VEL_XM, ZOUHE_RHO_XP = 128, 256
 
 
 class OrcDesc(C.Structure):

@@ -74,11 +74,13 @@ def cavity2d(nx: int, ny: int, u_lid: float, omega: float) -> O.Problem:
 
 
 def channel2d(nx: int, ny: int, u_in: float, ox: float, oy: float, r: float, omega: float,
-              config_mode: bool = False) -> O.Problem:
+              config_mode: int = 0) -> O.Problem:
     """cpp/d2q9_bgk_channel_packed.cpp: solid circle (x-ox)^2 + (y-oy)^2 <= r^2 and rows y = 0,
     y = ny-1 (:37-39).  Reference BCs (:64-69), in order: UX(0,:) = u_max; UX/UY/DENSITY(ON) = 0;
-    DENSITY(0,:) = DENSITY(nx-1,:) = 1 -- so solid cells of the end columns keep rho = 1.  Config mode:
-    an equilibrium inlet (rho = 1, u = (u_in, 0)) at x = 0 and a zero-gradient outlet at x = nx-1."""
+    DENSITY(0,:) = DENSITY(nx-1,:) = 1 -- so solid cells of the end columns keep rho = 1.  Config mode
+    1: an equilibrium inlet (rho = 1, u = (u_in, 0)) at x = 0 and a zero-gradient outlet at x = nx-1.
+    Config mode 2: a Zou-He velocity inlet (u = (u_in, 0)) and a Zou-He pressure outlet (rho = 1,
+    uy = 0), the open boundaries of Zou & He (1997)."""
     x, y = _grid2(nx, ny)
     solid = ((x - ox) ** 2 + (y - oy) ** 2 <= r * r) | (y == 0) | (y == ny - 1)
     end = (x == 0) | (x == nx - 1)
@@ -86,7 +88,10 @@ def channel2d(nx: int, ny: int, u_in: float, ox: float, oy: float, r: float, ome
     cls[(x == 0) & ~solid] = 2
     cls[(x == nx - 1) & ~solid] = 3
     cls[solid] = 1
-    if config_mode:
+    if config_mode == 2:
+        classes = [(0, 1.0, 0.0, 0.0, 0.0), (SOLID, 0.0, 0.0, 0.0, 0.0), (O.ZOUHE_VEL_XM, 1.0, u_in, 0.0, 0.0),
+                   (O.ZOUHE_RHO_XP, 1.0, 0.0, 0.0, 0.0)]
+    elif config_mode:
         classes = [(0, 1.0, 0.0, 0.0, 0.0), (SOLID, 0.0, 0.0, 0.0, 0.0), (EQ_INLET, 1.0, u_in, 0.0, 0.0),
                    (O.ZEROGRAD_XP, 1.0, 0.0, 0.0, 0.0)]
     else:

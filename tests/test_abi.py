@@ -152,7 +152,23 @@ def test_descriptor_validation_precedes_device():
     d.n_classes = 0
     bad.append((d, -1))
     d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (8, 8))
-    d.classes[0].flags = 0x100
+    d.classes[0].flags = 0x200
+    bad.append((d, -1))
+    # Zou-He classes: D2Q9 BGK only, one side per class, an inlet slower than 1, an outlet denser than 0
+    d = lb.make_desc(lb.D3Q27, lb.BGK, lb.F32, (8, 8, 8))
+    lb.set_classes(d, [(0, 1, 0, 0, 0), (lb.ZOUHE_VEL_XM, 1, 0.05, 0, 0)])
+    bad.append((d, -5))
+    d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, lb.F32, (8, 8), sc_G=-5.5)
+    lb.set_classes(d, [(0, 1, 0, 0, 0), (lb.ZOUHE_RHO_XP, 1, 0, 0, 0)])
+    bad.append((d, -5))
+    d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (8, 8))
+    lb.set_classes(d, [(0, 1, 0, 0, 0), (lb.ZOUHE_VEL_XM | lb.ZOUHE_RHO_XP, 1, 0.05, 0, 0)])
+    bad.append((d, -1))
+    d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (8, 8))
+    lb.set_classes(d, [(0, 1, 0, 0, 0), (lb.ZOUHE_VEL_XM, 1, 1.0, 0, 0)])
+    bad.append((d, -1))
+    d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (8, 8))
+    lb.set_classes(d, [(0, 1, 0, 0, 0), (lb.ZOUHE_RHO_XP, 0.0, 0, 0, 0)])
     bad.append((d, -1))
     d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F32, (8, 8), arithmetic=7)
     bad.append((d, -1))

@@ -191,6 +191,25 @@ def test_shanchen_periodic(arith):
     check_fp32(d, m, F0, 500, arith, fields=False)
 
 
+@pytest.mark.parametrize("arith", [ABS, DEV])
+def test_zouhe_channel(arith):
+    """A channel with a cylinder, a Zou-He velocity inlet and a Zou-He pressure outlet (Zou & He
+    1997; an extension beyond the reference): the FP64 engine against the FP64 oracle, the FP32 engine
+    against the oracle (see check_fp32), over 600 steps; the inlet keeps its velocity and the outlet
+    its density."""
+    d, m, F0 = channel2d(256, 64, 0.05, 100.0, 60, 32, 8, config_mode=2, seed=7, noise=1e-3)
+    F64, r64, u64 = run_engine(d, m, F0, 600, storage=lb.F64, arithmetic=DEV)
+    Fo, ro, uo = run_oracle(d, m, F0, 600)
+    assert rel_l2(F64, Fo) < 1e-12
+    assert rel_l2(u64, uo) < 1e-11
+    n, nx, ny = d.cells, 256, 64
+    inlet = [x + nx * y for y in range(1, ny - 1) for x in (0,)]
+    outlet = [nx - 1 + nx * y for y in range(1, ny - 1)]
+    assert np.max(np.abs(u64[inlet] - 0.05)) < 1e-13 and np.max(np.abs(u64[n:][inlet])) < 1e-13
+    assert np.max(np.abs(r64[outlet] - 1.0)) < 1e-13
+    check_fp32(d, m, F0, 600, arith)
+
+
 @pytest.mark.parametrize("kind", [lb.KERNEL_PLAIN, lb.KERNEL_ROWS])
 def test_shanchen_config_size(kind):
     """The Shan-Chen configuration at its own size (1024^2, G = -5.5, rho 0.693 + 0.01 noise, tau 1):

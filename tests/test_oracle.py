@@ -173,3 +173,48 @@ def test_zero_gradient_outlet_copies_upstream_column():
     F0 = O.init_equilibrium(p, u=np.concatenate([np.full(nx * ny, u0), np.zeros(nx * ny)]))
     F, rho, u = O.run(p, F0, 30)
     assert np.max(np.abs(F - F0)) < 1e-14
+
+
+def _zouhe_channel(nx, ny, u_in, omega, steps, dtype=np.float64):
+    d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F64, (nx, ny), omega=omega)
+    m = lb.setup_channel2d(d, u_in, -100.0, -100.0, 0.0, 2)  # Zou-He inlet and outlet, no obstacle
+    p = oracle_problem(d, m)
+    F0 = O.init_equilibrium(p, rho=np.where(m == 1, 0.0, 1.0))
+    F, rho, u = O.run(p, F0, steps, dtype=dtype)
+    return m.reshape(ny, nx), rho.reshape(ny, nx), u[:nx * ny].reshape(ny, nx), u[nx * ny:].reshape(ny, nx)
+
+
+def test_zouhe_channel_develops_poiseuille_flow():
+    """Zou-He velocity inlet (uniform u_in) and pressure outlet (rho = 1) on a walled channel: the inlet
+    cells carry exactly the prescribed velocity and the outlet cells the prescribed density, the volume
+    flux is the same through every column, and the developed profile is the Poiseuille parabola
+    between walls halfway between the solid and the first fluid rows."""
+    nx, ny, u_in = 64, 18, 0.02
+    m, rho, ux, uy = _zouhe_channel(nx, ny, u_in, 1.0 / 0.8, 8000)
+    fluid = slice(1, ny - 1)
+    assert np.max(np.abs(ux[fluid, 0] - u_in)) < 1e-13
+    assert np.max(np.abs(uy[fluid, 0])) < 1e-13
+    assert np.max(np.abs(rho[fluid, nx - 1] - 1.0)) < 1e-13
+    flux = (rho * ux)[fluid, :].sum(axis=0)
+    assert np.max(np.abs(flux / flux[0] - 1.0)) < 2e-3
+    y = np.arange(ny, dtype=np.float64)[fluid]
+    shape = (y - 0.5) * (ny - 1.5 - y)  # walls at y = 0.5 and y = ny - 1.5
+    prof = ux[fluid, 3 * nx // 4]
+    fit = shape * (prof @ shape) / (shape @ shape)
+    assert rel_l2(prof, fit) < 2e-2
+    assert abs(prof.mean() / u_in - 1.0) < 2e-2
+
+
+def test_zouhe_uniform_flow_is_kept():
+    """A uniform flow u_in through an open periodic-in-y channel with a Zou-He inlet (u_in) and outlet
+    (rho = 1) is a fixed point: the rebuilt populations are the equilibrium ones."""
+    nx, ny, u0 = 20, 6, 0.05
+    d = lb.make_desc(lb.D2Q9, lb.BGK, lb.F64, (nx, ny), omega=1.1)
+    lb.set_classes(d, [(0, 1, 0, 0, 0), (lb.ZOUHE_VEL_XM, 1, u0, 0, 0), (lb.ZOUHE_RHO_XP, 1, 0, 0, 0)])
+    m = np.zeros((ny, nx), np.uint8)
+    m[:, 0] = 1
+    m[:, nx - 1] = 2
+    p = oracle_problem(d, m.ravel())
+    F0 = O.init_equilibrium(p, u=np.concatenate([np.full(nx * ny, u0), np.zeros(nx * ny)]))
+    F, rho, u = O.run(p, F0, 30)
+    assert np.max(np.abs(F - F0)) < 1e-14

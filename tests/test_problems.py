@@ -20,7 +20,7 @@ def test_cavity2d_setup_matches_reference(n):
     same_problem(d, m, P.cavity2d(nx, ny, 0.1, P.omega_from_re(0.1, nx, 100.0, 0)))
 
 
-@pytest.mark.parametrize("config_mode", [False, True])
+@pytest.mark.parametrize("config_mode", [0, 1, 2])
 @pytest.mark.parametrize("geom", [(60, 24, 13, 12, 3), (1024, 256, 200, 128, 20), (97, 41, 30.5, 20.25, 7.3)])
 def test_channel2d_setup_matches_reference(geom, config_mode):
     nx, ny, ox, oy, r = geom
