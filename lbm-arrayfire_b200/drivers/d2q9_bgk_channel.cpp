@@ -9,10 +9,11 @@
 // format, MLUPS formula corrected).  Options:
 //   --config      config-mode boundaries: equilibrium inlet and zero-gradient outlet instead of the
 //                 reference's periodic channel with forced end columns
+//   --zouhe       Zou-He velocity inlet and pressure outlet (rho = 1) instead
 //   --csv PATH    "Iterations,MLUPS" every 100 iterations
 //   --dump PATH   final DENSITY, UX, UY as raw float64 [N | N | N], column-major
 //
-//   d2q9_bgk_channel [nx ny iterations] [--re R] [--u U] [--storage f32|f16s|bf16s] [--config]
+//   d2q9_bgk_channel [nx ny iterations] [--re R] [--u U] [--storage f32|f16s|bf16s] [--config|--zouhe]
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -40,6 +41,7 @@ int main(int argc, char** argv) {
         else if (s == "--csv" && a + 1 < argc) csv = argv[++a];
         else if (s == "--dump" && a + 1 < argc) dump = argv[++a];
         else if (s == "--config") config_mode = 1;
+        else if (s == "--zouhe") config_mode = 2;
         else if (s == "--storage" && a + 1 < argc) {
             const std::string v = argv[++a];
             storage = v == "f16s" ? LBM_F16S : v == "bf16s" ? LBM_BF16S : LBM_F32;

@@ -65,7 +65,7 @@ def test_d3q27_mrt_driver_runs_and_reports(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("config_mode", [False, True])
+@pytest.mark.parametrize("config_mode", [0, 1, 2])
 def test_d2q9_channel_driver_matches_oracle(tmp_path, config_mode):
     """cpp/d2q9_bgk_channel_packed.cpp's geometry rules at 140 x 60 (cylinder at (nx/5 + 1, ny/2 + ny/30),
     radius ny/10 + 1, u_max 0.1), 300 iterations through the driver against the FP64 oracle.  Re 60: the
@@ -76,7 +76,7 @@ def test_d2q9_channel_driver_matches_oracle(tmp_path, config_mode):
     build()
     dump = tmp_path / "fields.bin"
     args = [str(BIN / "d2q9_bgk_channel"), "140", "60", "300", "--re", "60", "--dump", str(dump)] + \
-        (["--config"] if config_mode else [])
+        {0: [], 1: ["--config"], 2: ["--zouhe"]}[config_mode]
     out = subprocess.run(args, capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr
     assert "Iterations: 300" in out.stdout
