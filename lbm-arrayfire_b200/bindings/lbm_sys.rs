@@ -50,6 +50,7 @@ pub const LBM_DEVICE: c_int = 1;
 pub const LBM_KERNEL_AUTO: c_int = 0;
 pub const LBM_KERNEL_PLAIN: c_int = 1;
 pub const LBM_KERNEL_ROWS: c_int = 2;
+pub const LBM_KERNEL_CLUSTER: c_int = 3;
 pub const LBM_BATCH_AUTO: c_int = 0;
 pub const LBM_BATCH_TILES: c_int = 1;
 pub const LBM_BATCH_ROWS: c_int = 2;
@@ -63,6 +64,8 @@ pub const LBM_CELL_SET_UY: u32 = 0x08;
 pub const LBM_CELL_SET_UZ: u32 = 0x10;
 pub const LBM_CELL_EQUILIBRIUM: u32 = 0x20;
 pub const LBM_CELL_ZEROGRAD_XP: u32 = 0x40;
+pub const LBM_CELL_ZOUHE_VEL_XM: u32 = 0x80;
+pub const LBM_CELL_ZOUHE_RHO_XP: u32 = 0x100;
 pub const LBM_NOALLOC_MAX_CELLS: i64 = 67108864;
 
 #[repr(C)]

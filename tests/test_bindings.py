@@ -169,3 +169,19 @@ def test_c_program_steps_a_lattice(tmp_path):
     so = O.sums(p, Fo)
     assert abs(m - so[0]) / so[0] < 1e-6
     assert np.allclose([jx, jy], so[1:3], rtol=1e-4, atol=1e-6)
+
+
+def test_rust_constants_match_the_header():
+    """Every cell-class flag (#define LBM_CELL_*) and kernel family (enum lbm_kernel) of the header has
+    a Rust constant of the same value."""
+    import re
+
+    h = HEADER.read_text()
+    r = RUST.read_text()
+    want = {k: int(v, 0) for k, v in re.findall(r"#define (LBM_CELL_\w+)\s+(0x[0-9a-fA-F]+)u", h)}
+    enum = re.search(r"enum lbm_kernel \{([^}]*)\}", h).group(1)
+    want.update({k: int(v) for k, v in re.findall(r"(LBM_KERNEL_\w+)\s*=\s*(\d+)", enum)})
+    have = {k: int(v, 0) for k, v in re.findall(r"pub const (LBM_(?:CELL|KERNEL)_\w+): \w+ = (0x[0-9a-fA-F]+|\d+);", r)}
+    assert len(want) >= 12
+    for k, v in want.items():
+        assert have.get(k) == v, (k, v, have.get(k))
