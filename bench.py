@@ -860,8 +860,11 @@ def run_ours(args, rank, world, local_rank):
 
     d, lat, el, clocks = measure(torch, lb, args, head_storage, dev, world, sample_clocks=(rank == 0))
     N = d.cells
-    # Shan-Chen: two launches per step, one with the one-pass kernel (the single-pass family)
+    # Shan-Chen: two launches per step, one with the one-pass kernel (the single-pass family); the
+    # cluster-resident family: one launch per 4096 steps
     launches_per_step = 2 if d.collision == 2 and lat.kernel() != lb.KERNEL_ROWS else 1
+    if lat.kernel() == lb.KERNEL_CLUSTER:
+        launches_per_step = -(-args.steps // 4096) / args.steps
     bytes_cell = algorithmic_bytes_per_cell(d)
     value = world * N * args.steps / el / 1e6
     avg_launch_s = el / (args.steps * launches_per_step)
@@ -880,16 +883,19 @@ def run_ours(args, rank, world, local_rank):
                    "lattice": list(d.shape), "cells": N, "storage": STORAGE_NAMES[head_storage],
                    "bytes_per_cell_update": bytes_cell,
                    "l2": f"inputs larger than L2: {N * d.q * storage_bytes(head_storage) / 1e9:.2f} GB per population buffer"
-                   if N * d.q * storage_bytes(head_storage) > 126e6 else "lattice is L2-resident (no flush)",
+                   if N * d.q * storage_bytes(head_storage) > 126e6 else
+                   ("lattice resident in one thread-block cluster's shared memory for up to 4096 steps per launch"
+                    if kernel_family == "cluster" else "lattice is L2-resident (no flush)"),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "kernel_family": kernel_family, "block": block_used},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_kind == "measured" else "fallback 6.65 TB/s",
                      "kernel": ("k_step_sc_window" if d.collision == 2 else "k_step_rows") if kernel_family == "rows"
+                     else "k_step_cluster" if kernel_family == "cluster"
                      else {0: "k_step_bgk", 1: "k_step_mrt", 2: "k_step_sc + k_sc_psi"}[d.collision],
                      "bytes_per_launch": bytes_cell * N / launches_per_step},
-        "gpu_launches": args.steps * launches_per_step,
+        "gpu_launches": round(args.steps * launches_per_step),
         "clocks": clocks,
     }
     # FP32 plain beside the 16-bit headline
