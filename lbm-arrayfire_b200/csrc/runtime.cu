@@ -513,6 +513,16 @@ static size_t cluster_smem(const lbm_ctx* c, int rows) {
     return (size_t)2 * c->q * rows * c->d.nx * c->sbytes + (size_t)rows * c->d.nx;
 }
 
+// The cluster kernel's dynamic shared-memory bound: the device's opt-in maximum per block.
+static int cluster_smem_bound(const lbm_ctx* c) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->d.device) != cudaSuccess) {
+        cudaGetLastError();
+        v = 200 * 1024;
+    }
+    return v;
+}
+
 template <class F>
 static void dispatch_cluster(const lbm_ctx* c, F&& f) {
     switch (c->d.storage) {
@@ -534,7 +544,8 @@ static bool cluster_eligible(lbm_ctx* c) {
             const int rows = (int)((d.ny + ctas - 1) / ctas);
             const size_t smem = cluster_smem(c, rows);
             if (smem > 200 * 1024) continue;
-            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cluster_smem_bound(c)) !=
+                    cudaSuccess ||
                 (ctas > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
                 cudaGetLastError();
                 continue;
@@ -582,9 +593,10 @@ static void launch_cluster(lbm_ctx* c, int from, cudaStream_t s, int k, bool wri
         attr[0].val.clusterDim.x = (unsigned)c->cl_ctas;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
-        // the attribute is per kernel, not per context: set it for this lattice before every launch
-        cudaFuncSetAttribute(k_step_cluster<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)cluster_smem(c, c->cl_rows));
+        // the attribute is per kernel, not per context: every context sets the same bound (the
+        // device's opt-in maximum), so contexts of different sizes, on any host thread, never lower it
+        // below another's launch
+        cudaFuncSetAttribute(k_step_cluster<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, cluster_smem_bound(c));
         cfg.gridDim = dim3((unsigned)c->cl_ctas);
         cfg.blockDim = dim3(kClusterThreads);
         cfg.dynamicSmemBytes = cluster_smem(c, c->cl_rows);
