@@ -14,8 +14,15 @@ of its plane n up and the c = -1 populations of its plane 1 down, as stored word
 bit-identical to the undivided lattice.  Ghost cells take a bounce-back solid class: their own updates
 are never read, and bounce-back keeps them finite.  The exchange is point-to-point
 (`torch.distributed` isend/irecv; NCCL over NVLink on GPUs, gloo on CPUs) on the slab's stream,
-and it is the only data-path communication.  Shan-Chen is not decomposed (its force needs psi of the
-neighbour planes as a second exchange per step).
+and it is the only data-path communication.
+
+Shan-Chen slabs carry two ghost planes per side.  The force at a cell needs psi = 1 - exp(-rho) of its
+neighbours, and psi of a cell needs that cell's streamed density, so the update of the first interior
+plane reads populations two planes below it: the adjacent ghost plane's c = 0 and c = +1 populations
+(its streamed density, and what streams into the interior) and the far ghost plane's c = +1 ones (6 + 3
+of the 9 per cell and side).  The ghost planes keep the global lattice's own cell classes there, since
+psi of a boundary class depends on it.  The update stays one kernel launch per step with one exchange
+after it; the ghost planes' own updates are never read.
 
 On a GPU the exchange overlaps the interior update (`lbm_step_planes`).  Within a step the slab's
 stream updates planes 2 .. n-1 in all but a few SMs, while a second (high-priority) CUDA stream, in
@@ -36,10 +43,10 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import (BGK, BOUNCE, D3Q27, MAX_CLASSES, MRT, SET_RHO, SET_UX, SET_UY, SET_UZ, STORAGE_BYTES, Desc,
-               Lattice, classes_of, set_classes, velocities)
+from . import (BGK, BOUNCE, D3Q27, MAX_CLASSES, MRT, SET_RHO, SET_UX, SET_UY, SET_UZ, SHANCHEN, STORAGE_BYTES,
+               Desc, Lattice, classes_of, set_classes, velocities)
 
-__all__ = ["split_planes", "axis_dirs", "local_problem", "scatter_populations", "Slab", "SlabSet"]
+__all__ = ["split_planes", "axis_dirs", "halo_plan", "local_problem", "scatter_populations", "Slab", "SlabSet"]
 
 def split_planes(n: int, world: int):
     """[(p0, p1)] per rank: n planes in `world` contiguous runs whose sizes differ by at most one."""
@@ -65,40 +72,65 @@ def _planes(d: Desc) -> int:
     return d.nz if d.dim == 3 else d.ny
 
 
-def local_problem(desc: Desc, mask, p0: int, p1: int):
-    """Descriptor and class mask of the slab [p0, p1) with its two ghost planes.
+def halo_plan(desc: Desc):
+    """(h, up, down): ghost planes per side, and the face transfers of one exchange.
 
-    The ghost class is appended to the descriptor's classes: full-way bounce-back with rho and u set
-    to zero, as the reference's solid cells."""
-    if desc.collision not in (BGK, MRT):
-        raise ValueError("slab decomposition covers BGK and MRT (Shan-Chen needs a psi exchange)")
-    if desc.n_classes >= MAX_CLASSES:
-        raise ValueError("no class index left for the ghost planes")
+    A slab of n planes holds local planes 0 .. n + 2h - 1: h ghost planes, its n own planes (h .. h+n-1),
+    h ghost planes.  up = [(k, dirs)]: a rank sends the populations `dirs` of its plane h + n - 1 - k to
+    its upper neighbour, which stores them in its ghost plane h - 1 - k; down = [(k, dirs)]: a rank
+    sends `dirs` of its plane h + k to its lower neighbour, into that one's ghost plane h + n' + k.
+    BGK and MRT: one plane, the c = +1 (c = -1) populations.  Shan-Chen: two planes, the adjacent one
+    with the c = 0 populations as well (psi of a ghost cell needs its streamed density)."""
+    up_dirs, down_dirs = axis_dirs(desc.lattice)
+    if desc.collision in (BGK, MRT):
+        return 1, [(0, up_dirs)], [(0, down_dirs)]
+    if desc.collision == SHANCHEN:
+        c = np.asarray(velocities(desc.lattice)[2 if desc.dim == 3 else 1])
+        zero = [int(i) for i in np.flatnonzero(c == 0)]
+        return 2, [(0, up_dirs + zero), (1, up_dirs)], [(0, down_dirs + zero), (1, down_dirs)]
+    raise ValueError("unknown collision model")
+
+
+def local_problem(desc: Desc, mask, p0: int, p1: int):
+    """Descriptor and class mask of the slab [p0, p1) with its ghost planes (halo_plan).
+
+    BGK / MRT: one ghost plane per side, of a class appended to the descriptor's classes: full-way
+    bounce-back with rho and u set to zero, as the reference's solid cells (its updates are never read;
+    bounce-back keeps them finite).  Shan-Chen: two ghost planes per side with the global lattice's
+    classes of those planes (periodic), since the interior reads psi of the adjacent ghost plane."""
+    h = halo_plan(desc)[0]
     n = p1 - p0
+    P = _planes(desc)
+    if n < h:
+        raise ValueError(f"a slab of {n} plane(s) cannot feed its neighbours' {h} ghost planes")
     d = Desc.from_buffer_copy(desc)
     if d.dim == 3:
-        d.nz = n + 2
+        d.nz = n + 2 * h
     else:
-        d.ny = n + 2
+        d.ny = n + 2 * h
+    d.mask = None
+    cells = desc.cells // P
+    g = None if mask is None else np.asarray(mask, dtype=np.uint8).ravel(order="F").reshape(P, cells)
+    if desc.collision == SHANCHEN:
+        if g is None:
+            return d, None
+        return d, np.ascontiguousarray(g[np.arange(p0 - h, p1 + h) % P]).ravel()
+    if desc.n_classes >= MAX_CLASSES:
+        raise ValueError("no class index left for the ghost planes")
     ghost = d.n_classes
     classes = classes_of(desc) + [(BOUNCE | SET_RHO | SET_UX | SET_UY | SET_UZ, 0.0, 0.0, 0.0, 0.0)]
     set_classes(d, classes)
-    cells = desc.cells // _planes(desc)
     m = np.full((n + 2, cells), ghost, dtype=np.uint8)
-    if mask is not None:
-        g = np.asarray(mask, dtype=np.uint8).ravel(order="F").reshape(_planes(desc), cells)
-        m[1:n + 1] = g[p0:p1]
-    else:
-        m[1:n + 1] = 0
-    d.mask = None
+    m[1:n + 1] = 0 if g is None else g[p0:p1]
     return d, m.ravel()
 
 
 def scatter_populations(desc: Desc, F, p0: int, p1: int) -> np.ndarray:
     """The slab's part of global populations F (flat [x, y(, z), i]), ghost planes included."""
     P = _planes(desc)
+    h = halo_plan(desc)[0]
     G = np.asarray(F).reshape(desc.q, P, desc.cells // P)
-    idx = np.arange(p0 - 1, p1 + 1) % P
+    idx = np.arange(p0 - h, p1 + h) % P
     return np.ascontiguousarray(G[:, idx, :]).ravel()
 
 
@@ -120,9 +152,13 @@ def _plane_views(lat, planes: int, device) -> dict:
     return {ptr: _device_bytes(ptr, nbytes, device).view(lat.q, planes, -1) for ptr in (cur, nxt)}
 
 
-def _interior(lat, n: int, dtype=np.float64) -> np.ndarray:
+def _interior(lat, n: int, h: int = 1, dtype=np.float64) -> np.ndarray:
     F = lat.get_populations(dtype)
-    return F.reshape(lat.q, n + 2, -1)[:, 1:n + 1, :]
+    return F.reshape(lat.q, n + 2 * h, -1)[:, h:n + h, :]
+
+
+def _words(plan_side) -> int:
+    return sum(len(dirs) for _, dirs in plan_side)
 
 
 class Slab:
@@ -146,11 +182,12 @@ class Slab:
         self.p0, self.p1 = split_planes(_planes(desc), world)[rank]
         self.n = self.p1 - self.p0
         self.desc, self.mask = local_problem(desc, mask, self.p0, self.p1)
+        self.h, up_plan, down_plan = halo_plan(desc)
         self.lat = (lattice_factory or Lattice)(self.desc, self.mask)
         if hasattr(self.lat, "set_cell_offset"):
-            # local plane 0 is global plane p0 - 1: the slab's cells hash (stochastic rounding) like the
+            # local plane 0 is global plane p0 - h: the slab's cells hash (stochastic rounding) like the
             # undivided lattice's
-            self.lat.set_cell_offset((self.p0 - 1) * (desc.cells // _planes(desc)))
+            self.lat.set_cell_offset((self.p0 - self.h) * (desc.cells // _planes(desc)))
         self.up_dirs, self.down_dirs = axis_dirs(desc.lattice)
         self.device = torch.device(device) if device is not None else torch.device("cpu")
         # a stream of the slab's own orders the steps, the face copies and the NCCL transfers (torch's
@@ -159,16 +196,21 @@ class Slab:
         self.stream = torch.cuda.Stream(device=self.device) if self.device.type == "cuda" else None
         if self.stream is not None:
             self.lat.set_stream(self.stream.cuda_stream)
-        # faces travel as raw bytes of the stored words (NCCL has no 16-bit integer type; a
-        # point-to-point transfer never touches the values); an injected stepper uses FP64 words
-        k = len(self.up_dirs) * self.lat.face_cells()
-        word, k = (torch.uint8, k * STORAGE_BYTES[self.desc.storage]) if lattice_factory is None else (torch.float64, k)
+        # faces of engine lattices travel as raw bytes of the stored words (NCCL has no 16-bit integer
+        # type; a point-to-point transfer never touches the values); other steppers (the oracle) use
+        # FP64 words
+        word, unit = (torch.uint8, STORAGE_BYTES[self.desc.storage]) if isinstance(self.lat, Lattice) \
+            else (torch.float64, 1)
+        cells = self.lat.face_cells()
+        self._up_seg, self._down_seg = _segments(up_plan, cells, unit), _segments(down_plan, cells, unit)
+        k = _words(up_plan) * cells * unit
         self._buf = {name: torch.empty(k, dtype=word, device=self.device)
                      for name in ("send_up", "send_down", "recv_down", "recv_up")}
         self.lat.set_populations(scatter_populations(desc, F0, self.p0, self.p1))
-        # the overlapped step (see the module docstring): GPU steppers with plane ranges, >= 3 planes
+        # the overlapped step (see the module docstring): GPU steppers with plane ranges, >= 3 planes,
+        # one ghost plane per side (not Shan-Chen)
         self.overlap = (overlap and self.device.type == "cuda" and hasattr(self.lat, "step_planes")
-                        and self.n >= 3)
+                        and self.n >= 3 and self.h == 1)
         if self.overlap:
             # the exchange stream runs first wherever SMs free up; the row pipeline leaves it some
             self._comm = torch.cuda.Stream(device=self.device, priority=-1)
@@ -179,12 +221,10 @@ class Slab:
             self._ready, self._done = torch.cuda.Event(), torch.cuda.Event()
 
     def _pack(self):
-        self.lat.face_get(self.n, self.up_dirs, self._buf["send_up"])
-        self.lat.face_get(1, self.down_dirs, self._buf["send_down"])
+        _pack(self.lat, self.n, self.h, self._up_seg, self._down_seg, self._buf["send_up"], self._buf["send_down"])
 
     def _unpack(self, from_down, from_up):
-        self.lat.face_set(0, self.up_dirs, from_down)
-        self.lat.face_set(self.n + 1, self.down_dirs, from_up)
+        _unpack(self.lat, self.n, self.h, self._up_seg, self._down_seg, from_down, from_up)
 
     def exchange(self):
         """Fill both ghost planes from the neighbours' boundary planes (the same steps on every rank)."""
@@ -253,7 +293,7 @@ class Slab:
 
     def interior_populations(self, dtype=np.float64) -> np.ndarray:
         """This rank's planes, [Q, n, plane cells]."""
-        return _interior(self.lat, self.n, dtype)
+        return _interior(self.lat, self.n, self.h, dtype)
 
     def gather_populations(self, dtype=np.float64):
         """Global populations (flat [x, y(, z), i]) on every rank (all_gather_object: for checks)."""
@@ -278,6 +318,34 @@ class Slab:
         return local.cpu().numpy()
 
 
+def _segments(plan_side, cells: int, unit: int):
+    """[(k, dirs, start, stop)]: where each transfer of one side (halo_plan) sits in its send buffer,
+    in buffer elements (`unit` elements per stored word)."""
+    out, at = [], 0
+    for k, dirs in plan_side:
+        size = len(dirs) * cells * unit
+        out.append((k, dirs, at, at + size))
+        at += size
+    return out
+
+
+def _pack(lat, n, h, up_seg, down_seg, send_up, send_down):
+    """The faces a slab of n planes sends up (from its top planes) and down (from its bottom planes)."""
+    for k, dirs, a, b in up_seg:
+        lat.face_get(h + n - 1 - k, dirs, send_up[a:b])
+    for k, dirs, a, b in down_seg:
+        lat.face_get(h + k, dirs, send_down[a:b])
+
+
+def _unpack(lat, n, h, up_seg, down_seg, from_down, from_up):
+    """Store what the lower neighbour sent up in the lower ghost planes and what the upper one sent
+    down in the upper ghost planes."""
+    for k, dirs, a, b in up_seg:
+        lat.face_set(h - 1 - k, dirs, from_down[a:b])
+    for k, dirs, a, b in down_seg:
+        lat.face_set(h + n + k, dirs, from_up[a:b])
+
+
 def _sums(lattice: int, Fi: np.ndarray) -> np.ndarray:
     cx, cy, cz, _, _ = velocities(lattice)
     per_dir = Fi.reshape(Fi.shape[0], -1).sum(axis=1)
@@ -296,22 +364,25 @@ class SlabSet:
         self.global_desc = desc
         self.ranges = split_planes(_planes(desc), parts)
         self.up_dirs, self.down_dirs = axis_dirs(desc.lattice)
+        self.h, up_plan, down_plan = halo_plan(desc)
         self.lats, self.ns = [], []
         for p0, p1 in self.ranges:
             d, m = local_problem(desc, mask, p0, p1)
             lat = (lattice_factory or Lattice)(d, m)
             if hasattr(lat, "set_cell_offset"):
-                lat.set_cell_offset((p0 - 1) * (desc.cells // _planes(desc)))
+                lat.set_cell_offset((p0 - self.h) * (desc.cells // _planes(desc)))
             lat.set_populations(scatter_populations(desc, F0, p0, p1))
             self.lats.append(lat)
             self.ns.append(p1 - p0)
-        k = len(self.up_dirs) * self.lats[0].face_cells()
+        cells = self.lats[0].face_cells()
+        self._up_seg, self._down_seg = _segments(up_plan, cells, 1), _segments(down_plan, cells, 1)
+        k = _words(up_plan) * cells
         word = {4: np.float32, 8: np.float64, 2: np.uint16}[STORAGE_BYTES[desc.storage]] \
-            if lattice_factory is None else np.float64
+            if isinstance(self.lats[0], Lattice) else np.float64
         self._up = [np.empty(k, dtype=word) for _ in self.lats]
         self._down = [np.empty(k, dtype=word) for _ in self.lats]
         # overlapped steps: every lattice on one stream of the set's own, the face copies on a second
-        self.overlap = overlap and lattice_factory is None and min(self.ns) >= 3
+        self.overlap = overlap and lattice_factory is None and min(self.ns) >= 3 and self.h == 1
         if self.overlap:
             import torch
 
@@ -329,11 +400,10 @@ class SlabSet:
     def exchange(self):
         R = len(self.lats)
         for r, lat in enumerate(self.lats):
-            lat.face_get(self.ns[r], self.up_dirs, self._up[r])
-            lat.face_get(1, self.down_dirs, self._down[r])
+            _pack(lat, self.ns[r], self.h, self._up_seg, self._down_seg, self._up[r], self._down[r])
         for r, lat in enumerate(self.lats):
-            lat.face_set(0, self.up_dirs, self._up[(r - 1) % R])
-            lat.face_set(self.ns[r] + 1, self.down_dirs, self._down[(r + 1) % R])
+            _unpack(lat, self.ns[r], self.h, self._up_seg, self._down_seg, self._up[(r - 1) % R],
+                    self._down[(r + 1) % R])
 
     def step(self, n: int = 1):
         for _ in range(n):
@@ -367,10 +437,11 @@ class SlabSet:
         main.wait_event(self._done)
 
     def gather_populations(self, dtype=np.float64) -> np.ndarray:
-        return np.concatenate([_interior(lat, n, dtype) for lat, n in zip(self.lats, self.ns)], axis=1).ravel()
+        return np.concatenate([_interior(lat, n, self.h, dtype) for lat, n in zip(self.lats, self.ns)],
+                              axis=1).ravel()
 
     def sums(self) -> np.ndarray:
-        return sum(_sums(self.global_desc.lattice, _interior(lat, n)) for lat, n in zip(self.lats, self.ns))
+        return sum(_sums(self.global_desc.lattice, _interior(lat, n, self.h)) for lat, n in zip(self.lats, self.ns))
 
     def close(self):
         for lat in self.lats:

@@ -14,9 +14,9 @@ import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
-from helpers import O, channel2d, lb, oracle_problem
+from helpers import O, P, channel2d, lb, oracle_problem
 
-from lbm_b200.slab import Slab, SlabSet, axis_dirs, local_problem, scatter_populations, split_planes
+from lbm_b200.slab import Slab, SlabSet, axis_dirs, halo_plan, local_problem, scatter_populations, split_planes
 
 
 class OracleStepper:
@@ -76,7 +76,29 @@ def periodic3d(storage=lb.F64, n=(8, 6, 7)):
     return d, None, np.repeat(w, d.cells) * (1.0 + 0.02 * rng.standard_normal(27 * d.cells))
 
 
-CASES = {"mrt_cavity3d": mrt_cavity3d, "channel2d": channel, "periodic3d": periodic3d}
+def shanchen2d(storage=lb.F64, nx=24, ny=20, G=-5.5):
+    """Periodic single-component Shan-Chen in its phase-separating regime (seeded density noise)."""
+    d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, storage, (nx, ny), omega=1.0, sc_G=G)
+    F0 = P.shanchen_start_state(P.shanchen(nx, ny, G), 0.693, 0.01, 5)
+    return d, None, F0
+
+
+def shanchen_walls(storage=lb.F64, nx=20, ny=17):
+    """Shan-Chen between two walls (rows y = 0 and y = ny - 1: bounce-back with a prescribed wall
+    density, which sets the walls' psi) and a row of forced density in the bulk: the slabs' ghost
+    rows must carry those classes."""
+    d, _, F0 = shanchen2d(storage, nx, ny)
+    lb.set_classes(d, [(0, 0.0, 0.0, 0.0, 0.0),
+                       (lb.BOUNCE | lb.SET_RHO | lb.SET_UX | lb.SET_UY, 0.4, 0.0, 0.0, 0.0),
+                       (lb.SET_RHO, 0.9, 0.0, 0.0, 0.0)])
+    m = np.zeros((nx, ny), dtype=np.uint8, order="F")
+    m[:, 0] = m[:, ny - 1] = 1
+    m[3:9, 7] = 2
+    return d, m.ravel(order="F"), F0
+
+
+CASES = {"mrt_cavity3d": mrt_cavity3d, "channel2d": channel, "periodic3d": periodic3d,
+         "shanchen2d": shanchen2d, "shanchen_walls": shanchen_walls}
 
 
 def test_split_planes_and_axis_dirs():
@@ -94,7 +116,7 @@ def test_split_planes_and_axis_dirs():
         assert sorted(int(opp[i]) for i in up) == down
 
 
-def test_local_problem_ghost_planes_and_rejects_shanchen():
+def test_local_problem_ghost_planes():
     d, m, F0 = mrt_cavity3d()
     ld, lm = local_problem(d, m, 3, 7)
     assert (ld.nx, ld.ny, ld.nz) == (12, 8, 6) and ld.n_classes == d.n_classes + 1
@@ -104,9 +126,30 @@ def test_local_problem_ghost_planes_and_rejects_shanchen():
     Fl = scatter_populations(d, F0, 0, 2).reshape(27, 4, -1)
     Fg = F0.reshape(27, 9, -1)
     assert np.array_equal(Fl[:, 0], Fg[:, 8]) and np.array_equal(Fl[:, 1:3], Fg[:, 0:2])
-    sc = lb.make_desc(lb.D2Q9, lb.SHANCHEN, lb.F32, (16, 16), omega=1.0, sc_G=-5.0)
+
+
+def test_shanchen_halo_two_planes_with_the_global_classes():
+    """Shan-Chen slabs: two ghost rows per side holding the global rows' classes (periodic), the
+    adjacent ghost row fed with the c = 0 and c = +1 (c = -1) populations and the far one with the
+    c = +1 (c = -1) ones; a slab must hold at least two rows."""
+    d, m, F0 = shanchen_walls()
+    h, up, down = halo_plan(d)
+    cy = lb.velocities(lb.D2Q9)[1]
+    assert h == 2 and [k for k, _ in up] == [0, 1] and [k for k, _ in down] == [0, 1]
+    assert sorted(cy[up[0][1]]) == [0, 0, 0, 1, 1, 1] and sorted(cy[up[1][1]]) == [1, 1, 1]
+    assert sorted(cy[down[0][1]]) == [-1, -1, -1, 0, 0, 0] and sorted(cy[down[1][1]]) == [-1, -1, -1]
+    ld, lm = local_problem(d, m, 0, 5)
+    assert (ld.nx, ld.ny) == (20, 9) and ld.n_classes == d.n_classes
+    rows = np.asarray(m).reshape(17, 20)
+    assert np.array_equal(lm.reshape(9, 20), rows[[15, 16, 0, 1, 2, 3, 4, 5, 6]])
+    Fl = scatter_populations(d, F0, 0, 5).reshape(9, 9, -1)
+    Fg = F0.reshape(9, 17, -1)
+    assert np.array_equal(Fl[:, :2], Fg[:, 15:17]) and np.array_equal(Fl[:, 2:9], Fg[:, 0:7])
+    assert local_problem(*shanchen2d()[:2], 2, 9)[1] is None  # no mask: none for the slab either
     with pytest.raises(ValueError):
-        local_problem(sc, None, 0, 8)
+        local_problem(d, m, 4, 5)
+    with pytest.raises(ValueError):
+        SlabSet(d, m, F0, 9, lattice_factory=OracleStepper)  # 17 rows over 9 slabs: one has a single row
 
 
 def test_face_calls_validate_buffers_and_context():
@@ -165,7 +208,7 @@ def _gloo_body(rank, world, port, case, out_dir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("case,world", [("mrt_cavity3d", 2), ("channel2d", 3)])
+@pytest.mark.parametrize("case,world", [("mrt_cavity3d", 2), ("channel2d", 3), ("shanchen_walls", 3)])
 def test_slab_gloo_ranks_equal_undivided_oracle(tmp_path, case, world):
     mp.start_processes(_gloo_body, args=(world, _free_port(), case, str(tmp_path)), nprocs=world, join=True,
                        start_method="spawn")
@@ -201,6 +244,63 @@ def test_slabset_of_engine_lattices_equals_one_lattice(storage, case, parts, ove
     finally:
         s.close()
     assert np.isfinite(got).all() and np.array_equal(got, ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [lb.F32, lb.BF16S, lb.F64])
+@pytest.mark.parametrize("case", ["shanchen2d", "shanchen_walls", "shanchen_wide"])
+@pytest.mark.parametrize("parts", [2, 3])
+@pytest.mark.parametrize("kernel", [lb.KERNEL_AUTO, lb.KERNEL_PLAIN])
+def test_shanchen_slabs_on_the_gpu_equal_one_lattice(storage, case, parts, kernel):
+    """Shan-Chen slabs on the engine (one-pass window kernel or the two-pass kernels, stochastic
+    rounding for BF16S hashed by global cell) with two ghost rows per side: bit-identical to one
+    lattice of the full size after 40 steps of phase separation."""
+    if case == "shanchen_wide":  # rows wider than one window strip, a ragged last strip
+        d, m, F0 = shanchen2d(storage, nx=300, ny=26)
+    else:
+        d, m, F0 = CASES[case](storage)
+
+    def engine(dd, mm):
+        lat = lb.Lattice(dd, mm)
+        lat.set_kernel(kernel)
+        return lat
+
+    dtype = np.float64 if storage == lb.F64 else np.float32
+    with engine(d, m) as lat:
+        lat.set_populations(np.asarray(F0, dtype=np.float64))
+        lat.step(40)
+        ref = lat.get_populations(dtype)
+        ref_sums = lat.sums()
+    s = SlabSet(d, m, F0, parts, lattice_factory=engine)
+    try:
+        s.step(40)
+        got = s.gather_populations(dtype)
+        sums = s.sums()
+    finally:
+        s.close()
+    assert np.isfinite(got).all() and np.array_equal(got, ref)
+    assert np.allclose(sums, ref_sums, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [lb.F32, lb.BF16S])
+def test_one_rank_shanchen_slab_on_the_gpu_equals_one_lattice(storage):
+    """The rank-side Slab for Shan-Chen: device byte buffers holding both ghost rows' transfers per
+    side, filled from the rank's own far rows (periodic wrap), equal to the undivided lattice."""
+    import torch
+
+    d, m, F0 = shanchen_walls(storage, nx=96, ny=30)
+    with lb.Lattice(d, m) as lat:
+        lat.set_populations(np.asarray(F0, dtype=np.float64))
+        lat.step(25)
+        ref = lat.get_populations(np.float32)
+    slab = Slab(d, m, F0, 0, 1, device="cuda:0")
+    assert not slab.overlap and slab.h == 2
+    assert slab._buf["send_up"].numel() == 9 * 96 * lb.STORAGE_BYTES[storage]
+    slab.step(25)
+    torch.cuda.synchronize()
+    assert np.array_equal(slab.gather_populations(np.float32), ref)
+    slab.close()
 
 
 def _plane_case(name, storage):
