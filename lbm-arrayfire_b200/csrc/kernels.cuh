@@ -381,6 +381,28 @@ __device__ __forceinline__ void store_cell(S* __restrict__ fout, const P& p, lon
     }
 }
 
+// store_cell with 32-bit population indices i N + c, for lattices whose Q N populations all have
+// 32-bit indices: one 32-bit add and one widening multiply-add per address instead of 64-bit index
+// arithmetic.  The same values, rounding bits and order as store_cell.
+template <class L, class S, bool ABS, class P, class R>
+__device__ __forceinline__ void store_cell32(S* __restrict__ fout, const P& p, uint32_t c, const R (&out)[L::Q],
+                                             const Rounding& rnd) {
+    const uint32_t N = (uint32_t)p.N;
+    if constexpr (!ABS && Codec<S>::kScaled) {
+        encode16<L, S>(out, rnd, c + p.cell_base,
+                       [&](auto I, S v) { fout[(uint32_t)decltype(I)::value * N + c] = v; });
+    } else {
+        static_for<L::Q>([&](auto I) {
+            constexpr int i = I;
+            const uint32_t idx = (uint32_t)i * N + c;
+            if constexpr (ABS)
+                Codec<S>::store(fout + idx, out[i], R(L::w(i)), R(p.scale));
+            else
+                fout[idx] = Codec<S>::enc(out[i], R(L::w(i)));
+        });
+    }
+}
+
 // Storage scale and its inverse for raw deviations: the codec's scale for the 16-bit codecs,
 // compile-time 1 otherwise.
 template <class S, class P, class R>
@@ -773,6 +795,54 @@ __device__ __forceinline__ R sc_psi_of(const StepParams<R>& p, const S* __restri
     return sc_psi_from<S, ABS>(p, v, cls, fl);
 }
 
+// Row offsets (y + dy) nx of the rows y - 1, y, y + 1 (periodic) as 32-bit cell indices, for the window
+// kernel on lattices whose 9 N populations all have 32-bit indices.
+struct WinRows {
+    uint32_t base[3];  // [dy + 1]
+    __device__ __forceinline__ WinRows(int y, int nx, int ny) {
+        base[0] = (uint32_t)(y == 0 ? ny - 1 : y - 1) * (uint32_t)nx;
+        base[1] = (uint32_t)y * (uint32_t)nx;
+        base[2] = (uint32_t)(y == ny - 1 ? 0 : y + 1) * (uint32_t)nx;
+    }
+    // source row of direction cy: pull from y - cy
+    __device__ __forceinline__ uint32_t src(int cy) const { return base[1 - cy]; }
+};
+
+// sc_pull_cell with 32-bit population indices i N + row + x (WinRows): the same loads, values and
+// class as sc_pull_cell, each address one 32-bit add and one widening multiply-add.
+template <class S, bool ABS, class R>
+__device__ __forceinline__ void sc_pull_cell32(const StepParams<R>& p, const S* __restrict__ fin, const WinRows& rows,
+                                               int x, uint32_t c, R (&v)[9], int& cls, uint32_t& fl) {
+    using L = D2Q9;
+    const uint32_t N = (uint32_t)p.N;
+    const int xm = x == 0 ? p.nx - 1 : x - 1;
+    const int xp = x == p.nx - 1 ? 0 : x + 1;
+    static_for<9>([&](auto I) {
+        constexpr int i = I;
+        constexpr int cx = L::cx(i), cy = L::cy(i);
+        const int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
+        const uint32_t idx = (uint32_t)i * N + rows.src(cy) + (uint32_t)xs;
+        if constexpr (ABS)
+            v[i] = Codec<S>::load(fin + idx, R(L::w(i)), R(p.inv_scale));
+        else
+            v[i] = Codec<S>::raw(__ldg(fin + idx), R(L::w(i)));
+    });
+    cls = p.mask ? (int)__ldg(p.mask + c) : 0;
+    fl = p.cls.flags[cls];
+    if (fl & kZeroGradXp) {  // pull_zerograd: c_x = -1 from the cell's own column
+        static_for<9>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (L::cx(i) == -1) {
+                const uint32_t idx = (uint32_t)i * N + rows.src(L::cy(i)) + (uint32_t)x;
+                if constexpr (ABS)
+                    v[i] = Codec<S>::load(fin + idx, R(L::w(i)), R(p.inv_scale));
+                else
+                    v[i] = Codec<S>::raw(__ldg(fin + idx), R(L::w(i)));
+            }
+        });
+    }
+}
+
 template <class S, bool ABS>
 __global__ void __launch_bounds__(512) k_sc_psi(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D2Q9;
@@ -825,8 +895,8 @@ __device__ __forceinline__ void sc_force(const StepParams<R>& p, const Rows<D2Q9
 // The Shan-Chen collision of one cell from its pulled populations v (class cls, flags fl) and the
 // force: moments, class overrides, velocity shift u_eq = u + tau F / rho (Shan & Chen 1993), BGK,
 // bounce-back, store.
-template <class S, bool ABS, class R>
-__device__ __forceinline__ void sc_collide_store(const StepParams<R>& p, long long c, const R (&v)[9], int cls,
+template <class S, bool ABS, class R, class Idx>
+__device__ __forceinline__ void sc_collide_store(const StepParams<R>& p, Idx c, const R (&v)[9], int cls,
                                                  uint32_t fl, R Fx, R Fy, const Rounding& rnd) {
     using L = D2Q9;
     R sc, isc;
@@ -853,7 +923,10 @@ __device__ __forceinline__ void sc_collide_store(const StepParams<R>& p, long lo
             out[L::opp(i)] = v[i];
         });
     }
-    store_cell<L, S, ABS>(static_cast<S*>(p.fout), p, c, out, rnd);
+    if constexpr (std::is_same<Idx, uint32_t>::value)
+        store_cell32<L, S, ABS>(static_cast<S*>(p.fout), p, c, out, rnd);
+    else
+        store_cell<L, S, ABS>(static_cast<S*>(p.fout), p, (long long)c, out, rnd);
 }
 
 // Second pass of the two-pass Shan-Chen step (psi from k_sc_psi in global memory).
@@ -886,7 +959,9 @@ __global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepPar
 // ring of 4 shared rows (two threads add the strip's edge columns, periodic wrap), and after one
 // block barrier takes the force at row y from ring rows y - 1 .. y + 1.  With 4 ring rows one barrier
 // per row suffices: a row's slot is rewritten two barriers after its last read.  psi, force and
-// collision are the two-pass kernels' device functions: bit-identical results.
+// collision are the two-pass kernels' device functions: bit-identical results.  I32: 32-bit
+// population indices (lattices with 9 N <= 2^32), which take about a third of the address arithmetic
+// of 64-bit ones; the same loads and stores.
 #ifndef LBM_SCW_TX
 #define LBM_SCW_TX 128
 #endif
@@ -895,11 +970,12 @@ __global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepPar
 #endif
 constexpr int kScwTX = LBM_SCW_TX;
 
-template <class S, bool ABS>
+template <class S, bool ABS, bool I32>
 __global__ void __launch_bounds__(kScwTX, sizeof(typename Codec<S>::Real) == 8 ? 4 : LBM_SCW_MINB) k_step_sc_window(const __grid_constant__ StepParams<typename Codec<S>::Real> p,
                                                            int rows_per_strip) {
     using L = D2Q9;
     using R = typename Codec<S>::Real;
+    using Idx = typename std::conditional<I32, uint32_t, long long>::type;
     constexpr int TX = kScwTX, PX = TX + 2;
     static_assert(TX >= 2, "two edge threads");
     __shared__ R ring[4][PX];
@@ -918,13 +994,21 @@ __global__ void __launch_bounds__(kScwTX, sizeof(typename Codec<S>::Real) == 8 ?
     const int le = tx == 0 ? 0 : PX - 1;
     auto psi_row = [&](int y, R (&v)[9], int& cls, uint32_t& fl) {
         const int yw = y < 0 ? y + ny : (y >= ny ? y - ny : y);
-        const Rows<L> rows(yw, 0, nx, ny, 1);
-        const long long c = rows.base[1][1] + xs;
-        sc_pull_cell<S, ABS>(p, fin, rows, xs, c, v, cls, fl);
         R w[9];
         int c2 = 0;
         uint32_t f2 = 0;
-        if (tx < 2) sc_pull_cell<S, ABS>(p, fin, rows, xe, rows.base[1][1] + xe, w, c2, f2);
+        Idx c;
+        if constexpr (I32) {
+            const WinRows rows(yw, nx, ny);
+            c = rows.base[1] + (uint32_t)xs;
+            sc_pull_cell32<S, ABS>(p, fin, rows, xs, c, v, cls, fl);
+            if (tx < 2) sc_pull_cell32<S, ABS>(p, fin, rows, xe, rows.base[1] + (uint32_t)xe, w, c2, f2);
+        } else {
+            const Rows<L> rows(yw, 0, nx, ny, 1);
+            c = rows.base[1][1] + xs;
+            sc_pull_cell<S, ABS>(p, fin, rows, xs, c, v, cls, fl);
+            if (tx < 2) sc_pull_cell<S, ABS>(p, fin, rows, xe, rows.base[1][1] + xe, w, c2, f2);
+        }
         const R ps = sc_psi_from<S, ABS>(p, v, cls, fl);
         ring[y & 3][tx + 1] = ps;
         if (own_x && y >= ys && y < ye) p.psi[c] = ps;
@@ -941,7 +1025,7 @@ __global__ void __launch_bounds__(kScwTX, sizeof(typename Codec<S>::Real) == 8 ?
         psi_row(y + 1, vn, cn, fn);  // the next row (the row below the strip on the last pass)
         __syncthreads();
         if (own_x) {
-            const long long c = (long long)y * nx + x;
+            const Idx c = (Idx)y * (Idx)nx + (Idx)x;
             R Fx, Fy;
             sc_force_from(p, [&](int dx, int dy) { return ring[(y + dy) & 3][tx + 1 + dx]; }, Fx, Fy);
             sc_collide_store<S, ABS>(p, c, vc, cc, fc, Fx, Fy, rnd);

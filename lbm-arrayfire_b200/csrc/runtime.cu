@@ -135,6 +135,7 @@ struct lbm_ctx {
     unsigned* tick = nullptr;      // the rounding's step counter pair (step_rounding)
     WaitLimits waits = kProductionWaits;  // the row pipeline's wait limits for the next launch
     bool stall_armed = false;      // lbm_test_stall_next_step: the next step launches with `stall`
+    bool scw_index64 = false;      // lbm_test_sc_window_index64: 64-bit indices in the window kernel
     WaitLimits stall = kProductionWaits;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int gsteps = 0;
@@ -377,15 +378,28 @@ static void dispatch_rows(const lbm_ctx* c, F&& f) {
 #ifndef LBM_SCW_HMAX
 #define LBM_SCW_HMAX 0  // > 0: at most this many rows per strip (several waves of CTAs on large lattices)
 #endif
+#ifndef LBM_SCW_IDX32
+#define LBM_SCW_IDX32 1  // 0: the window kernel always indexes populations in 64 bits (A/B)
+#endif
+// The window kernel indexes populations in 32 bits when all 9 N of them have 32-bit indices.
+static bool sc_window_i32(const lbm_ctx* c) {
+    return LBM_SCW_IDX32 && !c->scw_index64 && 9ULL * (unsigned long long)c->d.nx * (unsigned long long)c->d.ny <= (1ULL << 32);
+}
+// The window kernel instance of a context (storage S; absolute or deviation arithmetic; index width).
+template <class S>
+static auto sc_window_kernel(const lbm_ctx* c) {
+    const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
+    if (sc_window_i32(c)) return abs_arith ? k_step_sc_window<S, true, true> : k_step_sc_window<S, false, true>;
+    return abs_arith ? k_step_sc_window<S, true, false> : k_step_sc_window<S, false, false>;
+}
 static int prepare_rows(lbm_ctx* c) {
     if (c->d.collision == LBM_SHANCHEN) {
         // k_step_sc_window: strips of rows sized so that one wave of CTAs covers the lattice (A/B:
         // capping the strip height at 16/32/64 rows for several waves was slower or equal)
         int per_sm = 0, sms = 0, rc = LBM_OK;
-        const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
         dispatch_storage(c->d.storage, [&](auto tag) {
             using S = typename decltype(tag)::type;
-            auto kern = abs_arith ? k_step_sc_window<S, true> : k_step_sc_window<S, false>;
+            auto kern = sc_window_kernel<S>(c);
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kScwTX, 0) != cudaSuccess)
                 rc = set_error(LBM_ERR_CUDA, "occupancy query failed");
         });
@@ -422,7 +436,6 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
     // asked for (plane sets, graph capture) takes the plain kernel, bit-identical to it
     if (c->kernel_used == LBM_KERNEL_CLUSTER && block <= 0) block = 128;
     if (c->kernel_used == LBM_KERNEL_ROWS && c->d.collision == LBM_SHANCHEN) {
-        const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
         dispatch_storage(c->d.storage, [&](auto tag) {
             using S = typename decltype(tag)::type;
             using R = typename Codec<S>::Real;
@@ -432,10 +445,7 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
             p.parity = from;
             const int h = c->rows_rpg;
             const dim3 wg((unsigned)((c->d.nx + kScwTX - 1) / kScwTX), (unsigned)((c->d.ny + h - 1) / h), 1);
-            if (abs_arith)
-                k_step_sc_window<S, true><<<wg, kScwTX, 0, s>>>(p, h);
-            else
-                k_step_sc_window<S, false><<<wg, kScwTX, 0, s>>>(p, h);
+            sc_window_kernel<S>(c)<<<wg, kScwTX, 0, s>>>(p, h);
         });
         return;
     }
@@ -1312,6 +1322,15 @@ int lbm_test_stall_next_step(lbm_ctx* c, int64_t item, int64_t wait_clocks) {
                          "the stall applies to the row pipeline's bulk-copy stages: pin LBM_KERNEL_ROWS (BGK/MRT) first");
     c->stall = WaitLimits{(unsigned)item, (long long)wait_clocks};
     c->stall_armed = true;
+    return LBM_OK;
+}
+
+int lbm_test_sc_window_index64(lbm_ctx* c, int on) {
+    if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
+    LBM_CK(cudaSetDevice(c->d.device));
+    LBM_CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);  // captured launches name the kernel instance
+    c->scw_index64 = on != 0;
     return LBM_OK;
 }
 

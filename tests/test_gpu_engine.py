@@ -398,18 +398,19 @@ def test_row_pipeline_segmented_wide_rows_equal_plain(storage, case):
     assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.F64])
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.BF16S, lb.F64])
 @pytest.mark.parametrize("arith", [lb.ARITH_ABSOLUTE, lb.ARITH_DEVIATION])
 @pytest.mark.parametrize("shape,solid", [((128, 128), False), ((100, 50), True), ((20, 10), False),
                                          ((48, 36), True), ((200, 24), "zerograd")])
 def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
     """The one-pass Shan-Chen kernel (KERNEL_ROWS: a window sliding down y, psi of the next row in a
-    shared ring) against the two-pass kernels (KERNEL_PLAIN: psi through global memory): bit-identical
-    populations and fields, on full and partial column strips, a lattice narrower than a strip, with
-    solid (bounce-back, set-density) cells, and with zero-gradient outlet columns on both sides of the
-    first strip edge (x = 127 and 128: the window pulls them both as its own cells and as the
-    neighbouring strip's edge column)."""
-    if arith == lb.ARITH_ABSOLUTE and storage == lb.F16S:
+    shared ring), with 32-bit population indices (its choice on these lattices) and with 64-bit ones
+    (the form of lattices beyond 2^32 / 9 cells, forced by a test hook), against the two-pass kernels
+    (KERNEL_PLAIN: psi through global memory): bit-identical populations and fields, on full and
+    partial column strips, a lattice narrower than a strip, with solid (bounce-back, set-density)
+    cells, and with zero-gradient outlet columns on both sides of the first strip edge (x = 127 and
+    128: the window pulls them both as its own cells and as the neighbouring strip's edge column)."""
+    if arith == lb.ARITH_ABSOLUTE and storage in (lb.F16S, lb.BF16S):
         pytest.skip("absolute arithmetic is F32/F64 only")
     d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, storage, shape, omega=1.0, sc_G=-4.5, arithmetic=arith)
     m = None
@@ -426,19 +427,23 @@ def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
     rng = np.random.default_rng(4)
     rho = 0.693 + 0.01 * rng.uniform(-1.0, 1.0, size=n)
     out = {}
-    for kind in (lb.KERNEL_PLAIN, lb.KERNEL_ROWS):
+    for kind, index64 in ((lb.KERNEL_PLAIN, False), (lb.KERNEL_ROWS, False), (lb.KERNEL_ROWS, True)):
         with lb.Lattice(d, m) as lat:
             lat.set_kernel(kind)
+            if index64:
+                lat.test_sc_window_index64(True)
             lat.init_equilibrium(rho=rho)
             lat.step(40)
             lat.sync()
             assert lat.kernel() == kind
             r, u = lat.macros()
-            out[kind] = (lat.get_populations(np.float64), r, u)
-    a, b = out[lb.KERNEL_PLAIN], out[lb.KERNEL_ROWS]
-    assert np.isfinite(b[0]).all()
-    for x, y in zip(a, b):
-        assert np.array_equal(x, y)
+            out[kind, index64] = (lat.get_populations(np.float64), r, u)
+    a = out[lb.KERNEL_PLAIN, False]
+    for key in ((lb.KERNEL_ROWS, False), (lb.KERNEL_ROWS, True)):
+        b = out[key]
+        assert np.isfinite(b[0]).all()
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), key
 
 
 def test_row_pipeline_needs_eligible_shape():
