@@ -239,10 +239,11 @@ int   lbm_get_kernel(const lbm_ctx* c);              /* the family in use (PLAIN
  * once (it clears the error word).  The populations written by that step are invalid: set or
  * re-initialise them before stepping on.  Needs lbm_set_kernel(c, LBM_KERNEL_ROWS) (BGK or MRT).   */
 int  lbm_test_stall_next_step(lbm_ctx* c, int64_t item, int64_t wait_clocks);
-/* Test hook (no counterpart in the reference): on = 1 makes the one-pass Shan-Chen kernel index
- * populations in 64 bits even where 32-bit indices suffice (lattices with 9 N <= 2^32 take 32-bit ones),
- * so that tests can compare both forms bit for bit on small lattices; on = 0 restores the choice.   */
-int  lbm_test_sc_window_index64(lbm_ctx* c, int on);
+/* Test hook (no counterpart in the reference): on = 1 makes the plain step kernels and the one-pass
+ * Shan-Chen kernel index populations in 64 bits even where 32-bit indices suffice (they take 32-bit
+ * ones on lattices with Q N <= 2^32), so that tests can compare both forms bit for bit on small
+ * lattices; on = 0 restores the choice.                                                           */
+int  lbm_test_index64(lbm_ctx* c, int on);
 
 /* ---- conservation sums without allocation -----------------------------------------------
  * No counterpart in the reference.  For callers that cannot let a library call cudaMalloc or

@@ -150,7 +150,7 @@ extern "C" {
     pub fn lbm_set_kernel(c: *mut lbm_ctx, kind: c_int) -> c_int;
     pub fn lbm_get_kernel(c: *const lbm_ctx) -> c_int;
     pub fn lbm_test_stall_next_step(c: *mut lbm_ctx, item: i64, wait_clocks: i64) -> c_int;
-    pub fn lbm_test_sc_window_index64(c: *mut lbm_ctx, on: c_int) -> c_int;
+    pub fn lbm_test_index64(c: *mut lbm_ctx, on: c_int) -> c_int;
 
     pub fn lbm_sums_fp64_noalloc(populations: *const c_void, lattice: c_int, storage: c_int, nx: i64, ny: i64, nz: i64,
                                  storage_scale: c_double, stream: *mut c_void, out: *mut c_double) -> c_int;

@@ -56,28 +56,33 @@ struct StepParams {
     Mrt2Coef<R> mrt2;
 };
 
-// Row base offsets of the 3 (D2Q9) or 9 (D3Q27) neighbour rows of (y, z), wrap included.
-template <class L>
-struct Rows {
-    long long base[3][3];  // [dy+1][dz+1]
-    __device__ __forceinline__ Rows(int y, int z, int nx, int ny, int nz) {
+// Row base offsets of the 3 (D2Q9) or 9 (D3Q27) neighbour rows of (y, z), wrap included, as cell
+// indices of type I: long long, or uint32_t for lattices whose Q N populations all have 32-bit indices
+// (one 32-bit add and one widening multiply-add per population address instead of 64-bit arithmetic).
+template <class L, class I = long long>
+struct RowsT {
+    using Idx = I;
+    I base[3][3];  // [dy+1][dz+1]
+    __device__ __forceinline__ RowsT(int y, int z, int nx, int ny, int nz) {
         const int ys[3] = {y == 0 ? ny - 1 : y - 1, y, y == ny - 1 ? 0 : y + 1};
         const int zs[3] = {z == 0 ? nz - 1 : z - 1, z, z == nz - 1 ? 0 : z + 1};
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
             for (int b = 0; b < 3; ++b)
-                base[a][b] = ((long long)zs[b] * ny + ys[a]) * (long long)nx;
+                base[a][b] = ((I)zs[b] * (I)ny + (I)ys[a]) * (I)nx;
     }
     // source row of direction (cy, cz): pull from y - cy, z - cz
-    __device__ __forceinline__ long long src(int cy, int cz) const { return base[1 - cy][1 - cz]; }
+    __device__ __forceinline__ I src(int cy, int cz) const { return base[1 - cy][1 - cz]; }
 };
+template <class L>
+using Rows = RowsT<L, long long>;
 
 // Pull gather of one cell.  ABS = false: deviations in storage units (Codec::raw: f_i - w_i, times
 // the storage scale for the 16-bit codecs); ABS = true: the populations themselves.  x-wrap per thread; the source x of c_x = +1 is x-1 and of c_x = -1 is x+1
 // (af::shift: out[x] = in[x - c]).
-template <class L, class S, bool ABS, class P, class R>
-__device__ __forceinline__ void pull(const S* __restrict__ fin, const P& p, const Rows<L>& rows, int x,
+template <class L, class S, bool ABS, class P, class R, class Ix>
+__device__ __forceinline__ void pull(const S* __restrict__ fin, const P& p, const RowsT<L, Ix>& rows, int x,
                                      R (&d)[L::Q]) {
     const int xm = x == 0 ? p.nx - 1 : x - 1;
     const int xp = x == p.nx - 1 ? 0 : x + 1;
@@ -85,7 +90,7 @@ __device__ __forceinline__ void pull(const S* __restrict__ fin, const P& p, cons
         constexpr int i = I;
         constexpr int cx = L::cx(i), cy = L::cy(i), cz = L::cz(i);
         const int xs = cx == 1 ? xm : (cx == -1 ? xp : x);
-        const long long idx = (long long)i * p.N + rows.src(cy, cz) + xs;
+        const Ix idx = (Ix)i * (Ix)p.N + rows.src(cy, cz) + (Ix)xs;
         if constexpr (ABS)
             d[i] = Codec<S>::load(fin + idx, R(L::w(i)), R(p.inv_scale));
         else
@@ -95,13 +100,13 @@ __device__ __forceinline__ void pull(const S* __restrict__ fin, const P& p, cons
 
 // Zero-gradient outlet: populations arriving from +x are taken from cell x-1's streamed state,
 // i.e. F_i(x - 1 - c_i) = F_i(x, y - cy, z - cz) for c_x = -1.
-template <class L, class S, bool ABS, class P, class R>
-__device__ __forceinline__ void pull_zerograd(const S* __restrict__ fin, const P& p, const Rows<L>& rows, int x,
+template <class L, class S, bool ABS, class P, class R, class Ix>
+__device__ __forceinline__ void pull_zerograd(const S* __restrict__ fin, const P& p, const RowsT<L, Ix>& rows, int x,
                                               R (&d)[L::Q]) {
     static_for<L::Q>([&](auto I) {
         constexpr int i = I;
         if constexpr (L::cx(i) == -1) {
-            const long long idx = (long long)i * p.N + rows.src(L::cy(i), L::cz(i)) + x;
+            const Ix idx = (Ix)i * (Ix)p.N + rows.src(L::cy(i), L::cz(i)) + (Ix)x;
             if constexpr (ABS)
                 d[i] = Codec<S>::load(fin + idx, R(L::w(i)), R(p.inv_scale));
             else
@@ -403,6 +408,16 @@ __device__ __forceinline__ void store_cell32(S* __restrict__ fout, const P& p, u
     }
 }
 
+// store_cell or store_cell32 by the index type of c.
+template <class L, class S, bool ABS, class P, class R, class Ix>
+__device__ __forceinline__ void store_cell_ix(S* __restrict__ fout, const P& p, Ix c, const R (&out)[L::Q],
+                                              const Rounding& rnd) {
+    if constexpr (std::is_same<Ix, uint32_t>::value)
+        store_cell32<L, S, ABS>(fout, p, c, out, rnd);
+    else
+        store_cell<L, S, ABS>(fout, p, (long long)c, out, rnd);
+}
+
 // Storage scale and its inverse for raw deviations: the codec's scale for the 16-bit codecs,
 // compile-time 1 otherwise.
 template <class S, class P, class R>
@@ -416,9 +431,9 @@ __device__ __forceinline__ void storage_scale(const P& p, R& sc, R& isc) {
     }
 }
 
-template <class T>
+template <class T, class Ix>
 __device__ __forceinline__ void cell_class(const uint8_t* __restrict__ mask, const ClassTable<T>& ct,
-                                           long long c, int& cls, uint32_t& fl) {
+                                           Ix c, int& cls, uint32_t& fl) {
     cls = mask ? (int)__ldg(mask + c) : 0;
     fl = ct.flags[cls];
 }
@@ -489,12 +504,12 @@ __device__ __forceinline__ void bgk_collide(const P& p, int cls, uint32_t fl, R 
 // One cell of a BGK step read from and written to global memory.  P supplies mask, cls, nx, ny,
 // nz, N, omega, one_m_omega, scale and inv_scale (StepParams for one lattice, BatchLattice for one
 // member of an ensemble).
-template <class L, class S, bool ABS, class P>
+template <class L, class S, bool ABS, class Ix = long long, class P>
 __device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, S* __restrict__ fout, int x, int y,
                                          int z, const Rounding& rnd) {
     using R = typename Codec<S>::Real;
-    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
-    const long long c = rows.base[1][1] + x;
+    const RowsT<L, Ix> rows(y, z, p.nx, p.ny, p.nz);
+    const Ix c = rows.base[1][1] + (Ix)x;
     R v[L::Q];
     pull<L, S, ABS>(fin, p, rows, x, v);
     int cls;
@@ -505,10 +520,11 @@ __device__ __forceinline__ void bgk_cell(const P& p, const S* __restrict__ fin, 
     storage_scale<S>(p, sc, isc);
     R out[L::Q];
     bgk_collide<L, ABS, kExactWeights<S>>(p, cls, fl, v, sc, isc, out);
-    store_cell<L, S, ABS>(fout, p, c, out, rnd);
+    store_cell_ix<L, S, ABS>(fout, p, c, out, rnd);
 }
 
-template <class L, class S, bool ABS>
+// I32: 32-bit population indices (lattices with Q N <= 2^32).
+template <class L, class S, bool ABS, bool I32 = false>
 __global__ void __launch_bounds__(512) k_step_bgk(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
@@ -516,7 +532,8 @@ __global__ void __launch_bounds__(512) k_step_bgk(const __grid_constant__ StepPa
     const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, designated);
     const int y = L::DIM == 2 ? p.plo + (int)blockIdx.y * p.pstride : (int)blockIdx.y;
     const int z = L::DIM == 3 ? p.plo + (int)blockIdx.z * p.pstride : (int)blockIdx.z;
-    bgk_cell<L, S, ABS>(p, static_cast<const S*>(p.fin), static_cast<S*>(p.fout), x, y, z, rnd);
+    bgk_cell<L, S, ABS, typename std::conditional<I32, uint32_t, long long>::type>(
+        p, static_cast<const S*>(p.fin), static_cast<S*>(p.fout), x, y, z, rnd);
 }
 
 // ---- MRT (D3Q27) -------------------------------------------------------------------------
@@ -699,15 +716,16 @@ __device__ __forceinline__ void mrt2_collide(const P& p, int cls, uint32_t fl, c
     }
 }
 
-template <int BASIS, class S>
+template <int BASIS, class S, bool I32 = false>
 __global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D3Q27;
     using R = typename Codec<S>::Real;
+    using Ix = typename std::conditional<I32, uint32_t, long long>::type;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
     const int y = blockIdx.y, z = p.plo + (int)blockIdx.z * p.pstride;
-    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
-    const long long c = rows.base[1][1] + x;
+    const RowsT<L, Ix> rows(y, z, p.nx, p.ny, p.nz);
+    const Ix c = rows.base[1][1] + (Ix)x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
     R T[27];
     int cls;
@@ -738,18 +756,19 @@ __global__ void __launch_bounds__(256) k_step_mrt(const __grid_constant__ StepPa
     }
     const bool designated = (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0;
     const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, designated);
-    store_cell<L, S, false>(static_cast<S*>(p.fout), p, c, out, rnd);
+    store_cell_ix<L, S, false>(static_cast<S*>(p.fout), p, c, out, rnd);
 }
 
 // The plain (one thread per cell) step kernel of the two-rate collision.
-template <class S>
+template <class S, bool I32 = false>
 __global__ void __launch_bounds__(256) k_step_mrt2(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D3Q27;
     using R = typename Codec<S>::Real;
+    using Ix = typename std::conditional<I32, uint32_t, long long>::type;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
-    const Rows<L> rows(blockIdx.y, p.plo + (int)blockIdx.z * p.pstride, p.nx, p.ny, p.nz);
-    const long long c = rows.base[1][1] + x;
+    const RowsT<L, Ix> rows(blockIdx.y, p.plo + (int)blockIdx.z * p.pstride, p.nx, p.ny, p.nz);
+    const Ix c = rows.base[1][1] + (Ix)x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
     R v[27];
     pull<L, S, false>(fin, p, rows, x, v);
@@ -763,7 +782,7 @@ __global__ void __launch_bounds__(256) k_step_mrt2(const __grid_constant__ StepP
     mrt2_collide(p, cls, fl, v, sc, isc, out);
     const bool designated = (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0;
     const Rounding rnd = step_rounding<S>(p.tick, p.parity, p.sr, designated);
-    store_cell<L, S, false>(static_cast<S*>(p.fout), p, c, out, rnd);
+    store_cell_ix<L, S, false>(static_cast<S*>(p.fout), p, c, out, rnd);
 }
 
 // ---- Shan-Chen (D2Q9) --------------------------------------------------------------------

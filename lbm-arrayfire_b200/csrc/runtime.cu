@@ -135,7 +135,7 @@ struct lbm_ctx {
     unsigned* tick = nullptr;      // the rounding's step counter pair (step_rounding)
     WaitLimits waits = kProductionWaits;  // the row pipeline's wait limits for the next launch
     bool stall_armed = false;      // lbm_test_stall_next_step: the next step launches with `stall`
-    bool scw_index64 = false;      // lbm_test_sc_window_index64: 64-bit indices in the window kernel
+    bool index64 = false;          // lbm_test_index64: 64-bit population indices in every kernel
     WaitLimits stall = kProductionWaits;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int gsteps = 0;
@@ -378,13 +378,17 @@ static void dispatch_rows(const lbm_ctx* c, F&& f) {
 #ifndef LBM_SCW_HMAX
 #define LBM_SCW_HMAX 0  // > 0: at most this many rows per strip (several waves of CTAs on large lattices)
 #endif
-#ifndef LBM_SCW_IDX32
-#define LBM_SCW_IDX32 1  // 0: the window kernel always indexes populations in 64 bits (A/B)
+#ifndef LBM_IDX32
+#define LBM_IDX32 1  // 0: the plain and window kernels always index populations in 64 bits (A/B)
 #endif
-// The window kernel indexes populations in 32 bits when all 9 N of them have 32-bit indices.
-static bool sc_window_i32(const lbm_ctx* c) {
-    return LBM_SCW_IDX32 && !c->scw_index64 && 9ULL * (unsigned long long)c->d.nx * (unsigned long long)c->d.ny <= (1ULL << 32);
+// The plain step kernels and the Shan-Chen window kernel index populations in 32 bits when all Q N of
+// them have 32-bit indices (largest index Q N - 1).
+static bool idx32(const lbm_ctx* c) {
+    const unsigned long long n = (unsigned long long)c->d.nx * (unsigned long long)c->d.ny * (unsigned long long)c->d.nz;
+    const unsigned long long q = c->d.lattice == LBM_D3Q27 ? 27ULL : 9ULL;
+    return LBM_IDX32 && !c->index64 && q * n <= (1ULL << 32);
 }
+static bool sc_window_i32(const lbm_ctx* c) { return idx32(c); }
 // The window kernel instance of a context (storage S; absolute or deviation arithmetic; index width).
 template <class S>
 static auto sc_window_kernel(const lbm_ctx* c) {
@@ -479,27 +483,27 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
         p.pcnt = pcnt;
         p.pstride = pstride;
         const bool abs_arith = c->d.arithmetic == LBM_ARITH_ABSOLUTE;
+        const bool i32 = idx32(c);
         switch (c->d.collision) {
-            case LBM_BGK:
-                if (c->d.lattice == LBM_D2Q9) {
-                    if (abs_arith)
-                        k_step_bgk<D2Q9, S, true><<<grid, blk, 0, s>>>(p);
-                    else
-                        k_step_bgk<D2Q9, S, false><<<grid, blk, 0, s>>>(p);
-                } else {
-                    if (abs_arith)
-                        k_step_bgk<D3Q27, S, true><<<grid, blk, 0, s>>>(p);
-                    else
-                        k_step_bgk<D3Q27, S, false><<<grid, blk, 0, s>>>(p);
-                }
+            case LBM_BGK: {
+                auto kern = [&](auto lt) {
+                    using L = typename decltype(lt)::type;
+                    if (abs_arith) return i32 ? k_step_bgk<L, S, true, true> : k_step_bgk<L, S, true, false>;
+                    return i32 ? k_step_bgk<L, S, false, true> : k_step_bgk<L, S, false, false>;
+                };
+                if (c->d.lattice == LBM_D2Q9)
+                    kern(Tag<D2Q9>{})<<<grid, blk, 0, s>>>(p);
+                else
+                    kern(Tag<D3Q27>{})<<<grid, blk, 0, s>>>(p);
                 break;
+            }
             case LBM_MRT:  // deviation arithmetic only (validate_desc)
                 if (c->mrt2) {
-                    if constexpr (sizeof(S) == 2) k_step_mrt2<S><<<grid, blk, 0, s>>>(p);
+                    if constexpr (sizeof(S) == 2) (i32 ? k_step_mrt2<S, true> : k_step_mrt2<S, false>)<<<grid, blk, 0, s>>>(p);
                 } else if (c->d.mrt_basis == LBM_MRT_REF)
-                    k_step_mrt<kMrtRef, S><<<grid, blk, 0, s>>>(p);
+                    (i32 ? k_step_mrt<kMrtRef, S, true> : k_step_mrt<kMrtRef, S, false>)<<<grid, blk, 0, s>>>(p);
                 else
-                    k_step_mrt<kMrtGramSchmidt, S><<<grid, blk, 0, s>>>(p);
+                    (i32 ? k_step_mrt<kMrtGramSchmidt, S, true> : k_step_mrt<kMrtGramSchmidt, S, false>)<<<grid, blk, 0, s>>>(p);
                 break;
             default:
                 if (abs_arith) {
@@ -1325,12 +1329,12 @@ int lbm_test_stall_next_step(lbm_ctx* c, int64_t item, int64_t wait_clocks) {
     return LBM_OK;
 }
 
-int lbm_test_sc_window_index64(lbm_ctx* c, int on) {
+int lbm_test_index64(lbm_ctx* c, int on) {
     if (!c) return set_error(LBM_ERR_INVALID, "context is NULL");
     LBM_CK(cudaSetDevice(c->d.device));
     LBM_CK(cudaStreamSynchronize(c->stream));
     drop_graphs(c);  // captured launches name the kernel instance
-    c->scw_index64 = on != 0;
+    c->index64 = on != 0;
     return LBM_OK;
 }
 

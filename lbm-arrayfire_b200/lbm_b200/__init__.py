@@ -127,7 +127,7 @@ _SIGS = {
     "lbm_set_kernel": (C.c_int, [_P, C.c_int]),
     "lbm_get_kernel": (C.c_int, [_P]),
     "lbm_test_stall_next_step": (C.c_int, [_P, C.c_int64, C.c_int64]),
-    "lbm_test_sc_window_index64": (C.c_int, [_P, C.c_int]),
+    "lbm_test_index64": (C.c_int, [_P, C.c_int]),
     "lbm_set_cell_offset": (C.c_int, [_P, C.c_int64]),
     "lbm_step_planes": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int, _P]),
     "lbm_set_reserved_sms": (C.c_int, [_P, C.c_int]),
@@ -402,10 +402,10 @@ class Lattice:
         `wait_clocks` clocks; lbm_sync then reports LBM_ERR_TIMEOUT (see lbm_test_stall_next_step)."""
         _check(lib().lbm_test_stall_next_step(self._h, item, wait_clocks))
 
-    def test_sc_window_index64(self, on: bool = True):
-        """Test hook: the one-pass Shan-Chen kernel indexes populations in 64 bits (see
-        lbm_test_sc_window_index64)."""
-        _check(lib().lbm_test_sc_window_index64(self._h, int(bool(on))))
+    def test_index64(self, on: bool = True):
+        """Test hook: the plain step kernels and the one-pass Shan-Chen kernel index populations in 64
+        bits (see lbm_test_index64)."""
+        _check(lib().lbm_test_index64(self._h, int(bool(on))))
 
     def device_populations(self):
         nbytes = C.c_size_t()

@@ -431,7 +431,7 @@ def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
         with lb.Lattice(d, m) as lat:
             lat.set_kernel(kind)
             if index64:
-                lat.test_sc_window_index64(True)
+                lat.test_index64(True)
             lat.init_equilibrium(rho=rho)
             lat.step(40)
             lat.sync()
@@ -444,6 +444,42 @@ def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
         assert np.isfinite(b[0]).all()
         for x, y in zip(a, b):
             assert np.array_equal(x, y), key
+
+
+def _index_case(case, storage):
+    if case == "cavity2d":
+        return cavity2d(n=64, u_lid=0.1, re=300, storage=storage)
+    if case == "channel2d":  # equilibrium inlet, zero-gradient outlet, cylinder
+        return channel2d(96, 40, 0.04, 100.0, 24, 20, 6, storage=storage, config_mode=True, seed=1, noise=1e-3)
+    if case == "cavity3d":
+        return cavity3d(n=(24, 14, 12), u_lid=0.05, omega=1.3, storage=storage)
+    rates = lb.mrt_rates(1.7, 1.2) if case == "mrt_two_rate" else None
+    basis = lb.MRT_REF if case == "mrt_ref" else lb.MRT_GRAM_SCHMIDT
+    return mrt_cavity(n=12, u_lid=0.1, storage=storage, basis=basis, rates=rates)
+
+
+@pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.BF16S, lb.F64])
+@pytest.mark.parametrize("case", ["cavity2d", "channel2d", "cavity3d", "mrt_ref", "mrt_gs", "mrt_two_rate"])
+@pytest.mark.parametrize("arith", [lb.ARITH_DEVIATION, lb.ARITH_ABSOLUTE])
+def test_plain_kernels_32_and_64_bit_indices_agree(storage, case, arith):
+    """The plain step kernels (BGK, MRT in both bases, the two-rate MRT of 16-bit storage) with 32-bit
+    population indices (their choice on lattices with Q N <= 2^32) and with 64-bit ones (forced by a
+    test hook): bit-identical populations, with bounce-back, lid, inlet and zero-gradient classes."""
+    if arith == lb.ARITH_ABSOLUTE and (storage in (lb.F16S, lb.BF16S) or case.startswith("mrt")):
+        pytest.skip("absolute arithmetic: F32/F64 BGK only")
+    d, m, F0 = _index_case(case, storage)
+    d.arithmetic = arith
+    out = []
+    for index64 in (False, True):
+        with lb.Lattice(d, m) as lat:
+            lat.set_kernel(lb.KERNEL_PLAIN)
+            if index64:
+                lat.test_index64(True)
+            lat.set_populations(np.asarray(F0, dtype=np.float64))
+            lat.step(30)
+            assert lat.kernel() == lb.KERNEL_PLAIN
+            out.append(lat.get_populations(np.float64))
+    assert np.isfinite(out[0]).all() and np.array_equal(out[0], out[1])
 
 
 def test_row_pipeline_needs_eligible_shape():
