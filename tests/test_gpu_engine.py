@@ -451,33 +451,47 @@ def _index_case(case, storage):
         return cavity2d(n=64, u_lid=0.1, re=300, storage=storage)
     if case == "channel2d":  # equilibrium inlet, zero-gradient outlet, cylinder
         return channel2d(96, 40, 0.04, 100.0, 24, 20, 6, storage=storage, config_mode=True, seed=1, noise=1e-3)
+    if case == "channel2d_wide":  # rows wider than 1024 cells: the segmented row kernel
+        return channel2d(1088, 12, 0.04, 100.0, 300, 6, 3, storage=storage, config_mode=True, seed=1, noise=1e-3)
     if case == "cavity3d":
-        return cavity3d(n=(24, 14, 12), u_lid=0.05, omega=1.3, storage=storage)
+        return cavity3d(n=(32, 14, 12), u_lid=0.05, omega=1.3, storage=storage)
+    if case == "mrt_wide":  # D3Q27 rows wider than 1024 cells
+        d = lb.make_desc(lb.D3Q27, lb.MRT, storage, (1040, 4, 6), mrt_s=lb.mrt_rates(1.7, 1.1),
+                         mrt_basis=lb.MRT_GRAM_SCHMIDT)
+        m = lb.setup_cavity3d(d, 0.05)
+        w = lb.velocities(lb.D3Q27)[3]
+        rng = np.random.default_rng(13)
+        return d, m, np.repeat(w, d.cells) * (1.0 + 0.01 * rng.standard_normal(27 * d.cells))
     rates = lb.mrt_rates(1.7, 1.2) if case == "mrt_two_rate" else None
     basis = lb.MRT_REF if case == "mrt_ref" else lb.MRT_GRAM_SCHMIDT
-    return mrt_cavity(n=12, u_lid=0.1, storage=storage, basis=basis, rates=rates)
+    return mrt_cavity(n=16, u_lid=0.1, storage=storage, basis=basis, rates=rates)
 
 
 @pytest.mark.parametrize("storage", [lb.F32, lb.F16S, lb.BF16S, lb.F64])
-@pytest.mark.parametrize("case", ["cavity2d", "channel2d", "cavity3d", "mrt_ref", "mrt_gs", "mrt_two_rate"])
+@pytest.mark.parametrize("case", ["cavity2d", "channel2d", "channel2d_wide", "cavity3d", "mrt_ref", "mrt_gs",
+                                  "mrt_two_rate", "mrt_wide"])
 @pytest.mark.parametrize("arith", [lb.ARITH_DEVIATION, lb.ARITH_ABSOLUTE])
-def test_plain_kernels_32_and_64_bit_indices_agree(storage, case, arith):
+@pytest.mark.parametrize("kernel", [lb.KERNEL_PLAIN, lb.KERNEL_ROWS])
+def test_32_and_64_bit_indices_agree(storage, case, arith, kernel):
     """The plain step kernels (BGK, MRT in both bases, the two-rate MRT of 16-bit storage) with 32-bit
-    population indices (their choice on lattices with Q N <= 2^32) and with 64-bit ones (forced by a
-    test hook): bit-identical populations, with bounce-back, lid, inlet and zero-gradient classes."""
+    population indices, and the row kernels (row groups and row segments) with 32-bit output-plane
+    offsets -- their choice on lattices with Q N <= 2^32 -- against the 64-bit forms (forced by a test
+    hook): bit-identical populations, with bounce-back, lid, inlet and zero-gradient classes."""
     if arith == lb.ARITH_ABSOLUTE and (storage in (lb.F16S, lb.BF16S) or case.startswith("mrt")):
         pytest.skip("absolute arithmetic: F32/F64 BGK only")
+    if kernel == lb.KERNEL_ROWS and (storage == lb.F64 or arith == lb.ARITH_ABSOLUTE):
+        pytest.skip("the row pipeline takes F32 and 16-bit storage in deviation arithmetic")
     d, m, F0 = _index_case(case, storage)
     d.arithmetic = arith
     out = []
     for index64 in (False, True):
         with lb.Lattice(d, m) as lat:
-            lat.set_kernel(lb.KERNEL_PLAIN)
+            lat.set_kernel(kernel)
             if index64:
                 lat.test_index64(True)
             lat.set_populations(np.asarray(F0, dtype=np.float64))
             lat.step(30)
-            assert lat.kernel() == lb.KERNEL_PLAIN
+            assert lat.kernel() == kernel
             out.append(lat.get_populations(np.float64))
     assert np.isfinite(out[0]).all() and np.array_equal(out[0], out[1])
 
