@@ -363,21 +363,11 @@ __device__ __forceinline__ void encode16(const R (&out)[L::Q], const Rounding& r
     }
 }
 
-// Offset i N of direction i's plane, in elements: I32 (lattices with Q N <= 2^32) a 32-bit product,
-// uniform across the threads, so an address fo + i N is one widening multiply-add; 64-bit otherwise.
-template <bool I32>
-__device__ __forceinline__ auto plane_off(int i, long long N) {
-    if constexpr (I32)
-        return (uint32_t)i * (uint32_t)N;
-    else
-        return (long long)i * N;
-}
-
 // The 16-bit store of a cell's outputs at fo[i * N].
-template <class L, class S, bool I32 = false, class R>
+template <class L, class S, class R>
 __device__ __forceinline__ void store16(S* __restrict__ fo, long long N, const R (&out)[L::Q], const Rounding& rnd,
                                         uint32_t cell) {
-    encode16<L, S>(out, rnd, cell, [&](auto I, S v) { fo[plane_off<I32>(decltype(I)::value, N)] = v; });
+    encode16<L, S>(out, rnd, cell, [&](auto I, S v) { fo[(long long)decltype(I)::value * N] = v; });
 }
 
 template <class L, class S, bool ABS, class P, class R>

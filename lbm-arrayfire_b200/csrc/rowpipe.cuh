@@ -267,7 +267,7 @@ constexpr int kSegPitch = 1024;
 // One cell of the row pipeline: st points at the staged row of direction 0 (direction i at
 // st[i * SB]); x, xm, xp are the staged indices of the cell and of its left and right neighbours
 // (periodic wrap already applied), mrow[mi] its class, orow[ox] its place in the output row.
-template <class L, class S, int SB, int COLL, bool I32 = false, class P>
+template <class L, class S, int SB, int COLL, class P>
 __device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t* mrow, int x, int xm, int xp,
                                          int mi, int ox, typename Codec<S>::Real sc, typename Codec<S>::Real isc,
                                          S* orow, const Rounding& rnd, uint32_t cell) {
@@ -312,23 +312,23 @@ __device__ __forceinline__ void row_cell(const P& p, const S* st, const uint8_t*
     }
     S* __restrict__ fo = orow + ox;
     if constexpr (Codec<S>::kScaled) {
-        store16<L, S, I32>(fo, p.N, out, rnd, cell);
+        store16<L, S>(fo, p.N, out, rnd, cell);
     } else {
         static_for<Q>([&](auto I) {
             constexpr int i = I;
-            fo[plane_off<I32>(i, p.N)] = Codec<S>::enc(out[i], R(L::w(i)));
+            fo[(long long)i * p.N] = Codec<S>::enc(out[i], R(L::w(i)));
         });
     }
 }
 
 // A cell of a whole staged row of width nx (periodic in x); row0: the cell index of the row's x = 0.
-template <class L, class S, int SB, int COLL, bool I32 = false, class P>
+template <class L, class S, int SB, int COLL, class P>
 __device__ __forceinline__ void row_cell_wrap(const P& p, const S* st, const uint8_t* mrow, int x, int nx,
                                               typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow,
                                               const Rounding& rnd, uint32_t row0) {
     const int xm = x == 0 ? nx - 1 : x - 1;
     const int xp = x == nx - 1 ? 0 : x + 1;
-    row_cell<L, S, SB, COLL, I32>(p, st, mrow, x, xm, xp, x, x, sc, isc, orow, rnd, row0 + (uint32_t)x);
+    row_cell<L, S, SB, COLL>(p, st, mrow, x, xm, xp, x, x, sc, isc, orow, rnd, row0 + (uint32_t)x);
 }
 
 // Two adjacent cells (x even and x + 1) of a staged row, for 16-bit
@@ -340,7 +340,7 @@ __device__ __forceinline__ void row_cell_wrap(const P& p, const S* st, const uin
 // bits as the one-cell path (pair_rbits), so the kernel families stay bit-identical.
 // x: staged index of the first cell (even); xl, xr: staged indices of the pair's left and right neighbours
 // (periodic wrap or halo already applied).
-template <class L, class S, int SB, int COLL, bool I32 = false, class P>
+template <class L, class S, int SB, int COLL, class P>
 __device__ __forceinline__ void row_pair(const P& p, const S* st, const uint8_t* mrow, int x, int xl, int xr,
                                          typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow,
                                          const Rounding& rnd, uint32_t cell) {
@@ -410,22 +410,22 @@ __device__ __forceinline__ void row_pair(const P& p, const S* st, const uint8_t*
         const PairBits pb{(cell_hash16(cell + 1u, rnd.seed) << 16) | cell_hash16(cell, rnd.seed)};
         static_for<Q>([&](auto I) {
             constexpr int i = I;
-            *reinterpret_cast<uint32_t*>(fo + plane_off<I32>(i, p.N)) = Pair16<S>::rs(outB[i], outA[i], pb.template word<i, i>());
+            *reinterpret_cast<uint32_t*>(fo + (long long)i * p.N) = Pair16<S>::rs(outB[i], outA[i], pb.template word<i, i>());
         });
     } else {
         static_for<Q>([&](auto I) {
             constexpr int i = I;
-            *reinterpret_cast<uint32_t*>(fo + plane_off<I32>(i, p.N)) = Pair16<S>::rn(outB[i], outA[i]);
+            *reinterpret_cast<uint32_t*>(fo + (long long)i * p.N) = Pair16<S>::rn(outB[i], outA[i]);
         });
     }
 }
 
 // A pair of a whole staged row of width nx (periodic in x); row0: the cell index of the row's x = 0.
-template <class L, class S, int SB, int COLL, bool I32 = false, class P>
+template <class L, class S, int SB, int COLL, class P>
 __device__ __forceinline__ void row_pair_wrap(const P& p, const S* st, const uint8_t* mrow, int x, int nx,
                                               typename Codec<S>::Real sc, typename Codec<S>::Real isc, S* orow,
                                               const Rounding& rnd, uint32_t row0) {
-    row_pair<L, S, SB, COLL, I32>(p, st, mrow, x, x == 0 ? nx - 1 : x - 1, x + 2 == nx ? 0 : x + 2, sc, isc, orow, rnd,
+    row_pair<L, S, SB, COLL>(p, st, mrow, x, x == 0 ? nx - 1 : x - 1, x + 2 == nx ? 0 : x + 2, sc, isc, orow, rnd,
                              row0 + (uint32_t)x);
 }
 
@@ -439,8 +439,7 @@ __device__ __forceinline__ void row_pair_wrap(const P& p, const S* st, const uin
 template <class L, class S, int PITCH, int COLL>
 using RowShape = RowPipeShape<L, S, PITCH, false, kRowPair<L, S, COLL>, LBM_ROWPIPE_PAIR_WARPS3_ROWS>;
 
-// I32: the output planes' offsets i N as 32-bit products (lattices with Q N <= 2^32).
-template <class L, class S, int PITCH, int COLL, bool I32 = false>
+template <class L, class S, int PITCH, int COLL>
 __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, RowShape<L, S, PITCH, COLL>::CTAS)
     k_step_rows(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int rows, int* __restrict__ err,
                   const WaitLimits wl) {
@@ -555,10 +554,10 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
 #pragma unroll 1
         while (b < nb) {
             if constexpr (kPair)
-                row_pair_wrap<L, S, SB, COLL, I32>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, 2 * x, nx, sc, isc,
+                row_pair_wrap<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, 2 * x, nx, sc, isc,
                                               out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
             else
-                row_cell_wrap<L, S, SB, COLL, I32>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, x, nx, sc, isc,
+                row_cell_wrap<L, S, SB, COLL>(p, st0 + b * nx, ms0 ? ms0 + b * nx : nullptr, x, nx, sc, isc,
                                               out0 + (long long)b * nx, rnd, cell0 + (uint32_t)(b * nx));
             x += cr;
             b += cq;
@@ -584,7 +583,7 @@ __global__ void __launch_bounds__(RowShape<L, S, PITCH, COLL>::CONSUMERS + 32, R
 template <class L, class S, int COLL>
 using SegShape = RowPipeShape<L, S, kSegPitch, true, kRowPair<L, S, COLL>>;
 
-template <class L, class S, int COLL, bool I32 = false>
+template <class L, class S, int COLL>
 __global__ void __launch_bounds__(SegShape<L, S, COLL>::CONSUMERS + 32, SegShape<L, S, COLL>::CTAS)
     k_step_rows_seg(const __grid_constant__ StepParams<typename Codec<S>::Real> p, int segw, int* __restrict__ err,
                   const WaitLimits wl) {
@@ -707,12 +706,12 @@ __global__ void __launch_bounds__(SegShape<L, S, COLL>::CONSUMERS + 32, SegShape
             // pairs (xl, xl + 1): w is even, the halos hold both neighbours
 #pragma unroll 1
             for (int xl = 2 * tid; xl < w; xl += 2 * Sh::CONSUMERS)
-                row_pair<L, S, SB, COLL, I32>(p, st, mrow, xl, xl - 1, xl + 2, sc, isc, orow, rnd, cell0 + (uint32_t)xl);
+                row_pair<L, S, SB, COLL>(p, st, mrow, xl, xl - 1, xl + 2, sc, isc, orow, rnd, cell0 + (uint32_t)xl);
         } else {
 #pragma unroll 1
             for (int xl = tid; xl < w; xl += Sh::CONSUMERS)
-                row_cell<L, S, SB, COLL, I32>(p, st, mrow, xl, xl - 1, xl + 1, xl, xl, sc, isc, orow, rnd,
-                                              cell0 + (uint32_t)xl);
+                row_cell<L, S, SB, COLL>(p, st, mrow, xl, xl - 1, xl + 1, xl, xl, sc, isc, orow, rnd,
+                                         cell0 + (uint32_t)xl);
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);

@@ -293,49 +293,34 @@ static int rows_grid_for(const lbm_ctx* c, int pcnt, int pstride, bool side = fa
     return grid;
 }
 
-#ifndef LBM_IDX32
-#define LBM_IDX32 1  // 0: every step kernel indexes populations in 64 bits (A/B)
-#endif
-// The plain step kernels and the Shan-Chen window kernel index populations, and the row kernels offset
-// their output planes, in 32 bits when all Q N populations have 32-bit indices (largest Q N - 1).
-static bool idx32(const lbm_ctx* c) {
-    const unsigned long long n = (unsigned long long)c->d.nx * (unsigned long long)c->d.ny * (unsigned long long)c->d.nz;
-    const unsigned long long q = c->d.lattice == LBM_D3Q27 ? 27ULL : 9ULL;
-    return LBM_IDX32 && !c->index64 && q * n <= (1ULL << 32);
-}
 template <class L, class S, int PITCH, int COLL>
 static void launch_rows_t(lbm_ctx* c, const StepParams<typename Codec<S>::Real>& p, cudaStream_t s, bool side) {
     const int grid = rows_grid_for(c, p.pcnt, p.pstride, side);
-    const bool i32 = idx32(c);
     if (rows_segmented(c)) {
         using Sh = SegShape<L, S, COLL>;
-        auto kern = i32 ? k_step_rows_seg<L, S, COLL, true> : k_step_rows_seg<L, S, COLL, false>;
-        kern<<<grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err, c->waits);
+        k_step_rows_seg<L, S, COLL><<<grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err,
+                                                                                       c->waits);
         return;
     }
     using Sh = RowShape<L, S, PITCH, COLL>;
-    auto kern = i32 ? k_step_rows<L, S, PITCH, COLL, true> : k_step_rows<L, S, PITCH, COLL, false>;
+    auto kern = k_step_rows<L, S, PITCH, COLL>;
     kern<<<grid, Sh::CONSUMERS + 32, Sh::smem_bytes(), s>>>(p, c->rows_rpg, c->err, c->waits);  // + producer warp
 }
 
-// Both index forms of a row kernel get the shared-memory attribute (lbm_test_index64 may switch
-// between them after this); the occupancy of the two is the same launch bound.
 template <class L, class S, int PITCH, int COLL>
 static int prepare_rows_t(lbm_ctx* c) {
     int per_sm = 0, sms = 0;
     LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->d.device));
     if (rows_segmented(c)) {
         using Sh = SegShape<L, S, COLL>;
-        for (auto kern : {k_step_rows_seg<L, S, COLL, true>, k_step_rows_seg<L, S, COLL, false>})
-            LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
-        auto kern = idx32(c) ? k_step_rows_seg<L, S, COLL, true> : k_step_rows_seg<L, S, COLL, false>;
+        auto kern = k_step_rows_seg<L, S, COLL>;
+        LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
         LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
         c->rows_rpg = seg_width(Sh::SEGW_RUN);
     } else {
         using Sh = RowShape<L, S, PITCH, COLL>;
-        for (auto kern : {k_step_rows<L, S, PITCH, COLL, true>, k_step_rows<L, S, PITCH, COLL, false>})
-            LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
-        auto kern = idx32(c) ? k_step_rows<L, S, PITCH, COLL, true> : k_step_rows<L, S, PITCH, COLL, false>;
+        auto kern = k_step_rows<L, S, PITCH, COLL>;
+        LBM_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem_bytes()));
         LBM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Sh::CONSUMERS + 32, Sh::smem_bytes()));
         c->rows_rpg = Sh::rows_per_group((int)c->d.nx);
     }
@@ -393,6 +378,16 @@ static void dispatch_rows(const lbm_ctx* c, F&& f) {
 #ifndef LBM_SCW_HMAX
 #define LBM_SCW_HMAX 0  // > 0: at most this many rows per strip (several waves of CTAs on large lattices)
 #endif
+#ifndef LBM_IDX32
+#define LBM_IDX32 1  // 0: the plain and window kernels always index populations in 64 bits (A/B)
+#endif
+// The plain step kernels and the Shan-Chen window kernel index populations in 32 bits when all Q N of
+// them have 32-bit indices (largest index Q N - 1).
+static bool idx32(const lbm_ctx* c) {
+    const unsigned long long n = (unsigned long long)c->d.nx * (unsigned long long)c->d.ny * (unsigned long long)c->d.nz;
+    const unsigned long long q = c->d.lattice == LBM_D3Q27 ? 27ULL : 9ULL;
+    return LBM_IDX32 && !c->index64 && q * n <= (1ULL << 32);
+}
 static bool sc_window_i32(const lbm_ctx* c) { return idx32(c); }
 // The window kernel instance of a context (storage S; absolute or deviation arithmetic; index width).
 template <class S>

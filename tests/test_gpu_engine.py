@@ -471,16 +471,14 @@ def _index_case(case, storage):
 @pytest.mark.parametrize("case", ["cavity2d", "channel2d", "channel2d_wide", "cavity3d", "mrt_ref", "mrt_gs",
                                   "mrt_two_rate", "mrt_wide"])
 @pytest.mark.parametrize("arith", [lb.ARITH_DEVIATION, lb.ARITH_ABSOLUTE])
-@pytest.mark.parametrize("kernel", [lb.KERNEL_PLAIN, lb.KERNEL_ROWS])
-def test_32_and_64_bit_indices_agree(storage, case, arith, kernel):
+def test_plain_kernels_32_and_64_bit_indices_agree(storage, case, arith):
     """The plain step kernels (BGK, MRT in both bases, the two-rate MRT of 16-bit storage) with 32-bit
-    population indices, and the row kernels (row groups and row segments) with 32-bit output-plane
-    offsets -- their choice on lattices with Q N <= 2^32 -- against the 64-bit forms (forced by a test
-    hook): bit-identical populations, with bounce-back, lid, inlet and zero-gradient classes."""
+    population indices (their choice on lattices with Q N <= 2^32) and with 64-bit ones (forced by a
+    test hook): bit-identical populations, with bounce-back, lid, inlet and zero-gradient classes, on
+    rows narrower and wider than 1024 cells."""
     if arith == lb.ARITH_ABSOLUTE and (storage in (lb.F16S, lb.BF16S) or case.startswith("mrt")):
         pytest.skip("absolute arithmetic: F32/F64 BGK only")
-    if kernel == lb.KERNEL_ROWS and (storage == lb.F64 or arith == lb.ARITH_ABSOLUTE):
-        pytest.skip("the row pipeline takes F32 and 16-bit storage in deviation arithmetic")
+    kernel = lb.KERNEL_PLAIN
     d, m, F0 = _index_case(case, storage)
     d.arithmetic = arith
     out = []
