@@ -196,8 +196,9 @@ int   lbm_face_set(lbm_ctx* c, int64_t plane, const int32_t* dirs, int32_t ndirs
  * disjoint planes of the other); the caller orders every one of them before the next step's first
  * launch.  This lets a slab of a decomposed lattice update its two boundary planes (first 1, count 2,
  * stride n - 1) and exchange their faces on a side stream while its interior planes are updated (no
- * counterpart in the reference).  BGK and MRT; not Shan-Chen.  Planes outside the sets keep whatever
- * the other buffer held.                                                                           */
+ * counterpart in the reference).  Shan-Chen plane sets run the one-pass window kernel (bit-identical
+ * to the two passes; it writes psi of its own rows only).  Planes outside the sets keep whatever the
+ * other buffer held.                                                                               */
 int   lbm_step_planes(lbm_ctx* c, int64_t first, int64_t count, int64_t stride, int finish, void* stream);
 /* Splits the SMs between the context stream and side streams for the row pipeline's persistent grid
  * (0..64; default 0): its launches on the context stream leave `sms` SMs free, so that kernels on

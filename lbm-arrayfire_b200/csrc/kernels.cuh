@@ -1002,9 +1002,18 @@ __global__ void __launch_bounds__(kScwTX, sizeof(typename Codec<S>::Real) == 8 ?
     const int nx = p.nx, ny = p.ny;
     const int tx = threadIdx.x;
     const int x0 = blockIdx.x * TX;
-    const int ys = blockIdx.y * rows_per_strip;
-    if (ys >= ny) return;  // uniform over the block
-    const int ye = ys + rows_per_strip < ny ? ys + rows_per_strip : ny;
+    // rows plo + k pstride, k < pcnt: contiguous (pstride 1) in strips of rows_per_strip rows, else one
+    // row per strip
+    int ys, ye;
+    if (p.pstride == 1) {
+        const int end = p.plo + p.pcnt;
+        ys = p.plo + (int)blockIdx.y * rows_per_strip;
+        if (ys >= end) return;  // uniform over the block
+        ye = ys + rows_per_strip < end ? ys + rows_per_strip : end;
+    } else {
+        ys = p.plo + (int)blockIdx.y * p.pstride;
+        ye = ys + 1;
+    }
     const int x = x0 + tx;
     const bool own_x = x < nx;
     const int xs = own_x ? x : x % nx;  // past the edge: the periodic image (only its psi is used)

@@ -131,6 +131,7 @@ struct lbm_ctx {
     int reserved_sms = 0;          // lbm_set_reserved_sms: SMs the persistent grids leave free
     int cl_ctas = 0, cl_rows = 0;  // cluster-resident kernel: CTAs of the cluster, rows per CTA
     int rows_rpg = 1;              // its rows per group (segmented rows: the segment width)
+    long long scw_target = 0;      // Shan-Chen window kernel: resident CTAs of the device (0: not queried)
     int* err = nullptr;            // device error word of the row pipeline
     unsigned* tick = nullptr;      // the rounding's step counter pair (step_rounding)
     WaitLimits waits = kProductionWaits;  // the row pipeline's wait limits for the next launch
@@ -396,6 +397,12 @@ static auto sc_window_kernel(const lbm_ctx* c) {
     if (sc_window_i32(c)) return abs_arith ? k_step_sc_window<S, true, true> : k_step_sc_window<S, false, true>;
     return abs_arith ? k_step_sc_window<S, true, false> : k_step_sc_window<S, false, false>;
 }
+// Rows per strip of the Shan-Chen window kernel over `rows` contiguous rows: one wave of CTAs.
+static int sc_strip_rows(const lbm_ctx* c, long long rows) {
+    const long long gx = (c->d.nx + kScwTX - 1) / kScwTX;
+    const long long h = std::max<long long>(4, (rows * gx + c->scw_target - 1) / c->scw_target);
+    return (int)(LBM_SCW_HMAX > 0 ? std::min<long long>(h, LBM_SCW_HMAX) : h);
+}
 static int prepare_rows(lbm_ctx* c) {
     if (c->d.collision == LBM_SHANCHEN) {
         // k_step_sc_window: strips of rows sized so that one wave of CTAs covers the lattice (A/B:
@@ -409,10 +416,8 @@ static int prepare_rows(lbm_ctx* c) {
         });
         if (rc) return rc;
         LBM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->d.device));
-        const long long gx = (c->d.nx + kScwTX - 1) / kScwTX;
-        const long long target = std::max(1LL, (long long)std::max(per_sm, 1) * sms);
-        const long long h = std::max<long long>(4, (c->d.ny * gx + target - 1) / target);
-        c->rows_rpg = (int)(LBM_SCW_HMAX > 0 ? std::min<long long>(h, LBM_SCW_HMAX) : h);
+        c->scw_target = std::max(1LL, (long long)std::max(per_sm, 1) * sms);
+        c->rows_rpg = sc_strip_rows(c, c->d.ny);
         return LBM_OK;
     }
     int rc = LBM_OK;
@@ -424,10 +429,10 @@ static int prepare_rows(lbm_ctx* c) {
     return rc;
 }
 
-// Launch one time step reading buffer `from` and writing the other one.
-// Launch one time step reading buffer `from` and writing the other one, over planes [plo, plo + pcnt)
-// of the slowest axis, plo + k pstride for k < pcnt (pcnt < 0: all of them; Shan-Chen always steps
-// every plane).
+// Launch one time step reading buffer `from` and writing the other one, over planes plo + k pstride,
+// k < pcnt, of the slowest axis (pcnt < 0: all of them).  Plane sets of Shan-Chen take the one-pass
+// window kernel whatever the family (bit-identical to the two passes): it writes psi of its own rows
+// only, so launches of disjoint sets may run at the same time.
 static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo = 0, int pcnt = -1,
                         int pstride = 1, bool side = false) {
     const int planes = (int)(c->d.lattice == LBM_D3Q27 ? c->d.nz : c->d.ny);
@@ -439,7 +444,8 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
     // the cluster-resident family runs whole multi-step launches (launch_cluster); anything else it is
     // asked for (plane sets, graph capture) takes the plain kernel, bit-identical to it
     if (c->kernel_used == LBM_KERNEL_CLUSTER && block <= 0) block = 128;
-    if (c->kernel_used == LBM_KERNEL_ROWS && c->d.collision == LBM_SHANCHEN) {
+    const bool whole = plo == 0 && pcnt == planes && pstride == 1;
+    if (c->d.collision == LBM_SHANCHEN && (c->kernel_used == LBM_KERNEL_ROWS || !whole)) {
         dispatch_storage(c->d.storage, [&](auto tag) {
             using S = typename decltype(tag)::type;
             using R = typename Codec<S>::Real;
@@ -447,8 +453,13 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
             p.fin = c->f[from];
             p.fout = c->f[from ^ 1];
             p.parity = from;
-            const int h = c->rows_rpg;
-            const dim3 wg((unsigned)((c->d.nx + kScwTX - 1) / kScwTX), (unsigned)((c->d.ny + h - 1) / h), 1);
+            p.plo = plo;
+            p.pcnt = pcnt;
+            p.pstride = pstride;
+            // contiguous rows: strips of h rows; a strided set: one row per strip
+            const int h = whole ? c->rows_rpg : pstride > 1 ? 1 : sc_strip_rows(c, pcnt);
+            const unsigned gy = (unsigned)(pstride > 1 ? pcnt : (pcnt + h - 1) / h);
+            const dim3 wg((unsigned)((c->d.nx + kScwTX - 1) / kScwTX), gy, 1);
             sc_window_kernel<S>(c)<<<wg, kScwTX, 0, s>>>(p, h);
         });
         return;
@@ -1268,11 +1279,13 @@ int lbm_step_planes(lbm_ctx* c, int64_t first, int64_t count, int64_t stride, in
     const long long planes = c->d.lattice == LBM_D3Q27 ? c->d.nz : c->d.ny;
     if (first < 0 || count < 1 || stride < 1 || first >= planes || (count - 1) > (planes - 1 - first) / stride)
         return set_error(LBM_ERR_INVALID, "planes outside the lattice's slowest axis");
-    if (c->d.collision == LBM_SHANCHEN)
-        return set_error(LBM_ERR_UNSUPPORTED, "Shan-Chen steps every plane at once (its force reads psi of the neighbours)");
     LBM_CK(cudaSetDevice(c->d.device));
     if (!c->kernel_used) {
         int rc = autotune(c);
+        if (rc) return rc;
+    }
+    if (c->d.collision == LBM_SHANCHEN && !c->scw_target) {  // plane sets take the window kernel
+        int rc = prepare_rows(c);
         if (rc) return rc;
     }
     // a launch on a side stream runs in the SMs that lbm_set_reserved_sms keeps from the context stream

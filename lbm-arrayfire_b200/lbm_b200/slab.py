@@ -21,8 +21,9 @@ neighbours, and psi of a cell needs that cell's streamed density, so the update 
 plane reads populations two planes below it: the adjacent ghost plane's c = 0 and c = +1 populations
 (its streamed density, and what streams into the interior) and the far ghost plane's c = +1 ones (6 + 3
 of the 9 per cell and side).  The ghost planes keep the global lattice's own cell classes there, since
-psi of a boundary class depends on it.  The update stays one kernel launch per step with one exchange
-after it; the ghost planes' own updates are never read.
+psi of a boundary class depends on it.  The ghost planes' own updates are never read; the overlapped
+step updates the two bottom and the two top rows beside the interior (`lbm_step_planes` runs Shan-Chen
+plane sets on the one-pass window kernel).
 
 On a GPU the exchange overlaps the interior update (`lbm_step_planes`).  Within a step the slab's
 stream updates planes 2 .. n-1 in all but a few SMs, while a second (high-priority) CUDA stream, in
@@ -207,17 +208,17 @@ class Slab:
         self._buf = {name: torch.empty(k, dtype=word, device=self.device)
                      for name in ("send_up", "send_down", "recv_down", "recv_up")}
         self.lat.set_populations(scatter_populations(desc, F0, self.p0, self.p1))
-        # the overlapped step (see the module docstring): GPU steppers with plane ranges, >= 3 planes,
-        # one ghost plane per side (not Shan-Chen)
+        # the overlapped step (see the module docstring): GPU steppers with plane ranges and at least
+        # one plane that no neighbour reads (n > 2h)
         self.overlap = (overlap and self.device.type == "cuda" and hasattr(self.lat, "step_planes")
-                        and self.n >= 3 and self.h == 1)
+                        and self.n > 2 * self.h)
         if self.overlap:
             # the exchange stream runs first wherever SMs free up; the row pipeline leaves it some
             self._comm = torch.cuda.Stream(device=self.device, priority=-1)
             self.lat.set_reserved_sms(reserved_sms)
-            self._views = _plane_views(self.lat, self.n + 2, self.device)
-            self._up_idx = torch.tensor(self.up_dirs, device=self.device)
-            self._down_idx = torch.tensor(self.down_dirs, device=self.device)
+            self._views = _plane_views(self.lat, self.n + 2 * self.h, self.device)
+            self._up_idx = [torch.tensor(dirs, device=self.device) for _, dirs, _, _ in self._up_seg]
+            self._down_idx = [torch.tensor(dirs, device=self.device) for _, dirs, _, _ in self._down_seg]
             self._ready, self._done = torch.cuda.Event(), torch.cuda.Event()
 
     def _pack(self):
@@ -265,16 +266,14 @@ class Slab:
         the SMs the row pipeline leaves free, the boundary planes and the face exchange."""
         import torch
 
-        dist, lat, n, b = self.dist, self.lat, self.n, self._buf
-        main, comm, up_idx, down_idx = self.stream, self._comm, self._up_idx, self._down_idx
+        dist, lat, n, h, b = self.dist, self.lat, self.n, self.h, self._buf
+        main, comm = self.stream, self._comm
         self._ready.record(main)  # the previous step (and its exchange) is complete on `main`
         F = self._views[lat.device_buffers()[1]]  # the buffer this step writes
-        lat.step_planes(2, n - 2, False, main)  # the interior first: it takes its SMs before the side
+        _step_sides(lat, n, h, main, comm, self._ready)
         with torch.cuda.stream(comm):
-            comm.wait_event(self._ready)
-            lat.step_planes(1, 2, True, comm, stride=n - 1)  # planes 1 and n in one launch; ends the step
-            torch.index_select(F[:, n], 0, up_idx, out=b["send_up"].view(len(self.up_dirs), -1))
-            torch.index_select(F[:, 1], 0, down_idx, out=b["send_down"].view(len(self.down_dirs), -1))
+            _pack_views(F, n, h, self._up_seg, self._down_seg, self._up_idx, self._down_idx, b["send_up"],
+                        b["send_down"])
             if self.world == 1:
                 from_down, from_up = b["send_up"], b["send_down"]
             else:
@@ -286,8 +285,7 @@ class Slab:
                 for req in dist.batch_isend_irecv(ops):
                     req.wait()
                 from_down, from_up = b["recv_down"], b["recv_up"]
-            F[:, 0].index_copy_(0, up_idx, from_down.view(len(self.up_dirs), -1))
-            F[:, n + 1].index_copy_(0, down_idx, from_up.view(len(self.down_dirs), -1))
+            _unpack_views(F, n, h, self._up_seg, self._down_seg, self._up_idx, self._down_idx, from_down, from_up)
             self._done.record(comm)
         main.wait_event(self._done)
 
@@ -346,6 +344,56 @@ def _unpack(lat, n, h, up_seg, down_seg, from_down, from_up):
         lat.face_set(h + n + k, dirs, from_up[a:b])
 
 
+def _step_sides(lat, n, h, main, comm, ready):
+    """One step of a slab in pieces: its interior planes (2h .. n-1, read by no neighbour) on `main`, and
+    on `comm` (after `ready`) the planes its neighbours read (h .. 2h-1 and n .. n+h-1), which end the
+    step.  One ghost plane: both boundary planes in one strided launch."""
+    import torch
+
+    lat.step_planes(2 * h, n - 2 * h, False, main)  # the interior first: it takes its SMs before the side
+    with torch.cuda.stream(comm):
+        comm.wait_event(ready)
+        if h == 1:
+            lat.step_planes(1, 2, True, comm, stride=n - 1)
+        else:
+            lat.step_planes(h, h, False, comm)
+            lat.step_planes(n, h, True, comm)
+
+
+def _step_sides_all(lats, ns, h, main, comm, ready):
+    """_step_sides for every slab of a SlabSet: all interiors on `main` first, then the boundary planes."""
+    import torch
+
+    for lat, n in zip(lats, ns):
+        lat.step_planes(2 * h, n - 2 * h, False, main)
+    with torch.cuda.stream(comm):
+        comm.wait_event(ready)
+        for lat, n in zip(lats, ns):
+            if h == 1:
+                lat.step_planes(1, 2, True, comm, stride=n - 1)
+            else:
+                lat.step_planes(h, h, False, comm)
+                lat.step_planes(n, h, True, comm)
+
+
+def _pack_views(F, n, h, up_seg, down_seg, up_idx, down_idx, send_up, send_down):
+    """_pack from a [Q, planes, plane bytes] view of the buffer being written (on the current stream)."""
+    import torch
+
+    for (k, dirs, a, b), idx in zip(up_seg, up_idx):
+        torch.index_select(F[:, h + n - 1 - k], 0, idx, out=send_up[a:b].view(len(dirs), -1))
+    for (k, dirs, a, b), idx in zip(down_seg, down_idx):
+        torch.index_select(F[:, h + k], 0, idx, out=send_down[a:b].view(len(dirs), -1))
+
+
+def _unpack_views(F, n, h, up_seg, down_seg, up_idx, down_idx, from_down, from_up):
+    """_unpack into a [Q, planes, plane bytes] view of the buffer being written."""
+    for (k, dirs, a, b), idx in zip(up_seg, up_idx):
+        F[:, h - 1 - k].index_copy_(0, idx, from_down[a:b].view(len(dirs), -1))
+    for (k, dirs, a, b), idx in zip(down_seg, down_idx):
+        F[:, h + n + k].index_copy_(0, idx, from_up[a:b].view(len(dirs), -1))
+
+
 def _sums(lattice: int, Fi: np.ndarray) -> np.ndarray:
     cx, cy, cz, _, _ = velocities(lattice)
     per_dir = Fi.reshape(Fi.shape[0], -1).sum(axis=1)
@@ -382,7 +430,7 @@ class SlabSet:
         self._up = [np.empty(k, dtype=word) for _ in self.lats]
         self._down = [np.empty(k, dtype=word) for _ in self.lats]
         # overlapped steps: every lattice on one stream of the set's own, the face copies on a second
-        self.overlap = overlap and lattice_factory is None and min(self.ns) >= 3 and self.h == 1
+        self.overlap = overlap and isinstance(self.lats[0], Lattice) and min(self.ns) > 2 * self.h
         if self.overlap:
             import torch
 
@@ -392,9 +440,9 @@ class SlabSet:
                 lat.set_stream(self.stream.cuda_stream)
                 lat.set_reserved_sms(reserved_sms)
             self._comm = torch.cuda.Stream(device=self._dev, priority=-1)
-            self._views = [_plane_views(lat, n + 2, self._dev) for lat, n in zip(self.lats, self.ns)]
-            self._up_idx = torch.tensor(self.up_dirs, device=self._dev)
-            self._down_idx = torch.tensor(self.down_dirs, device=self._dev)
+            self._views = [_plane_views(lat, n + 2 * self.h, self._dev) for lat, n in zip(self.lats, self.ns)]
+            self._up_idx = [torch.tensor(dirs, device=self._dev) for _, dirs, _, _ in self._up_seg]
+            self._down_idx = [torch.tensor(dirs, device=self._dev) for _, dirs, _, _ in self._down_seg]
             self._ready, self._done = torch.cuda.Event(), torch.cuda.Event()
 
     def exchange(self):
@@ -419,20 +467,19 @@ class SlabSet:
         between the slabs' next buffers on the side stream, interior planes on the main stream."""
         import torch
 
-        main, comm, up_idx, down_idx = self.stream, self._comm, self._up_idx, self._down_idx
+        main, comm, h = self.stream, self._comm, self.h
         self._ready.record(main)
         F = [v[lat.device_buffers()[1]] for lat, v in zip(self.lats, self._views)]
         R = len(self.lats)
-        for lat, n in zip(self.lats, self.ns):
-            lat.step_planes(2, n - 2, False, main)
+        _step_sides_all(self.lats, self.ns, h, main, comm, self._ready)
         with torch.cuda.stream(comm):
-            comm.wait_event(self._ready)
-            for lat, n in zip(self.lats, self.ns):
-                lat.step_planes(1, 2, True, comm, stride=n - 1)
             for r, n in enumerate(self.ns):
                 lo, hi = (r - 1) % R, (r + 1) % R
-                F[r][:, 0].index_copy_(0, up_idx, F[lo][:, self.ns[lo]].index_select(0, up_idx))
-                F[r][:, n + 1].index_copy_(0, down_idx, F[hi][:, 1].index_select(0, down_idx))
+                # lower ghosts from the lower slab's top planes, upper ghosts from the upper slab's bottom ones
+                for (k, _, _, _), idx in zip(self._up_seg, self._up_idx):
+                    F[r][:, h - 1 - k].index_copy_(0, idx, F[lo][:, h + self.ns[lo] - 1 - k].index_select(0, idx))
+                for (k, _, _, _), idx in zip(self._down_seg, self._down_idx):
+                    F[r][:, h + n + k].index_copy_(0, idx, F[hi][:, h + k].index_select(0, idx))
             self._done.record(comm)
         main.wait_event(self._done)
 

@@ -251,10 +251,12 @@ def test_slabset_of_engine_lattices_equals_one_lattice(storage, case, parts, ove
 @pytest.mark.parametrize("case", ["shanchen2d", "shanchen_walls", "shanchen_wide"])
 @pytest.mark.parametrize("parts", [2, 3])
 @pytest.mark.parametrize("kernel", [lb.KERNEL_AUTO, lb.KERNEL_PLAIN])
-def test_shanchen_slabs_on_the_gpu_equal_one_lattice(storage, case, parts, kernel):
+@pytest.mark.parametrize("overlap", [False, True])
+def test_shanchen_slabs_on_the_gpu_equal_one_lattice(storage, case, parts, kernel, overlap):
     """Shan-Chen slabs on the engine (one-pass window kernel or the two-pass kernels, stochastic
-    rounding for BF16S hashed by global cell) with two ghost rows per side: bit-identical to one
-    lattice of the full size after 40 steps of phase separation."""
+    rounding for BF16S hashed by global cell) with two ghost rows per side, stepped then exchanged or
+    overlapped (the rows the neighbours read and their exchange on a side stream beside the interior
+    rows): bit-identical to one lattice of the full size after 40 steps of phase separation."""
     if case == "shanchen_wide":  # rows wider than one window strip, a ragged last strip
         d, m, F0 = shanchen2d(storage, nx=300, ny=26)
     else:
@@ -271,7 +273,8 @@ def test_shanchen_slabs_on_the_gpu_equal_one_lattice(storage, case, parts, kerne
         lat.step(40)
         ref = lat.get_populations(dtype)
         ref_sums = lat.sums()
-    s = SlabSet(d, m, F0, parts, lattice_factory=engine)
+    s = SlabSet(d, m, F0, parts, lattice_factory=engine, overlap=overlap)
+    assert s.overlap == overlap and s.h == 2
     try:
         s.step(40)
         got = s.gather_populations(dtype)
@@ -284,7 +287,8 @@ def test_shanchen_slabs_on_the_gpu_equal_one_lattice(storage, case, parts, kerne
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("storage", [lb.F32, lb.BF16S])
-def test_one_rank_shanchen_slab_on_the_gpu_equals_one_lattice(storage):
+@pytest.mark.parametrize("overlap", [False, True])
+def test_one_rank_shanchen_slab_on_the_gpu_equals_one_lattice(storage, overlap):
     """The rank-side Slab for Shan-Chen: device byte buffers holding both ghost rows' transfers per
     side, filled from the rank's own far rows (periodic wrap), equal to the undivided lattice."""
     import torch
@@ -294,8 +298,8 @@ def test_one_rank_shanchen_slab_on_the_gpu_equals_one_lattice(storage):
         lat.set_populations(np.asarray(F0, dtype=np.float64))
         lat.step(25)
         ref = lat.get_populations(np.float32)
-    slab = Slab(d, m, F0, 0, 1, device="cuda:0")
-    assert not slab.overlap and slab.h == 2
+    slab = Slab(d, m, F0, 0, 1, device="cuda:0", overlap=overlap)
+    assert slab.overlap == overlap and slab.h == 2
     assert slab._buf["send_up"].numel() == 9 * 96 * lb.STORAGE_BYTES[storage]
     slab.step(25)
     torch.cuda.synchronize()
@@ -363,17 +367,56 @@ def test_step_planes_in_pieces_equals_whole_steps(storage, kernel, case):
 
 
 @pytest.mark.gpu
-def test_step_planes_rejects_bad_ranges_and_shanchen():
+def test_step_planes_rejects_bad_ranges():
     d, m, _ = mrt_cavity3d(lb.F32, n=(32, 4, 5))
     with lb.Lattice(d, m) as lat:
         for first, count, stride in ((-1, 1, 1), (0, 0, 1), (4, 2, 1), (5, 1, 1), (0, 2, 0), (1, 2, 4), (1, 3, 2)):
             with pytest.raises(lb.LbmError):
                 lat.step_planes(first, count, True, stride=stride)
         assert lat.steps_done == 0
-    d = lb.make_desc(lb.D2Q9, lb.SHANCHEN, lb.F32, (32, 16), omega=1.0, sc_G=-5.0)
-    with lb.Lattice(d, None) as lat:
-        with pytest.raises(lb.LbmError):
-            lat.step_planes(0, 16, True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [lb.F32, lb.BF16S, lb.F64])
+@pytest.mark.parametrize("kernel", [lb.KERNEL_AUTO, lb.KERNEL_PLAIN, lb.KERNEL_ROWS])
+@pytest.mark.parametrize("case", ["shanchen_walls", "shanchen_wide"])
+def test_shanchen_step_planes_in_pieces_equals_whole_steps(storage, kernel, case):
+    """Shan-Chen plane sets (the one-pass window kernel whatever the family: contiguous rows, strided
+    rows, single rows) make the same step as lbm_step: bit-identical, stochastic rounding included,
+    with the pieces before the last on a side stream beside it."""
+    import torch
+
+    d, m, F0 = shanchen2d(storage, nx=300, ny=26) if case == "shanchen_wide" else shanchen_walls(storage, nx=96, ny=30)
+    planes = d.ny
+    F0 = np.asarray(F0, dtype=np.float64)
+    main, side = torch.cuda.Stream(), torch.cuda.Stream(priority=-1)
+    ready, done = torch.cuda.Event(), torch.cuda.Event()
+    dtype = np.float64 if storage == lb.F64 else np.float32
+    with lb.Lattice(d, m) as a, lb.Lattice(d, m) as b:
+        for lat in (a, b):
+            lat.set_kernel(kernel)
+            lat.set_populations(F0)
+        a.step(8)
+        b.set_stream(main)
+        # the slab's order (two bottom rows, two top rows beside the interior), contiguous ranges,
+        # single rows backwards, and the odd rows then the even ones
+        cuts = [[(2, 2, 1), (planes - 4, 2, 1), (4, planes - 8, 1), (0, 2, 1), (planes - 2, 2, 1)],
+                [(3, planes - 3, 1), (0, 3, 1)],
+                [(k, 1, 1) for k in range(planes - 1, -1, -1)],
+                [(1, planes // 2, 2), (0, (planes + 1) // 2, 2)]]
+        for t in range(8):
+            pieces = cuts[t % len(cuts)]
+            ready.record(main)
+            side.wait_event(ready)
+            for k, (first, count, stride) in enumerate(pieces):
+                last = k == len(pieces) - 1
+                b.step_planes(first, count, last, main if last else side, stride=stride)
+            done.record(side)
+            main.wait_event(done)
+        assert b.steps_done == a.steps_done == 8
+        ref, got = a.get_populations(dtype), b.get_populations(dtype)
+        b.set_stream(None)
+    assert np.isfinite(got).all() and np.array_equal(got, ref)
 
 
 @pytest.mark.gpu
