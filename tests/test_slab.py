@@ -447,13 +447,16 @@ def test_one_rank_slab_on_the_gpu_equals_one_lattice(storage, overlap):
 
 
 @pytest.mark.gpu
-def test_bench_slab_line():
-    """bench.py --slab: one JSON line with the overlapped, sequential and undivided step times."""
+@pytest.mark.parametrize("workload,dims", [("d3q27_mrt_gs_lid_256", "64x32x24"), ("d2q9_shanchen_1024", "256x64")])
+def test_bench_slab_line(workload, dims):
+    """bench.py --slab: one JSON line with the overlapped, sequential and undivided step times (D3Q27
+    MRT, and Shan-Chen with its two ghost rows per side)."""
     import subprocess
     import sys
 
     root = Path(__file__).resolve().parents[1]
-    cmd = [sys.executable, str(root / "bench.py"), "--slab", "--dims", "64x32x24", "--steps", "4", "--warmup", "1"]
+    cmd = [sys.executable, str(root / "bench.py"), "--slab", "--workload", workload, "--dims", dims, "--steps", "4",
+           "--warmup", "1"]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=str(root))
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads(out.stdout.strip().splitlines()[-1])
