@@ -789,9 +789,10 @@ __global__ void __launch_bounds__(256) k_step_mrt2(const __grid_constant__ StepP
 // Pass 1: psi = 1 - exp(-rho) of the streamed density of every cell.
 // psi = 1 - exp(-rho) of the streamed density of one cell (the pseudopotential of the Shan-Chen
 // force); also returns the cell's pulled populations and class, which the collision reuses.
-template <class S, bool ABS, class R>
-__device__ __forceinline__ void sc_pull_cell(const StepParams<R>& p, const S* __restrict__ fin, const Rows<D2Q9>& rows,
-                                             int x, long long c, R (&v)[9], int& cls, uint32_t& fl) {
+template <class S, bool ABS, class R, class Ix>
+__device__ __forceinline__ void sc_pull_cell(const StepParams<R>& p, const S* __restrict__ fin,
+                                             const RowsT<D2Q9, Ix>& rows, int x, Ix c, R (&v)[9], int& cls,
+                                             uint32_t& fl) {
     using L = D2Q9;
     pull<L, S, ABS>(fin, p, rows, x, v);
     cell_class(p.mask, p.cls, c, cls, fl);
@@ -807,9 +808,9 @@ __device__ __forceinline__ R sc_psi_from(const StepParams<R>& p, const R (&v)[9]
     if (fl & kSetRho) rho = R(p.cls.rho[cls]);
     return R(1) - exp(-rho);
 }
-template <class S, bool ABS, class R>
-__device__ __forceinline__ R sc_psi_of(const StepParams<R>& p, const S* __restrict__ fin, const Rows<D2Q9>& rows,
-                                       int x, long long c, R (&v)[9], int& cls, uint32_t& fl) {
+template <class S, bool ABS, class R, class Ix>
+__device__ __forceinline__ R sc_psi_of(const StepParams<R>& p, const S* __restrict__ fin, const RowsT<D2Q9, Ix>& rows,
+                                       int x, Ix c, R (&v)[9], int& cls, uint32_t& fl) {
     sc_pull_cell<S, ABS>(p, fin, rows, x, c, v, cls, fl);
     return sc_psi_from<S, ABS>(p, v, cls, fl);
 }
@@ -862,15 +863,17 @@ __device__ __forceinline__ void sc_pull_cell32(const StepParams<R>& p, const S* 
     }
 }
 
-template <class S, bool ABS>
+// I32: 32-bit population indices (lattices with 9 N <= 2^32).
+template <class S, bool ABS, bool I32 = false>
 __global__ void __launch_bounds__(512) k_sc_psi(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D2Q9;
     using R = typename Codec<S>::Real;
+    using Ix = typename std::conditional<I32, uint32_t, long long>::type;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
     const int y = blockIdx.y, z = blockIdx.z;
-    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
-    const long long c = rows.base[1][1] + x;
+    const RowsT<L, Ix> rows(y, z, p.nx, p.ny, p.nz);
+    const Ix c = rows.base[1][1] + (Ix)x;
     R v[9];
     int cls;
     uint32_t fl;
@@ -898,16 +901,16 @@ __device__ __forceinline__ void sc_force_from(const StepParams<R>& p, PsiAt&& ps
 }
 
 // The force at cell (x, y) from the psi field in global memory (periodic).
-template <class R>
-__device__ __forceinline__ void sc_force(const StepParams<R>& p, const Rows<D2Q9>& rows, int x,
-                                         long long c, R& Fx, R& Fy) {
+template <class R, class Ix>
+__device__ __forceinline__ void sc_force(const StepParams<R>& p, const RowsT<D2Q9, Ix>& rows, int x, Ix c, R& Fx,
+                                         R& Fy) {
     const int xm = x == 0 ? p.nx - 1 : x - 1;
     const int xp = x == p.nx - 1 ? 0 : x + 1;
     sc_force_from(p, [&](int dx, int dy) {
         if (dx == 0 && dy == 0) return __ldg(p.psi + c);
         // neighbour x + c_i: the source row of the opposite direction
         const int xn = dx == 1 ? xp : (dx == -1 ? xm : x);
-        return __ldg(p.psi + rows.src(-dy, 0) + xn);
+        return __ldg(p.psi + (rows.src(-dy, 0) + (Ix)xn));
     }, Fx, Fy);
 }
 
@@ -949,15 +952,16 @@ __device__ __forceinline__ void sc_collide_store(const StepParams<R>& p, Idx c, 
 }
 
 // Second pass of the two-pass Shan-Chen step (psi from k_sc_psi in global memory).
-template <class S, bool ABS>
+template <class S, bool ABS, bool I32 = false>
 __global__ void __launch_bounds__(512) k_step_sc(const __grid_constant__ StepParams<typename Codec<S>::Real> p) {
     using L = D2Q9;
     using R = typename Codec<S>::Real;
+    using Ix = typename std::conditional<I32, uint32_t, long long>::type;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= p.nx) return;
     const int y = blockIdx.y, z = blockIdx.z;
-    const Rows<L> rows(y, z, p.nx, p.ny, p.nz);
-    const long long c = rows.base[1][1] + x;
+    const RowsT<L, Ix> rows(y, z, p.nx, p.ny, p.nz);
+    const Ix c = rows.base[1][1] + (Ix)x;
     const S* __restrict__ fin = static_cast<const S*>(p.fin);
     R v[9];
     pull<L, S, ABS>(fin, p, rows, x, v);

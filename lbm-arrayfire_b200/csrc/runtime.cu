@@ -382,8 +382,8 @@ static void dispatch_rows(const lbm_ctx* c, F&& f) {
 #ifndef LBM_IDX32
 #define LBM_IDX32 1  // 0: the plain and window kernels always index populations in 64 bits (A/B)
 #endif
-// The plain step kernels and the Shan-Chen window kernel index populations in 32 bits when all Q N of
-// them have 32-bit indices (largest index Q N - 1).
+// The plain step kernels (the two Shan-Chen passes included) and the Shan-Chen window kernel index
+// populations in 32 bits when all Q N of them have 32-bit indices (largest index Q N - 1).
 static bool idx32(const lbm_ctx* c) {
     const unsigned long long n = (unsigned long long)c->d.nx * (unsigned long long)c->d.ny * (unsigned long long)c->d.nz;
     const unsigned long long q = c->d.lattice == LBM_D3Q27 ? 27ULL : 9ULL;
@@ -518,11 +518,11 @@ static void launch_step(lbm_ctx* c, int from, cudaStream_t s, int block, int plo
                 break;
             default:
                 if (abs_arith) {
-                    k_sc_psi<S, true><<<grid, blk, 0, s>>>(p);
-                    k_step_sc<S, true><<<grid, blk, 0, s>>>(p);
+                    (i32 ? k_sc_psi<S, true, true> : k_sc_psi<S, true, false>)<<<grid, blk, 0, s>>>(p);
+                    (i32 ? k_step_sc<S, true, true> : k_step_sc<S, true, false>)<<<grid, blk, 0, s>>>(p);
                 } else {
-                    k_sc_psi<S, false><<<grid, blk, 0, s>>>(p);
-                    k_step_sc<S, false><<<grid, blk, 0, s>>>(p);
+                    (i32 ? k_sc_psi<S, false, true> : k_sc_psi<S, false, false>)<<<grid, blk, 0, s>>>(p);
+                    (i32 ? k_step_sc<S, false, true> : k_step_sc<S, false, false>)<<<grid, blk, 0, s>>>(p);
                 }
                 break;
         }

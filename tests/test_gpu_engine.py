@@ -404,9 +404,9 @@ def test_row_pipeline_segmented_wide_rows_equal_plain(storage, case):
                                          ((48, 36), True), ((200, 24), "zerograd")])
 def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
     """The one-pass Shan-Chen kernel (KERNEL_ROWS: a window sliding down y, psi of the next row in a
-    shared ring), with 32-bit population indices (its choice on these lattices) and with 64-bit ones
-    (the form of lattices beyond 2^32 / 9 cells, forced by a test hook), against the two-pass kernels
-    (KERNEL_PLAIN: psi through global memory): bit-identical populations and fields, on full and
+    shared ring) against the two-pass kernels (KERNEL_PLAIN: psi through global memory), each with
+    32-bit population indices (their choice on these lattices) and with 64-bit ones (the form of
+    lattices beyond 2^32 / 9 cells, forced by a test hook): bit-identical populations and fields, on full and
     partial column strips, a lattice narrower than a strip, with solid (bounce-back, set-density)
     cells, and with zero-gradient outlet columns on both sides of the first strip edge (x = 127 and
     128: the window pulls them both as its own cells and as the neighbouring strip's edge column)."""
@@ -427,7 +427,8 @@ def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
     rng = np.random.default_rng(4)
     rho = 0.693 + 0.01 * rng.uniform(-1.0, 1.0, size=n)
     out = {}
-    for kind, index64 in ((lb.KERNEL_PLAIN, False), (lb.KERNEL_ROWS, False), (lb.KERNEL_ROWS, True)):
+    for kind, index64 in ((lb.KERNEL_PLAIN, False), (lb.KERNEL_PLAIN, True), (lb.KERNEL_ROWS, False),
+                          (lb.KERNEL_ROWS, True)):
         with lb.Lattice(d, m) as lat:
             lat.set_kernel(kind)
             if index64:
@@ -439,7 +440,7 @@ def test_shanchen_fused_equals_two_pass(storage, arith, shape, solid):
             r, u = lat.macros()
             out[kind, index64] = (lat.get_populations(np.float64), r, u)
     a = out[lb.KERNEL_PLAIN, False]
-    for key in ((lb.KERNEL_ROWS, False), (lb.KERNEL_ROWS, True)):
+    for key in ((lb.KERNEL_PLAIN, True), (lb.KERNEL_ROWS, False), (lb.KERNEL_ROWS, True)):
         b = out[key]
         assert np.isfinite(b[0]).all()
         for x, y in zip(a, b):
